@@ -1,0 +1,12 @@
+"""B200-native v-omega Fourier-Chebyshev DNS time step.
+
+Host-side mirror of the reference's interface over the C ABI of
+``libdnsb200.so`` (declared in ``include/dns_b200.h``).  All compute runs in
+the CUDA library; this package only moves buffers and parameters.
+"""
+from .abi import (  # noqa: F401
+    BACKWARD, DEVICE, FORWARD, HOST, NO_PADDING, PADDING, PREC_FP64, PREC_MIXED,
+    Context, DnsError, DnsParams, EXPORTS, LIB_PATH, load_library, make_params,
+    read_parameter_file,
+)
+from .seed import seeded_state  # noqa: F401

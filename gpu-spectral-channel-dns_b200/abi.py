@@ -1,0 +1,264 @@
+"""ctypes binding of libdnsb200.so (include/dns_b200.h).
+
+The library is the only compute path: if it is missing, or no CUDA device is
+present, creating a context raises; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdnsb200.so")
+
+FORWARD, BACKWARD = 0, 1
+PADDING, NO_PADDING = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+HOST, DEVICE = 0, 1
+
+# every entry point declared in include/dns_b200.h
+EXPORTS = [
+    "dns_status_string", "dns_last_error", "dns_abi_version", "dns_params_default",
+    "dns_read_parameter_file", "dns_create", "dns_destroy", "dns_geometry", "dns_get_stream",
+    "dns_synchronize", "dns_memory_bytes", "dns_set_state", "dns_get_state",
+    "dns_get_history", "dns_set_history", "dns_bootstrap", "dns_step",
+    "dns_transform_3d_one", "dns_transform", "dns_cuda_transpose", "dns_cheby_s2p",
+    "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
+    "dns_init_aux_matrix",
+]
+
+
+class DnsParams(C.Structure):
+    _fields_ = [
+        ("mx", C.c_int), ("my", C.c_int), ("mz", C.c_int),
+        ("n_pi_x", C.c_double), ("n_pi_y", C.c_double),
+        ("Re", C.c_double), ("Ro", C.c_double), ("dt", C.c_double),
+        ("U0", C.c_double), ("U1", C.c_double), ("U2", C.c_double),
+        ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+class DnsRunParams(C.Structure):
+    _fields_ = [
+        ("start_type", C.c_int), ("start_step", C.c_int), ("end_step", C.c_int),
+        ("save_internal", C.c_int), ("save_recovery_internal", C.c_int),
+        ("output_file_prefix", C.c_char * 512), ("recovery_file_prefix", C.c_char * 512),
+    ]
+
+
+class DnsError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"dns status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libdnsb200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"{p} is missing: run build.py (nvcc, sm_100a) first")
+    lib = C.CDLL(p)
+    vp = C.c_void_p
+    sz = C.c_size_t
+    i = C.c_int
+    lib.dns_status_string.restype = C.c_char_p
+    lib.dns_status_string.argtypes = [i]
+    lib.dns_last_error.restype = C.c_char_p
+    lib.dns_last_error.argtypes = []
+    lib.dns_abi_version.restype = i
+    sigs = {
+        "dns_params_default": [C.POINTER(DnsParams)],
+        "dns_read_parameter_file": [C.c_char_p, C.POINTER(DnsParams), C.POINTER(DnsRunParams)],
+        "dns_create": [C.POINTER(DnsParams), C.POINTER(vp)],
+        "dns_destroy": [vp],
+        "dns_geometry": [vp, C.POINTER(C.c_int)],
+        "dns_get_stream": [vp, C.POINTER(vp)],
+        "dns_synchronize": [vp],
+        "dns_memory_bytes": [vp, C.POINTER(sz)],
+        "dns_set_state": [vp, vp, vp, sz, i],
+        "dns_get_state": [vp, vp, vp, sz, i],
+        "dns_get_history": [vp, vp, vp, sz, i],
+        "dns_set_history": [vp, vp, vp, sz, i],
+        "dns_bootstrap": [vp],
+        "dns_step": [vp, i],
+        "dns_transform_3d_one": [vp, i, vp, sz, vp, sz, i],
+        "dns_transform": [vp, i, i, C.POINTER(vp), sz, C.POINTER(vp), sz],
+        "dns_cuda_transpose": [vp, i, vp, sz, vp, sz],
+        "dns_cheby_s2p": [vp, vp, sz, i],
+        "dns_cheby_p2s": [vp, vp, sz, i],
+        "dns_get_uvw": [vp, C.POINTER(vp), sz],
+        "dns_compute_lamb": [vp, C.POINTER(vp), C.POINTER(vp), sz],
+        "dns_rhs_nonlinear": [vp, vp, vp, vp, sz],
+        "dns_solve_eq": [vp, vp, vp, i, sz],
+        "dns_init_aux_matrix": [vp, vp, vp, i],
+    }
+    for name, args in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = i
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, st):
+    if st != 0:
+        raise DnsError(st, lib.dns_last_error().decode(errors="replace"))
+
+
+def make_params(mx, my, mz, n_pi_x=4.0, n_pi_y=2.0, Re=1300.0, Ro=0.0, dt=0.005,
+                U=(0.5, 0.5, 0.0), precision=PREC_FP64, device=0) -> DnsParams:
+    p = DnsParams()
+    p.mx, p.my, p.mz = mx, my, mz
+    p.n_pi_x, p.n_pi_y = n_pi_x, n_pi_y
+    p.Re, p.Ro, p.dt = Re, Ro, dt
+    p.U0, p.U1, p.U2 = U
+    p.precision = precision
+    p.device = device
+    return p
+
+
+def read_parameter_file(path):
+    lib = load_library()
+    p = DnsParams()
+    r = DnsRunParams()
+    _check(lib, lib.dns_read_parameter_file(path.encode(), C.byref(p), C.byref(r)))
+    return p, r
+
+
+def _ptrs(seq):
+    arr = (C.c_void_p * len(seq))(*[C.c_void_p(int(x)) for x in seq])
+    return arr
+
+
+class Context:
+    """One DNS problem on one GPU (a ``dns_ctx``)."""
+
+    def __init__(self, params: DnsParams):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib, self.lib.dns_create(C.byref(params), C.byref(h)))
+        self.h = h
+        self.params = params
+        g = (C.c_int * 8)()
+        _check(self.lib, self.lib.dns_geometry(self.h, g))
+        self.Nx, self.Ny, self.Nz, self.Kx, self.Px, self.Py, self.Pz, self.H = list(g)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dns_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- helpers -----------------------------------------------------------
+    def _call(self, name, *args):
+        _check(self.lib, getattr(self.lib, name)(self.h, *args))
+
+    @property
+    def stream(self):
+        s = C.c_void_p()
+        self._call("dns_get_stream", C.byref(s))
+        return s.value
+
+    def memory_bytes(self):
+        b = C.c_size_t()
+        self._call("dns_memory_bytes", C.byref(b))
+        return b.value
+
+    def synchronize(self):
+        self._call("dns_synchronize")
+
+    # -- state (numpy host arrays, shape (Nz, Kx, Ny) complex128) -----------
+    def _pencils(self, a):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.shape != (self.Nz, self.Kx, self.Ny):
+            raise ValueError(f"expected shape {(self.Nz, self.Kx, self.Ny)}, got {a.shape}")
+        return a
+
+    def set_state(self, V, O):
+        V = self._pencils(V)
+        O = self._pencils(O)
+        self._call("dns_set_state", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
+
+    def get_state(self):
+        V = np.empty((self.Nz, self.Kx, self.Ny), dtype=np.complex128)
+        O = np.empty_like(V)
+        self._call("dns_get_state", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
+        return V, O
+
+    def get_history(self):
+        V = np.empty((self.Nz, self.Kx, self.Ny), dtype=np.complex128)
+        O = np.empty_like(V)
+        self._call("dns_get_history", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
+        return V, O
+
+    def set_history(self, Nv, No):
+        Nv = self._pencils(Nv)
+        No = self._pencils(No)
+        self._call("dns_set_history", Nv.ctypes.data, No.ctypes.data, self.Ny * 16, HOST)
+
+    def set_state_device(self, v_ptr, o_ptr, pitch):
+        self._call("dns_set_state", C.c_void_p(v_ptr), C.c_void_p(o_ptr), pitch, DEVICE)
+
+    def get_state_device(self, v_ptr, o_ptr, pitch):
+        self._call("dns_get_state", C.c_void_p(v_ptr), C.c_void_p(o_ptr), pitch, DEVICE)
+
+    def bootstrap(self):
+        self._call("dns_bootstrap")
+
+    def step(self, n=1):
+        self._call("dns_step", int(n))
+
+    # -- reference-layout entry points (device pointers as ints) -----------
+    def transform_3d_one(self, direction, phys, pitch, spec, tpitch, pad=PADDING):
+        self._call("dns_transform_3d_one", int(direction), C.c_void_p(phys), pitch,
+                   C.c_void_p(spec), tpitch, int(pad))
+
+    def transform(self, direction, phys, pitch, spec, tpitch):
+        self._call("dns_transform", int(direction), len(phys), _ptrs(phys), pitch, _ptrs(spec), tpitch)
+
+    def cuda_transpose(self, direction, xyz, pitch, zxy, tpitch):
+        self._call("dns_cuda_transpose", int(direction), C.c_void_p(xyz), pitch, C.c_void_p(zxy), tpitch)
+
+    def cheby_s2p(self, zxy, tpitch, pad=PADDING):
+        self._call("dns_cheby_s2p", C.c_void_p(zxy), tpitch, int(pad))
+
+    def cheby_p2s(self, zxy, tpitch, pad=PADDING):
+        self._call("dns_cheby_p2s", C.c_void_p(zxy), tpitch, int(pad))
+
+    def get_uvw(self, fields, tpitch):
+        self._call("dns_get_uvw", _ptrs(fields), tpitch)
+
+    def compute_lamb(self, fin, fout, pitch):
+        self._call("dns_compute_lamb", _ptrs(fin), _ptrs(fout), pitch)
+
+    def rhs_nonlinear(self, lx, ly, lz, tpitch):
+        self._call("dns_rhs_nonlinear", C.c_void_p(lx), C.c_void_p(ly), C.c_void_p(lz), tpitch)
+
+    def solve_eq(self, inv, rhs, N, tpitch):
+        self._call("dns_solve_eq", C.c_void_p(inv), C.c_void_p(rhs), int(N), tpitch)
+
+    def init_aux_matrix(self, inv_v, inv_o, where=DEVICE):
+        if where == HOST:
+            self._call("dns_init_aux_matrix", inv_v.ctypes.data, inv_o.ctypes.data, HOST)
+        else:
+            self._call("dns_init_aux_matrix", C.c_void_p(inv_v), C.c_void_p(inv_o), DEVICE)

@@ -1,0 +1,589 @@
+// dns_ctx: device buffers, FFT tables, operator inverses and the C ABI of
+// libdnsb200.so (include/dns_b200.h).
+//
+// One context = one problem on one device, one CUDA stream, no host threads.
+// The reference splits a step over two host threads, the GPU and PCIe
+// (source/solver.cpp:35-101, source/rhs.cpp:15-183); here the whole step is
+// six kernels on one stream, captured once into a CUDA graph:
+//
+//   y3  state (v, omega_y) -> getUVW -> padded s2p -> six pencil fields
+//   zb  spanwise inverse FFT with padding, transpose to streamwise rows
+//   x   streamwise C2R -> Lamb vector + rotation -> R2C
+//   zf  spanwise forward FFT with truncation, transpose back to pencils
+//   y1  p2s -> rhsNonlinear -> collocation values -> CN/AB2 right-hand sides
+//   y2  v solve, tilting term, omega solve (explicit inverses streamed)
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/dns_b200.h"
+#include "kernels.cuh"
+#include "setup.cuh"
+#include "ypass.cuh"
+#include "zxpass.cuh"
+
+namespace {
+thread_local std::string g_err;
+
+dns_status fail(dns_status s, const std::string& m) {
+  g_err = m;
+  return s;
+}
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return fail(DNS_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename C> struct DevFft {
+  FftPlan plan;
+  C* tw = nullptr;
+  short* drev = nullptr;
+  FftTab<C> tab() const {
+    FftTab<C> t;
+    t.plan = plan;
+    t.tw = tw;
+    t.drev = drev;
+    return t;
+  }
+};
+
+template <typename C> cudaError_t make_fft(int L, DevFft<C>& f) {
+  if (!fft_make_plan(L, &f.plan)) return cudaErrorInvalidValue;
+  std::vector<C> tw(L);
+  std::vector<short> dr(L);
+  const long double PI = 3.141592653589793238462643383279502884L;
+  for (int j = 0; j < L; ++j) {
+    const long double a = -2.0L * PI * (long double)j / (long double)L;
+    tw[j] = cmk<C>((double)cosl(a), (double)sinl(a));
+    dr[j] = (short)fft_digitrev(f.plan, j);
+  }
+  cudaError_t e = cudaMalloc(&f.tw, sizeof(C) * L);
+  if (e) return e;
+  e = cudaMalloc(&f.drev, sizeof(short) * L);
+  if (e) return e;
+  e = cudaMemcpy(f.tw, tw.data(), sizeof(C) * L, cudaMemcpyHostToDevice);
+  if (e) return e;
+  return cudaMemcpy(f.drev, dr.data(), sizeof(short) * L, cudaMemcpyHostToDevice);
+}
+template <typename C> void free_fft(DevFft<C>& f) {
+  cudaFree(f.tw);
+  cudaFree(f.drev);
+  f.tw = nullptr;
+  f.drev = nullptr;
+}
+
+bool fft_len_ok(int L) {
+  FftPlan p;
+  return L >= 2 && L <= 16384 && fft_make_plan(L, &p);
+}
+
+long long roundup(long long a, long long b) { return (a + b - 1) / b * b; }
+}  // namespace
+
+struct dns_ctx {
+  dns_params P;
+  DnsGeom g;
+  PhysParams ph;
+  cudaStream_t st = nullptr;
+  size_t bytes = 0;
+  long long PyS = 0, KxS = 0, RS = 0;
+  // tables
+  DevFft<double2> fz_d, fx_d, fyP_d, fy0_d;
+  DevFft<float2> fz_f, fx_f, fyP_f;
+  double *T0 = nullptr, *T2 = nullptr, *T4 = nullptr;
+  double *Ut = nullptr, *dUt = nullptr, *ddUt = nullptr, *Uy = nullptr;
+  // state
+  double2 *V = nullptr, *O = nullptr, *Nvp = nullptr, *Nop = nullptr, *rv = nullptr, *ro = nullptr;
+  double2* AT = nullptr;
+  void* F6 = nullptr;
+  void* G6 = nullptr;
+  double2* scratch = nullptr;
+  int* status = nullptr;
+  bool have_state = false, booted = false, inverses = false;
+  cudaGraphExec_t graph = nullptr;
+
+  template <typename T> cudaError_t alloc(T** p, size_t n) {
+    bytes += n * sizeof(T);
+    return cudaMalloc((void**)p, n * sizeof(T));
+  }
+};
+
+namespace {
+dns_status check_status(dns_ctx* c) {
+  int s = 0;
+  CK(cudaMemcpyAsync(&s, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (s & 1) return fail(DNS_ERR_TIMEOUT, "a device wait ran past its iteration limit");
+  if (s & 2) return fail(DNS_ERR_SINGULAR, "an operator matrix had a zero pivot");
+  return DNS_OK;
+}
+
+dns_status build_inverses(dns_ctx* c) {
+  if (c->inverses) return DNS_OK;
+  const long long nunits = (long long)c->g.Kx * c->g.Kh;
+  CK(launch_gj_invert(0, 0, nunits, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt, c->AT,
+                      nullptr, nullptr, c->status, c->st));
+  dns_status s = check_status(c);
+  if (s != DNS_OK) return s;
+  c->inverses = true;
+  return DNS_OK;
+}
+
+template <typename C>
+cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const DevFft<C>& fx,
+                             const DevFft<C>& fyP) {
+  const DnsGeom& g = c->g;
+  const long long H = g.H;
+  PencilArr F6p{c->F6, c->PyS, H * c->PyS};
+  RowArr G6r{c->G6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
+  RowArr G3r{c->F6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
+  PencilArr F3p{c->G6, c->PyS, H * c->PyS};
+  cudaError_t e;
+  if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->st))) return e;
+  if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st))) return e;
+  if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->st))) return e;
+  if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
+  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, c->Ut, c->ddUt, g, c->ph,
+                        fyP.tab(), c->fy0_d.tab(), boot, c->st)))
+    return e;
+  if (!boot)
+    if ((e = launch_y2(c->AT, c->V, c->O, c->rv, c->ro, c->dUt, g, c->ph, c->fy0_d.tab(),
+                       c->status, c->st)))
+      return e;
+  return cudaSuccess;
+}
+
+cudaError_t enqueue(dns_ctx* c, int boot) {
+  if (c->P.precision == DNS_PREC_MIXED) return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f);
+  return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d);
+}
+
+dns_status need_scratch(dns_ctx* c) {
+  if (c->scratch) return DNS_OK;
+  CK(c->alloc(&c->scratch, (size_t)c->g.Py * c->g.Pz * c->RS));
+  return DNS_OK;
+}
+
+cudaMemcpyKind kind_of(int where, bool to_device) {
+  if (where == DNS_DEVICE) return cudaMemcpyDeviceToDevice;
+  return to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+}
+}  // namespace
+
+extern "C" {
+
+const char* dns_status_string(dns_status s) {
+  switch (s) {
+    case DNS_OK: return "ok";
+    case DNS_ERR_ARG: return "invalid argument";
+    case DNS_ERR_CUDA: return "CUDA error";
+    case DNS_ERR_STATE: return "call out of order";
+    case DNS_ERR_TIMEOUT: return "device wait timed out";
+    case DNS_ERR_SINGULAR: return "singular operator";
+    case DNS_ERR_IO: return "file error";
+    case DNS_ERR_NONFINITE: return "non-finite state";
+  }
+  return "unknown";
+}
+
+const char* dns_last_error(void) { return g_err.c_str(); }
+int dns_abi_version(void) { return DNS_B200_ABI_VERSION; }
+
+dns_status dns_params_default(dns_params* p) {
+  if (!p) return fail(DNS_ERR_ARG, "null params");
+  std::memset(p, 0, sizeof(*p));
+  p->mx = 128; p->my = 128; p->mz = 128;
+  p->n_pi_x = 4.0; p->n_pi_y = 2.0;
+  p->Re = 2600; p->Ro = 0.015; p->dt = 0.005;
+  p->U0 = 0.5; p->U1 = 0.5; p->U2 = 0.0;
+  p->precision = DNS_PREC_FP64;
+  p->device = 0;
+  return DNS_OK;
+}
+
+dns_status dns_read_parameter_file(const char* path, dns_params* p, dns_run_params* rp) {
+  if (!path || !p) return fail(DNS_ERR_ARG, "null argument");
+  std::ifstream in(path);
+  if (!in.is_open()) return fail(DNS_ERR_IO, std::string("cannot open ") + path);
+  dns_params q;
+  dns_params_default(&q);
+  dns_run_params r;
+  std::memset(&r, 0, sizeof(r));
+  std::string outp, recp;
+  if (!(in >> q.mx >> q.my >> q.mz >> q.n_pi_x >> q.n_pi_y >> q.Re >> q.Ro >> q.dt))
+    return fail(DNS_ERR_IO, "parameter file: numerical records missing or malformed");
+  if (!(in >> r.start_type >> r.start_step >> r.end_step >> r.save_internal >> r.save_recovery_internal))
+    return fail(DNS_ERR_IO, "parameter file: step record missing or malformed");
+  if (!(in >> outp >> recp)) return fail(DNS_ERR_IO, "parameter file: output prefixes missing");
+  if (outp.size() >= sizeof(r.output_file_prefix) || recp.size() >= sizeof(r.recovery_file_prefix))
+    return fail(DNS_ERR_IO, "parameter file: prefix too long");
+  std::strcpy(r.output_file_prefix, outp.c_str());
+  std::strcpy(r.recovery_file_prefix, recp.c_str());
+  *p = q;
+  if (rp) *rp = r;
+  return DNS_OK;
+}
+
+dns_status dns_create(const dns_params* p, dns_ctx** out) {
+  if (!p || !out) return fail(DNS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->mx <= 0 || p->my <= 0 || p->mz <= 0 || p->mz % 4 != 0)
+    return fail(DNS_ERR_ARG, "mx, my, mz must be positive and mz a multiple of 4");
+  if (!(p->Re > 0) || !(p->dt > 0) || !(p->n_pi_x > 0) || !(p->n_pi_y > 0))
+    return fail(DNS_ERR_ARG, "Re, dt and box lengths must be positive");
+  if (p->precision != DNS_PREC_FP64 && p->precision != DNS_PREC_MIXED)
+    return fail(DNS_ERR_ARG, "unknown precision");
+  DnsGeom g = dns_make_geom(p->mx, p->my, p->mz);
+  if (g.Nx < 2 || g.Nz < 2 || g.Nx % 2 || g.Nz % 2 || g.Ny < 5)
+    return fail(DNS_ERR_ARG, "need even Nx, Nz >= 2 and Ny >= 5");
+  if (!fft_len_ok(g.Px) || !fft_len_ok(g.Pz) || !fft_len_ok(p->mz) || !fft_len_ok(p->mz / 2))
+    return fail(DNS_ERR_ARG, "mx, my, mz and mz/2 must be products of 2 and 3 (2^a 3^b)");
+  if (g.Px < g.Nx || g.Pz < g.Nz) return fail(DNS_ERR_ARG, "padded sizes below mode counts");
+  if (gj_cluster_size(g.Ny) < 0) return fail(DNS_ERR_ARG, "Ny too large for the operator inversion");
+  if (2 * g.Ny > 1024) return fail(DNS_ERR_ARG, "Ny too large for the solve kernel");
+
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (p->device < 0 || p->device >= ndev) return fail(DNS_ERR_ARG, "no such CUDA device");
+  CK(cudaSetDevice(p->device));
+
+  dns_ctx* c = new dns_ctx();
+  c->P = *p;
+  c->g = g;
+  c->ph.aphi = p->n_pi_x / 2;
+  c->ph.beta = p->n_pi_y / 2;
+  c->ph.Re = p->Re;
+  c->ph.Ro = p->Ro;
+  c->ph.dt = p->dt;
+  c->ph.U0 = p->U0;
+  c->ph.U1 = p->U1;
+  c->ph.U2 = p->U2;
+  c->PyS = roundup(g.Py, 8);
+  c->KxS = roundup(g.Kx, 8);
+  c->RS = roundup(g.Px / 2 + 1, 8);
+  auto bail = [&](dns_status s) { dns_destroy(c); return s; };
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) return bail(fail(DNS_ERR_CUDA, "stream"));
+  cudaError_t e = cudaSuccess;
+  e = e ? e : make_fft(g.Pz, c->fz_d);
+  e = e ? e : make_fft(g.Px, c->fx_d);
+  e = e ? e : make_fft(p->mz, c->fyP_d);
+  e = e ? e : make_fft(p->mz / 2, c->fy0_d);
+  e = e ? e : make_fft(g.Pz, c->fz_f);
+  e = e ? e : make_fft(g.Px, c->fx_f);
+  e = e ? e : make_fft(p->mz, c->fyP_f);
+  if (e) return bail(fail(DNS_ERR_CUDA, std::string("fft tables: ") + cudaGetErrorString(e)));
+
+  const int Ny = g.Ny;
+  std::vector<double> T0((size_t)Ny * Ny), T2((size_t)Ny * Ny), T4((size_t)Ny * Ny);
+  host_T_matrix(Ny - 1, T0.data(), T2.data(), T4.data());
+  std::vector<double> U(Ny), dU(Ny), ddU(Ny), Uy(g.Py);
+  host_base_flow(Ny, p->U0, p->U1, p->U2, U.data(), dU.data(), ddU.data());
+  host_base_flow(g.Py, p->U0, p->U1, p->U2, Uy.data(), nullptr, nullptr);
+  const size_t NN = (size_t)Ny * Ny;
+  const size_t csz = p->precision == DNS_PREC_MIXED ? 8 : 16;
+  const size_t f6 = std::max((size_t)6 * g.H * c->PyS, (size_t)3 * g.Py * g.Pz * c->KxS);
+  const size_t g6 = std::max((size_t)6 * g.Py * g.Pz * c->KxS, (size_t)3 * g.H * c->PyS);
+  const size_t hn = (size_t)g.H * Ny;
+  if ((e = c->alloc(&c->T0, NN)) || (e = c->alloc(&c->T2, NN)) || (e = c->alloc(&c->T4, NN)) ||
+      (e = c->alloc(&c->Ut, Ny)) || (e = c->alloc(&c->dUt, Ny)) || (e = c->alloc(&c->ddUt, Ny)) ||
+      (e = c->alloc(&c->Uy, g.Py)) || (e = c->alloc(&c->V, hn)) || (e = c->alloc(&c->O, hn)) ||
+      (e = c->alloc(&c->Nvp, hn)) || (e = c->alloc(&c->Nop, hn)) || (e = c->alloc(&c->rv, hn)) ||
+      (e = c->alloc(&c->ro, hn)) || (e = c->alloc(&c->status, 1)) ||
+      (e = c->alloc((unsigned char**)&c->F6, f6 * csz)) ||
+      (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
+      (e = c->alloc(&c->AT, (size_t)g.Kx * g.Kh * 2 * NN)))
+    return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
+  cudaMemcpy(c->T0, T0.data(), NN * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->T2, T2.data(), NN * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->T4, T4.data(), NN * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->Ut, U.data(), Ny * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->dUt, dU.data(), Ny * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->ddUt, ddU.data(), Ny * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->Uy, Uy.data(), g.Py * 8, cudaMemcpyHostToDevice);
+  cudaMemset(c->status, 0, sizeof(int));
+  cudaMemset(c->Nvp, 0, hn * 16);
+  cudaMemset(c->Nop, 0, hn * 16);
+  if ((e = cudaDeviceSynchronize())) return bail(fail(DNS_ERR_CUDA, cudaGetErrorString(e)));
+  *out = c;
+  return DNS_OK;
+}
+
+dns_status dns_destroy(dns_ctx* c) {
+  if (!c) return DNS_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
+  free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
+  void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
+                  c->Nop, c->rv, c->ro, c->AT, c->F6, c->G6, c->scratch, c->status};
+  for (void* q : ptrs) cudaFree(q);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return DNS_OK;
+}
+
+dns_status dns_geometry(const dns_ctx* c, int out[8]) {
+  if (!c || !out) return fail(DNS_ERR_ARG, "null argument");
+  out[0] = c->g.Nx; out[1] = c->g.Ny; out[2] = c->g.Nz; out[3] = c->g.Kx;
+  out[4] = c->g.Px; out[5] = c->g.Py; out[6] = c->g.Pz; out[7] = (int)c->g.H;
+  return DNS_OK;
+}
+
+dns_status dns_get_stream(dns_ctx* c, void** s) {
+  if (!c || !s) return fail(DNS_ERR_ARG, "null argument");
+  *s = (void*)c->st;
+  return DNS_OK;
+}
+
+dns_status dns_synchronize(dns_ctx* c) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->P.device));
+  CK(cudaStreamSynchronize(c->st));
+  return check_status(c);
+}
+
+dns_status dns_memory_bytes(const dns_ctx* c, size_t* b) {
+  if (!c || !b) return fail(DNS_ERR_ARG, "null argument");
+  *b = c->bytes;
+  return DNS_OK;
+}
+
+static dns_status copy_pencils(dns_ctx* c, double2* dev, const void* src, void* dst, size_t pitch,
+                               int where, bool to_dev) {
+  const size_t w = (size_t)c->g.Ny * 16;
+  if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
+  if (to_dev)
+    CK(cudaMemcpy2DAsync(dev, w, src, pitch, w, (size_t)c->g.H, kind_of(where, true), c->st));
+  else
+    CK(cudaMemcpy2DAsync(dst, pitch, dev, w, w, (size_t)c->g.H, kind_of(where, false), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DNS_OK;
+}
+
+dns_status dns_set_state(dns_ctx* c, const void* v, const void* o, size_t pitch, int where) {
+  if (!c || !v || !o) return fail(DNS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = copy_pencils(c, c->V, v, nullptr, pitch, where, true);
+  if (s == DNS_OK) s = copy_pencils(c, c->O, o, nullptr, pitch, where, true);
+  if (s == DNS_OK) { c->have_state = true; c->booted = false; }
+  return s;
+}
+
+dns_status dns_get_state(dns_ctx* c, void* v, void* o, size_t pitch, int where) {
+  if (!c || !v || !o) return fail(DNS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = copy_pencils(c, c->V, nullptr, v, pitch, where, false);
+  if (s == DNS_OK) s = copy_pencils(c, c->O, nullptr, o, pitch, where, false);
+  return s;
+}
+
+dns_status dns_get_history(dns_ctx* c, void* nv, void* no, size_t pitch, int where) {
+  if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = copy_pencils(c, c->Nvp, nullptr, nv, pitch, where, false);
+  if (s == DNS_OK) s = copy_pencils(c, c->Nop, nullptr, no, pitch, where, false);
+  return s;
+}
+
+dns_status dns_set_history(dns_ctx* c, const void* nv, const void* no, size_t pitch, int where) {
+  if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = copy_pencils(c, c->Nvp, nv, nullptr, pitch, where, true);
+  if (s == DNS_OK) s = copy_pencils(c, c->Nop, no, nullptr, pitch, where, true);
+  if (s == DNS_OK) c->booted = true;
+  return s;
+}
+
+dns_status dns_bootstrap(dns_ctx* c) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  if (!c->have_state) return fail(DNS_ERR_STATE, "dns_set_state must precede dns_bootstrap");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = build_inverses(c);
+  if (s != DNS_OK) return s;
+  CK(enqueue(c, 1));
+  s = check_status(c);
+  if (s == DNS_OK) c->booted = true;
+  return s;
+}
+
+dns_status dns_step(dns_ctx* c, int nsteps) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  if (nsteps < 0) return fail(DNS_ERR_ARG, "nsteps < 0");
+  if (!c->have_state || !c->booted)
+    return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = build_inverses(c);
+  if (s != DNS_OK) return s;
+  if (!c->graph) {
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue(c, 0);
+    cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+    if (e) return fail(DNS_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+    CK(e2);
+    CK(cudaGraphInstantiate(&c->graph, gr, 0));
+    cudaGraphDestroy(gr);
+  }
+  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
+  return DNS_OK;
+}
+
+// ---- reference-layout entry points ----------------------------------------
+
+static dns_status check_spec_pitch(dns_ctx* c, size_t tpitch) {
+  if (tpitch % 16 || tpitch < (size_t)c->P.mz * 16)
+    return fail(DNS_ERR_ARG, "tpitch must be a multiple of 16 and hold mz complex values");
+  return DNS_OK;
+}
+static dns_status check_phys_pitch(dns_ctx* c, size_t pitch) {
+  if (pitch % 16 || pitch < (size_t)(c->g.Px / 2 + 1) * 16)
+    return fail(DNS_ERR_ARG, "pitch must be a multiple of 16 and hold mx/2+1 complex values");
+  return DNS_OK;
+}
+
+dns_status dns_transform_3d_one(dns_ctx* c, int dir, void* phys, size_t pitch, void* spec,
+                                size_t tpitch, int pad) {
+  if (!c || !phys || !spec) return fail(DNS_ERR_ARG, "null argument");
+  if ((dir != DNS_FORWARD && dir != DNS_BACKWARD) || (pad != DNS_PADDING && pad != DNS_NO_PADDING))
+    return fail(DNS_ERR_ARG, "bad direction or padding mode");
+  dns_status s;
+  if ((s = check_spec_pitch(c, tpitch)) || (s = check_phys_pitch(c, pitch))) return s;
+  if ((s = need_scratch(c))) return s;
+  CK(cudaSetDevice(c->P.device));
+  const DnsGeom& g = c->g;
+  PencilArr sp{spec, (long long)(tpitch / 16), 0};
+  RowArr sr{c->scratch, c->RS, 0};
+  const long long nrows = (long long)g.Py * g.Pz;
+  const long long rps = (long long)(pitch / 8);
+  if (dir == DNS_BACKWARD) {
+    if (pad == DNS_PADDING) CK(launch_cheby_inplace<double2>(sp, g.H, 0, g.Ny, c->fyP_d.tab(), c->st));
+    else CK(launch_cheby_inplace<double2>(sp, g.H, 1, g.Ny, c->fy0_d.tab(), c->st));
+    CK(launch_zb<double2>(sp, sr, 1, g, c->fz_d.tab(), c->st));
+    CK(launch_x_c2r<double2>(sr, (double*)phys, rps, nrows, g, c->fx_d.tab(), c->st));
+  } else {
+    CK(launch_x_r2c<double2>((const double*)phys, rps, sr, nrows, g, c->fx_d.tab(),
+                             1.0 / g.Px / g.Pz, c->st));
+    CK(launch_zf<double2>(sr, sp, 1, g, c->fz_d.tab(), c->st));
+    if (pad == DNS_PADDING) CK(launch_cheby_inplace<double2>(sp, g.H, 2, g.Ny, c->fyP_d.tab(), c->st));
+    else CK(launch_cheby_inplace<double2>(sp, g.H, 3, g.Ny, c->fy0_d.tab(), c->st));
+  }
+  return DNS_OK;
+}
+
+dns_status dns_transform(dns_ctx* c, int dir, int nf, void* const* phys, size_t pitch,
+                         void* const* spec, size_t tpitch) {
+  if (!c || !phys || !spec || nf < 1 || nf > 6) return fail(DNS_ERR_ARG, "bad arguments");
+  for (int i = 0; i < nf; ++i) {
+    dns_status s = dns_transform_3d_one(c, dir, phys[i], pitch, spec[i], tpitch, DNS_PADDING);
+    if (s) return s;
+  }
+  return DNS_OK;
+}
+
+dns_status dns_cuda_transpose(dns_ctx* c, int dir, void* xyz, size_t pitch, void* zxy, size_t tpitch) {
+  if (!c || !xyz || !zxy) return fail(DNS_ERR_ARG, "null argument");
+  if (dir != DNS_FORWARD && dir != DNS_BACKWARD) return fail(DNS_ERR_ARG, "bad direction");
+  if (pitch % 16 || tpitch % 16 || tpitch < (size_t)c->g.Py * 16 || pitch < (size_t)c->g.Kx * 16)
+    return fail(DNS_ERR_ARG, "bad pitch");
+  CK(cudaSetDevice(c->P.device));
+  CK(launch_transpose_ref(dir == DNS_FORWARD ? 0 : 1, (double2*)xyz, (long long)(pitch / 16),
+                          (double2*)zxy, (long long)(tpitch / 16), c->g, c->st));
+  return DNS_OK;
+}
+
+static dns_status cheby_call(dns_ctx* c, void* zxy, size_t tpitch, int pad, bool s2p) {
+  if (!c || !zxy) return fail(DNS_ERR_ARG, "null argument");
+  if (pad != DNS_PADDING && pad != DNS_NO_PADDING) return fail(DNS_ERR_ARG, "bad padding mode");
+  dns_status s = check_spec_pitch(c, tpitch);
+  if (s) return s;
+  CK(cudaSetDevice(c->P.device));
+  PencilArr sp{zxy, (long long)(tpitch / 16), 0};
+  const int mode = (s2p ? 0 : 2) + (pad == DNS_PADDING ? 0 : 1);
+  const DevFft<double2>& t = (pad == DNS_PADDING) ? c->fyP_d : c->fy0_d;
+  CK(launch_cheby_inplace<double2>(sp, c->g.H, mode, c->g.Ny, t.tab(), c->st));
+  return DNS_OK;
+}
+dns_status dns_cheby_s2p(dns_ctx* c, void* zxy, size_t tpitch, int pad) { return cheby_call(c, zxy, tpitch, pad, true); }
+dns_status dns_cheby_p2s(dns_ctx* c, void* zxy, size_t tpitch, int pad) { return cheby_call(c, zxy, tpitch, pad, false); }
+
+dns_status dns_get_uvw(dns_ctx* c, void* const f[6], size_t tpitch) {
+  if (!c || !f) return fail(DNS_ERR_ARG, "null argument");
+  for (int i = 0; i < 6; ++i) if (!f[i]) return fail(DNS_ERR_ARG, "null field");
+  if (tpitch % 16 || tpitch < (size_t)c->g.Ny * 16) return fail(DNS_ERR_ARG, "bad tpitch");
+  CK(cudaSetDevice(c->P.device));
+  double2* ff[6];
+  for (int i = 0; i < 6; ++i) ff[i] = (double2*)f[i];
+  CK(launch_get_uvw(ff, (long long)(tpitch / 16), c->g, c->ph, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_compute_lamb(dns_ctx* c, void* const in[6], void* const out[3], size_t pitch) {
+  if (!c || !in || !out) return fail(DNS_ERR_ARG, "null argument");
+  for (int i = 0; i < 6; ++i) if (!in[i]) return fail(DNS_ERR_ARG, "null field");
+  for (int i = 0; i < 3; ++i) if (!out[i]) return fail(DNS_ERR_ARG, "null field");
+  if (pitch % 8 || pitch < (size_t)c->g.Px * 8) return fail(DNS_ERR_ARG, "bad pitch");
+  CK(cudaSetDevice(c->P.device));
+  const double* i6[6];
+  double* o3[3];
+  for (int i = 0; i < 6; ++i) i6[i] = (const double*)in[i];
+  for (int i = 0; i < 3; ++i) o3[i] = (double*)out[i];
+  CK(launch_lamb_rows(i6, o3, (long long)(pitch / 8), (long long)c->g.Py * c->g.Pz, c->g, c->Uy,
+                      c->ph.Ro, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_rhs_nonlinear(dns_ctx* c, void* lx, void* ly, const void* lz, size_t tpitch) {
+  if (!c || !lx || !ly || !lz) return fail(DNS_ERR_ARG, "null argument");
+  if (tpitch % 16 || tpitch < (size_t)c->g.Ny * 16) return fail(DNS_ERR_ARG, "bad tpitch");
+  CK(cudaSetDevice(c->P.device));
+  CK(launch_rhs_nonlinear((double2*)lx, (double2*)ly, (const double2*)lz, (long long)(tpitch / 16),
+                          c->g, c->ph, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_solve_eq(dns_ctx* c, const void* inv, void* rhs, int N, size_t tpitch) {
+  if (!c || !inv || !rhs) return fail(DNS_ERR_ARG, "null argument");
+  if (N < 1 || N > 4096 || tpitch % 16 || tpitch < (size_t)N * 16) return fail(DNS_ERR_ARG, "bad N or tpitch");
+  CK(cudaSetDevice(c->P.device));
+  CK(launch_solve_eq((const double2*)inv, (double2*)rhs, (long long)(tpitch / 16), N, c->g.H, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_init_aux_matrix(dns_ctx* c, void* inv_v, void* inv_o, int where) {
+  if (!c || !inv_v || !inv_o) return fail(DNS_ERR_ARG, "null argument");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
+  CK(cudaSetDevice(c->P.device));
+  const long long NN = (long long)c->g.Ny * c->g.Ny;
+  if (where == DNS_DEVICE) {
+    CK(launch_gj_invert(1, 0, c->g.H, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt, nullptr,
+                        (double2*)inv_v, (double2*)inv_o, c->status, c->st));
+    return check_status(c);
+  }
+  // host destination: invert in batches through a device staging buffer
+  const long long batch = std::max(1LL, std::min<long long>(c->g.H, (1LL << 30) / (NN * 32)));
+  double2 *dv = nullptr, *dO = nullptr;
+  CK(cudaMalloc(&dv, (size_t)batch * NN * 16));
+  if (cudaMalloc(&dO, (size_t)batch * NN * 16)) { cudaFree(dv); return fail(DNS_ERR_CUDA, "staging"); }
+  dns_status s = DNS_OK;
+  for (long long u0 = 0; u0 < c->g.H && s == DNS_OK; u0 += batch) {
+    const long long nu = std::min(batch, c->g.H - u0);
+    cudaError_t e = launch_gj_invert(1, u0, nu, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt,
+                                     nullptr, dv, dO, c->status, c->st);
+    if (!e) e = cudaMemcpyAsync((double2*)inv_v + u0 * NN, dv, (size_t)nu * NN * 16, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaMemcpyAsync((double2*)inv_o + u0 * NN, dO, (size_t)nu * NN * 16, cudaMemcpyDeviceToHost, c->st);
+    if (e) s = fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+    else s = check_status(c);
+  }
+  cudaFree(dv);
+  cudaFree(dO);
+  return s;
+}
+
+}  // extern "C"

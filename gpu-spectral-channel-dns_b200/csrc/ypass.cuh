@@ -1,0 +1,24 @@
+// Launchers of the wall-normal pass kernels (ypass.cu).
+#pragma once
+#include "kernels.cuh"
+
+template <typename C>
+cudaError_t launch_cheby_inplace(PencilArr arr, long long npencils, int mode, int Ny,
+                                 FftTab<C> tab, cudaStream_t st);
+cudaError_t launch_get_uvw(double2* const f[6], long long ps, DnsGeom g, PhysParams ph,
+                           cudaStream_t st);
+cudaError_t launch_rhs_nonlinear(double2* lx, double2* ly, const double2* lz, long long ps,
+                                 DnsGeom g, PhysParams ph, cudaStream_t st);
+cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int N,
+                            long long npencils, cudaStream_t st);
+template <typename C>
+cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
+                      PhysParams ph, FftTab<C> tab, cudaStream_t st);
+template <typename C>
+cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
+                      double2* Nop, double2* rv, double2* ro, const double* Ut,
+                      const double* ddUt, DnsGeom g, PhysParams ph, FftTab<C> tabP,
+                      FftTab<double2> tab0, int boot, cudaStream_t st);
+cudaError_t launch_y2(const double2* AT, double2* V, double2* O, const double2* rv,
+                      const double2* ro, const double* dUt, DnsGeom g, PhysParams ph,
+                      FftTab<double2> tab0, int* status, cudaStream_t st);

@@ -1,0 +1,371 @@
+// Spanwise (z) and streamwise (x) pass kernels.
+//
+// Reference counterparts:
+//   transpose_forward / transpose_backward ... source/transpose.cu:223-257, 358-382
+//   setZerosKernel ........................... source/transform.cu:355-377
+//   2D cuFFT Z2D / D2Z + normalizeKernel ..... source/transform.cu:176, 240, 388-412
+//   computeLambVectorKernel / computeLambDevice source/nonlinear.cu:366-428
+//
+// Spanwise pass: a CTA owns a tile of TX streamwise modes x TY wall-normal
+// points and transforms those TX*TY lines along the span in shared memory.
+// It reads one layout (pencil-major, wall-normal index contiguous) and
+// writes the other (row-major, streamwise index contiguous) with TX- or
+// TY-element contiguous runs, so the x-y-z transpose, the span remap
+// ky' = ky or ky + Pz - Nz, the zero padding Nz -> Pz (and truncation), and
+// the zeroing of both Nyquist modes are folded into the one pass.
+//
+// Streamwise pass: two real rows share one complex FFT (a + i b).
+#include "kernels.cuh"
+#include "zxpass.cuh"
+
+namespace {
+template <typename C>
+__device__ __forceinline__ C* prow(const RowArr& a, int f, long long row) {
+  return (C*)a.base + (long long)f * a.fs + row * a.rs;
+}
+template <typename C>
+__device__ __forceinline__ C* ppen(const PencilArr& a, int f, long long p) {
+  return (C*)a.base + (long long)f * a.fs + p * a.ps;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// spanwise backward: pencils [f][kz*Kx+kx][y] -> rows [f][y][zp][kx]
+// ---------------------------------------------------------------------------
+template <typename C, int TX, int TY>
+__global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* lines = (C*)smem_raw;
+  const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  const int NL = TX * TY;
+  const int hz = Nz / 2;
+  // zero band [Nz/2, Pz - Nz/2] (Nyquist and padding)
+  const int nzero = Pz - Nz + 1;
+  for (int t = threadIdx.x; t < NL * nzero; t += blockDim.x) {
+    const int li = t / nzero;
+    const int n = hz + (t - li * nzero);
+    lines[(size_t)li * Pz + tab.drev[n]] = cmk<C>(0.0, 0.0);
+  }
+  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
+    const int yl = t % TY;
+    const int kxl = (t / TY) % TX;
+    const int kz = t / NL;
+    if (kz == hz) continue;
+    const int n = (kz < hz) ? kz : kz + (Pz - Nz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    C v = cmk<C>(0.0, 0.0);
+    if (kx < Kx - 1 && y < Py) v = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
+    lines[(size_t)(kxl * TY + yl) * Pz + tab.drev[n]] = v;
+  }
+  fft_batch<C, true>(lines, NL, Pz, tab.plan, tab.tw);
+  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
+    const int kxl = t % TX;
+    const int zp = (t / TX) % Pz;
+    const int yl = t / (TX * Pz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    if (kx < Kx && y < Py)
+      prow<C>(out, f, (long long)y * Pz + zp)[kx] = lines[(size_t)(kxl * TY + yl) * Pz + zp];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// spanwise forward: rows [f][y][zp][kx] -> pencils [f][kz*Kx+kx][y]
+// ---------------------------------------------------------------------------
+template <typename C, int TX, int TY>
+__global__ void k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* lines = (C*)smem_raw;
+  const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  const int NL = TX * TY;
+  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
+    const int kxl = t % TX;
+    const int zp = (t / TX) % Pz;
+    const int yl = t / (TX * Pz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    C v = cmk<C>(0.0, 0.0);
+    if (kx < Kx && y < Py) v = prow<C>(in, f, (long long)y * Pz + zp)[kx];
+    lines[(size_t)(kxl * TY + yl) * Pz + tab.drev[zp]] = v;
+  }
+  fft_batch<C, false>(lines, NL, Pz, tab.plan, tab.tw);
+  const int hz = Nz / 2;
+  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
+    const int yl = t % TY;
+    const int kxl = (t / TY) % TX;
+    const int kz = t / NL;
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
+    if (kx < Kx && y < Py)
+      ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * Pz + n];
+  }
+}
+
+namespace {
+// Hermitian half-spectra a, b (bins 0..Kx-1, Nyquist and padding zero) packed
+// as Z = A + iB over the full length Px, so that IFFT(Z) = a(x) + i b(x).
+// The imaginary parts of the DC bins are dropped (C2R convention).
+template <typename C>
+__device__ __forceinline__ C pack_c2r(const C* a, const C* b, int n, int Px, int hx) {
+  if (n == 0) return cmk<C>((double)a[0].x, (double)b[0].x);
+  if (n < hx) {
+    const C av = a[n], bv = b[n];
+    C z; z.x = av.x - bv.y; z.y = av.y + bv.x; return z;
+  }
+  if (n > Px - hx) {
+    const int k = Px - n;
+    const C av = a[k], bv = b[k];
+    C z; z.x = av.x + bv.y; z.y = bv.x - av.y; return z;  // conj(a) + i conj(b)
+  }
+  return cmk<C>(0.0, 0.0);
+}
+// unpack the spectra of the real and imaginary parts of a complex signal
+template <typename C>
+__device__ __forceinline__ C unpack_r2c(const C* Z, int k, int Px, bool imag_part) {
+  const C zk = Z[k];
+  const C zm = Z[(Px - k) % Px];
+  C r;
+  if (!imag_part) { r.x = (zk.x + zm.x); r.y = (zk.y - zm.y); }   // Zk + conj(Zm)
+  else { r.x = (zk.y + zm.y); r.y = (zm.x - zk.x); }              // -i (Zk - conj(Zm))
+  return r;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// fused streamwise pass: 6 half-spectra rows -> physical -> Lamb vector with
+// the rotation term -> 3 half-spectra rows, x 1/(Px Pz).
+// Input fields u, v(span), w(wall), omega_x, omega_y, omega_z; output
+// lambda_x, lambda_y(span), lambda_z(wall).  RB rows per CTA (even, rows of
+// one wall-normal plane).
+// ---------------------------------------------------------------------------
+template <typename C>
+__global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+                          const double* __restrict__ Uy, double Ro, int RB) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  typedef decltype(C().x) T;
+  const int Px = g.Px;
+  const int hx = g.Nx / 2;
+  C* zin = (C*)smem_raw;               // 3*RB lines
+  C* zout = zin + (size_t)3 * RB * Px; // RB lines (lx + i ly) then RB/2 (lz pairs)
+  const long long r0 = (long long)blockIdx.x * RB;
+  const long long nrows = (long long)g.Py * g.Pz;
+  for (int t = threadIdx.x; t < RB * 3 * Px; t += blockDim.x) {
+    const int rl = t / (3 * Px);
+    const int rem = t - rl * 3 * Px;
+    const int q = rem / Px;
+    const int n = rem - q * Px;
+    const long long row = r0 + rl;
+    C z = cmk<C>(0.0, 0.0);
+    if (row < nrows) {
+      const C* a = prow<C>(in, 2 * q, row);
+      const C* b = prow<C>(in, 2 * q + 1, row);
+      z = pack_c2r<C>(a, b, n, Px, hx);
+    }
+    zin[(size_t)(rl * 3 + q) * Px + tab.drev[n]] = z;
+  }
+  fft_batch<C, true>(zin, 3 * RB, Px, tab.plan, tab.tw);
+  const T ro = (T)Ro;
+  for (int t = threadIdx.x; t < RB * Px; t += blockDim.x) {
+    const int rl = t / Px;
+    const int j = t - rl * Px;
+    const long long row = r0 + rl;
+    const int y = (int)(row / g.Pz);
+    const T Ub = (row < nrows) ? (T)Uy[y] : (T)0;
+    const C z0 = zin[(size_t)(rl * 3 + 0) * Px + j];
+    const C z1 = zin[(size_t)(rl * 3 + 1) * Px + j];
+    const C z2 = zin[(size_t)(rl * 3 + 2) * Px + j];
+    const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
+    const T lx = oz * v - oy * w - ro * w;
+    const T ly = ox * w - oz * u;
+    const T lz = oy * u - ox * v + ro * (u + Ub);
+    const int pos = tab.drev[j];
+    C A; A.x = lx; A.y = ly;
+    zout[(size_t)rl * Px + pos] = A;
+    T* B = (T*)(zout + (size_t)(RB + rl / 2) * Px + pos);
+    B[rl & 1] = lz;
+  }
+  fft_batch<C, false>(zout, RB + RB / 2, Px, tab.plan, tab.tw);
+  const int Kx = g.Kx;
+  const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
+  for (int t = threadIdx.x; t < RB * 3 * Kx; t += blockDim.x) {
+    const int k = t % Kx;
+    const int fl = (t / Kx) % 3;
+    const int rl = t / (3 * Kx);
+    const long long row = r0 + rl;
+    if (row >= nrows) continue;
+    C v;
+    if (fl < 2) v = unpack_r2c<C>(zout + (size_t)rl * Px, k, Px, fl == 1);
+    else v = unpack_r2c<C>(zout + (size_t)(RB + rl / 2) * Px, k, Px, (rl & 1) != 0);
+    prow<C>(out, fl, row)[k] = v * sc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// standalone streamwise C2R / R2C (drop-in transform_3d_one pieces)
+// complex rows in [row][kx] (pitch rs) <-> real rows [row][x] (pitch rps)
+// ---------------------------------------------------------------------------
+template <typename C>
+__global__ void k_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
+                        FftTab<C> tab, int RB) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* z = (C*)smem_raw;  // RB/2 lines
+  const int Px = g.Px;
+  const int hx = g.Nx / 2;
+  const long long r0 = (long long)blockIdx.x * RB;
+  const int NP = RB / 2;
+  for (int t = threadIdx.x; t < NP * Px; t += blockDim.x) {
+    const int q = t / Px;
+    const int n = t - q * Px;
+    const long long ra = r0 + 2 * q, rb = ra + 1;
+    C v = cmk<C>(0.0, 0.0);
+    if (ra < nrows) {
+      const C* a = prow<C>(in, 0, ra);
+      const C* b = (rb < nrows) ? prow<C>(in, 0, rb) : a;
+      v = pack_c2r<C>(a, b, n, Px, hx);
+      if (rb >= nrows) v.y = 0;
+    }
+    z[(size_t)q * Px + tab.drev[n]] = v;
+  }
+  fft_batch<C, true>(z, NP, Px, tab.plan, tab.tw);
+  for (int t = threadIdx.x; t < RB * Px; t += blockDim.x) {
+    const int rl = t / Px;
+    const int j = t - rl * Px;
+    const long long row = r0 + rl;
+    if (row >= nrows) continue;
+    const C v = z[(size_t)(rl / 2) * Px + j];
+    outr[row * rps + j] = (rl & 1) ? v.y : v.x;
+  }
+}
+
+template <typename C>
+__global__ void k_x_r2c(const T_of<C>* inr, long long rps, RowArr out, long long nrows,
+                        DnsGeom g, FftTab<C> tab, int RB, double scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  typedef T_of<C> T;
+  C* z = (C*)smem_raw;
+  const int Px = g.Px;
+  const long long r0 = (long long)blockIdx.x * RB;
+  const int NP = RB / 2;
+  for (int t = threadIdx.x; t < NP * Px; t += blockDim.x) {
+    const int q = t / Px;
+    const int j = t - q * Px;
+    const long long ra = r0 + 2 * q, rb = ra + 1;
+    C v = cmk<C>(0.0, 0.0);
+    if (ra < nrows) v.x = inr[ra * rps + j];
+    if (rb < nrows) v.y = inr[rb * rps + j];
+    z[(size_t)q * Px + tab.drev[j]] = v;
+  }
+  fft_batch<C, false>(z, NP, Px, tab.plan, tab.tw);
+  const int nk = Px / 2 + 1;  // the reference keeps all mx/2+1 bins
+  const T sc = (T)(0.5 * scale);
+  for (int t = threadIdx.x; t < RB * nk; t += blockDim.x) {
+    const int rl = t / nk;
+    const int k = t - rl * nk;
+    const long long row = r0 + rl;
+    if (row >= nrows) continue;
+    const C v = unpack_r2c<C>(z + (size_t)(rl / 2) * Px, k, Px, (rl & 1) != 0);
+    prow<C>(out, 0, row)[k] = v * sc;
+  }
+}
+
+// pointwise Lamb vector on physical rows (drop-in computeLambVector):
+// lambda may alias (u, v, w) as in the reference.
+__global__ void k_lamb_rows(const double* u, const double* v, const double* w,
+                            const double* ox, const double* oy, const double* oz,
+                            double* lx, double* ly, double* lz, long long rps, int Px,
+                            int Pz, long long nrows, const double* __restrict__ Uy, double Ro) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long row = idx / Px;
+  const int j = (int)(idx - row * Px);
+  if (row >= nrows) return;
+  const long long o = row * rps + j;
+  const double U = Uy[row / Pz];
+  const double uu = u[o], vv = v[o], ww = w[o], a = ox[o], b = oy[o], c = oz[o];
+  lx[o] = c * vv - b * ww - Ro * ww;
+  ly[o] = a * ww - c * uu;
+  lz[o] = b * uu - a * vv + Ro * (uu + U);
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <typename C> struct ZTile;
+template <> struct ZTile<double2> { enum { TX = 4, TY = 4 }; };
+template <> struct ZTile<float2> { enum { TX = 8, TY = 4 }; };
+
+template <typename C>
+cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
+  const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
+  const size_t sm = (size_t)TX * TY * g.Pz * sizeof(C);
+  cudaFuncSetAttribute(k_zb<C, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
+  k_zb<C, TX, TY><<<grid, 256, sm, st>>>(in, out, g, tab);
+  return cudaGetLastError();
+}
+template <typename C>
+cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
+  const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
+  const size_t sm = (size_t)TX * TY * g.Pz * sizeof(C);
+  cudaFuncSetAttribute(k_zf<C, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
+  k_zf<C, TX, TY><<<grid, 256, sm, st>>>(in, out, g, tab);
+  return cudaGetLastError();
+}
+template <typename C>
+cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
+                           double Ro, cudaStream_t st) {
+  const int RB = 2;
+  const size_t sm = (size_t)(3 * RB + RB + RB / 2) * g.Px * sizeof(C);
+  cudaFuncSetAttribute(k_x_fused<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const long long nrows = (long long)g.Py * g.Pz;
+  k_x_fused<C><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(in, out, g, tab, Uy, Ro, RB);
+  return cudaGetLastError();
+}
+template <typename C>
+cudaError_t launch_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
+                         FftTab<C> tab, cudaStream_t st) {
+  const int RB = 4;
+  const size_t sm = (size_t)(RB / 2) * g.Px * sizeof(C);
+  cudaFuncSetAttribute(k_x_c2r<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_x_c2r<C><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(in, outr, rps, nrows, g, tab, RB);
+  return cudaGetLastError();
+}
+template <typename C>
+cudaError_t launch_x_r2c(const T_of<C>* inr, long long rps, RowArr out, long long nrows,
+                         DnsGeom g, FftTab<C> tab, double scale, cudaStream_t st) {
+  const int RB = 4;
+  const size_t sm = (size_t)(RB / 2) * g.Px * sizeof(C);
+  cudaFuncSetAttribute(k_x_r2c<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_x_r2c<C><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(inr, rps, out, nrows, g, tab, RB, scale);
+  return cudaGetLastError();
+}
+cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], long long rps,
+                             long long nrows, DnsGeom g, const double* Uy, double Ro,
+                             cudaStream_t st) {
+  const long long n = nrows * g.Px;
+  const int th = 256;
+  k_lamb_rows<<<(unsigned)((n + th - 1) / th), th, 0, st>>>(
+      in6[0], in6[1], in6[2], in6[3], in6[4], in6[5], out3[0], out3[1], out3[2], rps, g.Px, g.Pz,
+      nrows, Uy, Ro);
+  return cudaGetLastError();
+}
+
+#define INST_Z(C)                                                                                  \
+  template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
+  template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
+  template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
+                                         double, cudaStream_t);                                   \
+  template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \
+                                       FftTab<C>, cudaStream_t);                                  \
+  template cudaError_t launch_x_r2c<C>(const T_of<C>*, long long, RowArr, long long, DnsGeom,     \
+                                       FftTab<C>, double, cudaStream_t);
+INST_Z(double2)
+INST_Z(float2)

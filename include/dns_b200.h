@@ -1,0 +1,166 @@
+/*
+ * dns_b200.h -- C ABI of libdnsb200.so, a B200 (sm_100a) implementation of
+ * the v-omega Fourier-Chebyshev DNS time step of Riveryh/gpu-spectral-
+ * channel-DNS (rotating plane Couette / channel flow; AB2 nonlinear, CN
+ * linear, 3/2-padded dealiasing, Chebyshev collocation walls).
+ *
+ * Plain pointers and sizes only.  Every call returns a dns_status; on error
+ * dns_last_error() gives a message (per thread).  Device pointers are
+ * CUDA device addresses on the context's device; all work is ordered on
+ * the context's stream (dns_get_stream) and is asynchronous unless stated.
+ *
+ * Layouts follow the reference (include/data.h:189-334):
+ *   spectral "ZXY"  complex double [ky][kx][k], ky < Nz, kx < Kx = Nx/2+1,
+ *                   pencil pitch `tpitch` bytes (reference tPitch);
+ *   physical "XYZ"  double [z][y][x], z < Py = mz/2+1 wall-normal points,
+ *                   y < Pz = my spanwise, x < Px = mx, row pitch `pitch`
+ *                   bytes (reference pitch); the same buffer holds complex
+ *                   rows of mx/2+1 entries before the streamwise transform.
+ * Axis names are the reference's: x streamwise, y spanwise, z wall-normal;
+ * reference "w" is the wall-normal velocity, "omega_z" the wall-normal
+ * vorticity; the solver state is (w, omega_z) = (v, omega_y) in standard
+ * notation, with pencil (0,0) holding the mean u0 / w0 profiles.
+ */
+#ifndef DNS_B200_H
+#define DNS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNS_B200_ABI_VERSION 1
+
+typedef struct dns_ctx dns_ctx;
+
+typedef enum dns_status {
+  DNS_OK = 0,
+  DNS_ERR_ARG = 1,         /* bad argument / unsupported size */
+  DNS_ERR_CUDA = 2,        /* CUDA runtime error */
+  DNS_ERR_STATE = 3,       /* call out of order (e.g. step before state) */
+  DNS_ERR_TIMEOUT = 4,     /* a device wait ran past its iteration limit */
+  DNS_ERR_SINGULAR = 5,    /* an operator matrix had a zero pivot */
+  DNS_ERR_IO = 6,          /* file could not be read / parsed */
+  DNS_ERR_NONFINITE = 7    /* state contains NaN or Inf */
+} dns_status;
+
+/* direction and padding enums of the reference
+ * (include/transpose.cuh:9-11, include/transform.cuh:13) */
+enum { DNS_FORWARD = 0, DNS_BACKWARD = 1 };
+enum { DNS_PADDING = 0, DNS_NO_PADDING = 1 };
+/* arithmetic of the transform / nonlinear path */
+enum { DNS_PREC_FP64 = 0, DNS_PREC_MIXED = 1 };
+/* where a host-facing buffer lives */
+enum { DNS_HOST = 0, DNS_DEVICE = 1 };
+
+/* Numerical parameters: the first three records of parameter.txt
+ * (include/parameters.h:4-13, source/operation.cpp:123-127) plus the base
+ * flow U(y) = U0 + U1 y + U2 y^2 (reference: plane Couette (0.5, 0.5, 0),
+ * source/coefficient.cu:149-159) and the precision of the transform path. */
+typedef struct dns_params {
+  int mx, my, mz;          /* padded x, padded span, 4*(Ny-1) */
+  double n_pi_x, n_pi_y;   /* Lx = n_pi_x*pi, Lz = n_pi_y*pi */
+  double Re, Ro, dt;
+  double U0, U1, U2;
+  int precision;           /* DNS_PREC_FP64 or DNS_PREC_MIXED */
+  int device;              /* CUDA device ordinal */
+} dns_params;
+
+/* Step / IO records 4-6 of parameter.txt (include/parameters.h:16-27). */
+typedef struct dns_run_params {
+  int start_type, start_step, end_step, save_internal, save_recovery_internal;
+  char output_file_prefix[512];
+  char recovery_file_prefix[512];
+} dns_run_params;
+
+const char* dns_status_string(dns_status s);
+const char* dns_last_error(void);
+int dns_abi_version(void);
+
+/* Reference defaults (problem::problem(), include/data.h:295-304 and
+ * input/parameter.txt) with the Couette base flow. */
+dns_status dns_params_default(dns_params* p);
+
+/* Replaces RPCF_Paras::read_para (source/operation.cpp:115-138); unlike the
+ * reference, a missing or short file is an error. */
+dns_status dns_read_parameter_file(const char* path, dns_params* p, dns_run_params* rp);
+
+/* Replaces problem(conf) + getDeviceInfo + allocDeviceMem + initFFT +
+ * allocHostMemory (source/data.cpp:3-31, source/RPCFKernels.cu:17-128,
+ * source/transform.cu:18-93, source/solver.cpp:216-257).  The operator
+ * inverses (source/solver.cpp:260-320) are built on the device on the first
+ * dns_bootstrap / dns_step. */
+dns_status dns_create(const dns_params* p, dns_ctx** out);
+dns_status dns_destroy(dns_ctx* ctx);
+
+/* sizes: Nx, Ny, Nz, Kx, Px, Py, Pz, H (= Kx*Nz pencils) */
+dns_status dns_geometry(const dns_ctx* ctx, int out[8]);
+dns_status dns_get_stream(dns_ctx* ctx, void** cuda_stream);
+dns_status dns_synchronize(dns_ctx* ctx);
+/* bytes of device memory held by the context */
+dns_status dns_memory_bytes(const dns_ctx* ctx, size_t* bytes);
+
+/* ---- fused time step (the drop-in for nextStep) ---------------------- */
+
+/* State in the reference's host layout: rhs_v / rhs_omega_y after a solve
+ * (source/solver.cpp:95-96): [Nz][Kx] pencils of `pitch` bytes, Ny complex
+ * doubles used per pencil, pencil (0,0) = u0 / w0.  where = DNS_HOST or
+ * DNS_DEVICE.  Synchronous. */
+dns_status dns_set_state(dns_ctx* ctx, const void* v, const void* omega, size_t pitch, int where);
+dns_status dns_get_state(dns_ctx* ctx, void* v, void* omega, size_t pitch, int where);
+/* The AB2 history: nonlinear terms at the Ny collocation points
+ * (reference nonlinear_v / nonlinear_omega_y after a step). Synchronous. */
+dns_status dns_get_history(dns_ctx* ctx, void* nv, void* nomega, size_t pitch, int where);
+dns_status dns_set_history(dns_ctx* ctx, const void* nv, const void* nomega, size_t pitch, int where);
+
+/* The "extra previous step" of source/main_loop.cpp:39-52: store the
+ * nonlinear term of the current state as the AB2 history, so the first step
+ * is forward Euler in the nonlinear term as in the reference. */
+dns_status dns_bootstrap(dns_ctx* ctx);
+
+/* nsteps x nextStep (source/solver.cpp:35-101): getUVW, transforms, Lamb
+ * vector, rhsNonlinear, CN/AB2 right-hand sides, v solve, omega right-hand
+ * side with the tilting term, omega solve -- one CUDA graph per step, no
+ * host round trip. */
+dns_status dns_step(dns_ctx* ctx, int nsteps);
+
+/* ---- reference-layout entry points (device pointers) ----------------- */
+
+/* transform_3d_one (source/transform.cu:95-319): dir = DNS_BACKWARD maps
+ * the spectral pencils (nz coefficients) to the physical field (the pencils
+ * are overwritten, as in the reference); DNS_FORWARD maps the physical
+ * field to pz coefficients per pencil.  pad = DNS_PADDING uses the pz
+ * wall-normal points, DNS_NO_PADDING the nz points. */
+dns_status dns_transform_3d_one(dns_ctx* ctx, int dir, void* phys, size_t pitch, void* spec,
+                                size_t tpitch, int pad);
+/* transform (source/transform.cu:321-351): BACKWARD on six fields
+ * (u, v, w, omega_x, omega_y, omega_z), FORWARD on three (lamb_z, lamb_y,
+ * lamb_x order of the reference is immaterial). */
+dns_status dns_transform(dns_ctx* ctx, int dir, int nfields, void* const* phys, size_t pitch,
+                         void* const* spec, size_t tpitch);
+/* cuda_transpose (source/transpose.cu:115-166); xyz is complex. */
+dns_status dns_cuda_transpose(dns_ctx* ctx, int dir, void* xyz, size_t pitch, void* zxy,
+                              size_t tpitch);
+/* cheby_s2p / cheby_p2s (source/transform.cu:538-748), in place. */
+dns_status dns_cheby_s2p(dns_ctx* ctx, void* zxy, size_t tpitch, int pad);
+dns_status dns_cheby_p2s(dns_ctx* ctx, void* zxy, size_t tpitch, int pad);
+/* getUVW (source/velocity.cu:22-170): reads f[2] (w) and f[5] (omega_z),
+ * writes all six. */
+dns_status dns_get_uvw(dns_ctx* ctx, void* const f[6], size_t tpitch);
+/* computeLambVector (source/nonlinear.cu:307-428): out may alias in[0..2]. */
+dns_status dns_compute_lamb(dns_ctx* ctx, void* const in[6], void* const out[3], size_t pitch);
+/* rhsNonlinear (source/nonlinear.cu:130-242). */
+dns_status dns_rhs_nonlinear(dns_ctx* ctx, void* lamb_x, void* lamb_y, const void* lamb_z,
+                             size_t tpitch);
+/* solveEq (source/solver.cpp:107-123): rhs <- inv * rhs for every pencil;
+ * inv row-major [ky][kx][N][N] complex, rhs pitched pencils. */
+dns_status dns_solve_eq(dns_ctx* ctx, const void* inv, void* rhs, int N, size_t tpitch);
+/* initAuxMatrix (source/solver.cpp:260-320): explicit inverses of the v and
+ * omega operators of every pencil, row-major [ky][kx][nz][nz] complex. */
+dns_status dns_init_aux_matrix(dns_ctx* ctx, void* inv_v, void* inv_omega, int where);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DNS_B200_H */
