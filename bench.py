@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""DNS steps/s at 256x129x256 (Nx x Ny x Nz modes; reference parameters
+mx, my, mz = 384, 384, 512; physical grid 384 x 257 x 384), rotating plane
+Couette, Re = 3000, rotation number 0.02, dt = 0.001, seeded divergence-free
+initial field (seed 0, amplitude 0.1).
+
+The headline `value` is the mixed form (FP32 transforms and Lamb vector,
+FP64 operators, solves and AB2/CN state) in steps/s with the state resident
+in HBM; the plain FP64 form is timed in the same run and the mixed form's
+relative L2 error against it is reported (must be <= 1e-6).  `e2e` is the
+mixed step through the public C ABI with the state copied in from pinned host
+memory and back out every step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (launched by torchrun) every rank runs an independent
+replica of the problem (the step does not shard at this size); the time is
+the maximum over ranks and `value` sums the replicas' steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "gpu-spectral-channel-dns_b200")
+
+METRIC = "DNS steps/s at 256x129x256: mixed vs FP64 form at 1e-6 rel err; % HBM roofline"
+CONFIGS = {
+    # the headline workload (mixed vs FP64)
+    "256x129x256": dict(Nx=256, Ny=129, Nz=256, mx=384, my=384, mz=512, Re=3000.0, Ro=0.02,
+                        dt=0.001, amplitude=0.1, seed=0),
+    # smaller grids of the same family, for profiling captures and parity runs
+    "128x65x128": dict(Nx=128, Ny=65, Nz=128, mx=192, my=192, mz=256, Re=3000.0, Ro=0.02,
+                       dt=0.001, amplitude=0.1, seed=0),
+    "32x33x32": dict(Nx=32, Ny=33, Nz=32, mx=48, my=48, mz=128, Re=1300.0, Ro=0.1, dt=0.005,
+                     amplitude=0.05, seed=0),
+}
+CFG = CONFIGS["256x129x256"]
+KERNELS = ["y3_uvw_s2p", "zb_span_inverse", "x_c2r_lamb_r2c", "zf_span_forward", "y1_p2s_rhs",
+           "y2_solve"]
+
+
+def load_pkg():
+    if "dns_b200" in sys.modules:
+        return sys.modules["dns_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "dns_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dns_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per kernel launch (one step), element size c (16 FP64 /
+# 8 FP32 complex); s = 16 (FP64 state / operator complex)
+# ---------------------------------------------------------------------------
+def kernel_bytes(g, c):
+    Kx, Nz, Ny, Py, Pz = g["Kx"], g["Nz"], g["Ny"], g["Py"], g["Pz"]
+    H = Kx * Nz
+    s = 16
+    slots = Kx * (Nz // 2 + 1)
+    return {
+        "y3_uvw_s2p": s * 2 * H * Ny + c * 6 * H * Py,
+        "zb_span_inverse": c * 6 * H * Py + c * 6 * Kx * Pz * Py,
+        "x_c2r_lamb_r2c": c * 6 * Kx * Pz * Py + c * 3 * Kx * Pz * Py,
+        "zf_span_forward": c * 3 * Kx * Pz * Py + c * 3 * H * Py,
+        # lambda in; v, omega, history in; rhs and history out
+        "y1_p2s_rhs": c * 3 * H * Py + s * 4 * H * Ny + s * 4 * H * Ny,
+        # explicit inverses (v and omega, shared by +-kz), rhs and v^n in, state out
+        "y2_solve": s * 2 * slots * Ny * Ny + s * 3 * H * Ny + s * 2 * H * Ny,
+    }
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit())
+        mx = max((float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for n, v in zip(names, r[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline():
+    """Time the oracle (FP64 NumPy port of the reference step) on the host:
+    the full nonlinear phase at 256x129x256 plus the CN/AB2 right-hand sides
+    and the two solves on a sample of pencils, scaled to all pencils."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from oracle import rpcf_oracle as O
+    pkg = load_pkg()
+    p = O.Params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"], dt=CFG["dt"])
+    pb = O.Problem(p)
+    sz = pb.sz
+    V, Om = pkg.seeded_state(sz.nx, sz.nz, sz.ny, p.n_pi_x, p.n_pi_y, CFG["amplitude"], CFG["seed"])
+    pb.set_state(V, Om)
+    t0 = time.perf_counter()
+    Nv, No = pb.nonlinear()
+    t_nl = time.perf_counter() - t0
+    # linear RHS + solves on S pencils (their inverses built outside the timing)
+    S = 256
+    rng = np.random.default_rng(0)
+    sel = rng.choice(sz.ny * sz.hnx, size=S, replace=False)
+    ky, kx = np.unravel_index(sel, (sz.ny, sz.hnx))
+    N = sz.nz - 1
+    invs = []
+    for a, b in zip(ky, kx):
+        Av = O.coef_v(N, pb.U, pb.ddU, pb.T0, pb.T2, pb.T4, p.Re, p.dt, pb.kmn[a, b], pb.ia[a, b])
+        Ao = O.coef_omega(N, pb.U, pb.T0, pb.T2, p.Re, p.dt, pb.kmn[a, b], pb.ia[a, b])
+        invs.append((np.linalg.inv(Av), np.linalg.inv(Ao)))
+    t0 = time.perf_counter()
+    sub = O.Problem(p)
+    sub.kmn = pb.kmn[ky, kx][None, :]
+    sub.ia = pb.ia[ky, kx][None, :]
+    sub.ib = pb.ib[ky, kx][None, :]
+    Vs = V[ky, kx][None]
+    Os = Om[ky, kx][None]
+    rv = sub.linear_v(Vs)
+    k = np.arange(4, sz.nz)
+    rv[..., 4:] += (Nv[ky, kx][None][..., k - 2] * 1.5 - Nv[ky, kx][None][..., k - 2] * 0.5) * p.dt
+    vn = np.stack([iv @ r for (iv, _), r in zip(invs, rv[0])])[None]
+    ro = sub.linear_omega(Os, vn, Vs)
+    on = np.stack([io @ r for (_, io), r in zip(invs, ro[0])])
+    t_lin = (time.perf_counter() - t0) * (sz.ny * sz.hnx) / S
+    step_s = t_nl + t_lin
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": (f"oracle FP64 NumPy step at 256x129x256: full nonlinear phase ({t_nl:.1f} s) "
+                       f"+ CN/AB2 rhs and solves on {S} of {sz.ny * sz.hnx} pencils scaled "
+                       f"({t_lin:.2f} s); operator inverses excluded as setup"),
+            "step_seconds": step_s}
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    V0, O0 = pkg.seeded_state(CFG["Nx"], CFG["Ny"], CFG["Nz"], 4.0, 2.0, CFG["amplitude"], CFG["seed"])
+
+    def make(prec):
+        ctx = pkg.Context(pkg.make_params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"],
+                                          dt=CFG["dt"], precision=prec, device=dev))
+        ctx.set_state(V0, O0)
+        ctx.bootstrap()
+        return ctx
+
+    def timed(ctx, K, W):
+        ctx.step(W)
+        ctx.synchronize()
+        s = torch.cuda.ExternalStream(ctx.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0.record(s)
+        ctx.step(K)
+        e1.record(s)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / K
+
+    K, W = args.steps, args.warmup
+    t_setup = time.perf_counter()
+    c64 = make(pkg.PREC_FP64)
+    setup_s = time.perf_counter() - t_setup
+    ms64 = timed(c64, K, W)
+    cmx = make(pkg.PREC_MIXED)
+    with ClockSampler(dev) as clk:
+        msmx = timed(cmx, K, W)
+    # accuracy of the mixed form against the FP64 form after W + K steps
+    V64, O64 = c64.get_state()
+    Vmx, Omx = cmx.get_state()
+    err_v = float(np.linalg.norm(Vmx - V64) / np.linalg.norm(V64))
+    err_o = float(np.linalg.norm(Omx - O64) / np.linalg.norm(O64))
+    # per-kernel durations, measured with CUDA events on the launching stream
+    kms64 = c64.step_profiled(K)
+    kmsmx = cmx.step_profiled(K)
+    c64.close()
+    # end to end through the C ABI with pinned host buffers
+    Vh = torch.empty((cmx.Nz, cmx.Kx, cmx.Ny), dtype=torch.complex128, pin_memory=True)
+    Oh = torch.empty_like(Vh, pin_memory=True)
+    Vh.copy_(torch.from_numpy(Vmx))
+    Oh.copy_(torch.from_numpy(Omx))
+    pitch = cmx.Ny * 16
+    vp, op = Vh.data_ptr(), Oh.data_ptr()
+    lib = cmx.lib
+    import ctypes
+    for _ in range(2):
+        lib.dns_set_state(cmx.h, ctypes.c_void_p(vp), ctypes.c_void_p(op), pitch, pkg.HOST)
+        cmx.step(1)
+        lib.dns_get_state(cmx.h, ctypes.c_void_p(vp), ctypes.c_void_p(op), pitch, pkg.HOST)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        st = lib.dns_set_state(cmx.h, ctypes.c_void_p(vp), ctypes.c_void_p(op), pitch, pkg.HOST)
+        cmx.step(1)
+        st |= lib.dns_get_state(cmx.h, ctypes.c_void_p(vp), ctypes.c_void_p(op), pitch, pkg.HOST)
+        if st:
+            raise RuntimeError(lib.dns_last_error().decode())
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / K
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    geo = dict(Kx=cmx.Kx, Nz=cmx.Nz, Ny=cmx.Ny, Py=cmx.Py, Pz=cmx.Pz)
+    mem = cmx.memory_bytes()
+    cmx.close()
+    return dict(ms64=ms64, msmx=msmx, err_v=err_v, err_o=err_o, kms64=kms64, kmsmx=kmsmx,
+                e2e_ms=e2e_ms, geo=geo, clocks=clk.summary(), setup_s=setup_s, mem=mem,
+                state_bytes=2 * geo["Kx"] * geo["Nz"] * geo["Ny"] * 16)
+
+
+def roofline(kms, geo, c, peak):
+    kb = kernel_bytes(geo, c)
+    top = max(kms, key=kms.get)
+    achieved = kb[top] / (kms[top] * 1e-3) / 1e9
+    return top, {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
+                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                 "bytes_per_launch": kb[top], "ms_per_launch": round(kms[top], 4)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default="256x129x256", choices=sorted(CONFIGS))
+    args = ap.parse_args()
+    global CFG
+    CFG = CONFIGS[args.config]
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        from oracle.ref_build import ref_arm  # noqa: WPS433 (test/baseline infrastructure)
+        if rank == 0:
+            print(json.dumps(ref_arm.run(args, CFG, METRIC)))
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    r = run_ours(args, rank, world)
+    peak, peak_kind = measured_peaks()
+    top64, roof64 = roofline(r["kms64"], r["geo"], 16, peak)
+    topmx, roofmx = roofline(r["kmsmx"], r["geo"], 8, peak)
+    step_bytes64 = sum(kernel_bytes(r["geo"], 16).values())
+    step_bytes_mx = sum(kernel_bytes(r["geo"], 8).values())
+    out = None
+    if rank == 0:
+        cpu = None if (args.no_cpu_baseline or world > 1 or args.config != "256x129x256") else cpu_baseline()
+        n = world
+        value = n * 1000.0 / r["msmx"]
+        out = {
+            "metric": METRIC,
+            "value": round(value, 2),
+            "unit": "steps/s",
+            "n_gpus": n,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(r["msmx"], 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 transforms/Lamb + f64 solves/state (mixed)",
+            "data": "synthetic seeded divergence-free field (seed 0, amplitude 0.1)",
+            "config": {"workload": (f"rotating plane Couette {args.config} modes (mx,my,mz="
+                                    f"{CFG['mx']},{CFG['my']},{CFG['mz']}; physical {CFG['mx']}x"
+                                    f"{CFG['mz'] // 2 + 1}x{CFG['my']}), Re {CFG['Re']:g}, "
+                                    f"Ro {CFG['Ro']:g}, dt {CFG['dt']:g}"),
+                       "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
+                       "l2": "per-step working set ~10-16 GB >> 126 MB L2 (no flush needed)"},
+            "fp64": {"steps_per_s": round(n * 1000.0 / r["ms64"], 2), "ms_per_step": round(r["ms64"], 4),
+                     "roofline": roof64, "step_bytes_algorithmic": step_bytes64,
+                     "step_frac_of_peak": round(step_bytes64 / (r["ms64"] * 1e-3) / 1e9 / peak, 4)},
+            "mixed_vs_fp64": {"speedup": round(r["ms64"] / r["msmx"], 3),
+                              "rel_l2_err_v": r["err_v"], "rel_l2_err_omega_y": r["err_o"],
+                              "within_1e-6": bool(r["err_v"] <= 1e-6 and r["err_o"] <= 1e-6),
+                              "after_steps": args.steps + args.warmup},
+            "roofline": dict(roofmx, peak_kind=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"),
+            "step_frac_of_peak": round(step_bytes_mx / (r["msmx"] * 1e-3) / 1e9 / peak, 4),
+            "kernel_ms": {"fp64": {k: round(v, 4) for k, v in r["kms64"].items()},
+                          "mixed": {k: round(v, 4) for k, v in r["kmsmx"].items()}},
+            "e2e": {"value": round(n * 1000.0 / r["e2e_ms"], 2), "unit": "steps/s",
+                    "h2d_bytes_per_step": r["state_bytes"], "d2h_bytes_per_step": r["state_bytes"]},
+            "gpu_launches": 6 * args.steps,
+            "cpu_baseline": cpu,
+            "clocks": r["clocks"],
+            "setup_seconds": round(r["setup_s"], 2),
+            "device_bytes": r["mem"],
+        }
+        print(json.dumps(out))
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -23,7 +23,8 @@ EXPORTS = [
     "dns_status_string", "dns_last_error", "dns_abi_version", "dns_params_default",
     "dns_read_parameter_file", "dns_create", "dns_destroy", "dns_geometry", "dns_get_stream",
     "dns_synchronize", "dns_memory_bytes", "dns_set_state", "dns_get_state",
-    "dns_get_history", "dns_set_history", "dns_bootstrap", "dns_step",
+    "dns_get_history", "dns_set_history", "dns_bootstrap", "dns_step", "dns_step_profiled",
+    "dns_kernel_name",
     "dns_transform_3d_one", "dns_transform", "dns_cuda_transpose", "dns_cheby_s2p",
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix",
@@ -74,6 +75,8 @@ def load_library(path: str | None = None):
     lib.dns_last_error.restype = C.c_char_p
     lib.dns_last_error.argtypes = []
     lib.dns_abi_version.restype = i
+    lib.dns_kernel_name.restype = C.c_char_p
+    lib.dns_kernel_name.argtypes = [i]
     sigs = {
         "dns_params_default": [C.POINTER(DnsParams)],
         "dns_read_parameter_file": [C.c_char_p, C.POINTER(DnsParams), C.POINTER(DnsRunParams)],
@@ -89,6 +92,7 @@ def load_library(path: str | None = None):
         "dns_set_history": [vp, vp, vp, sz, i],
         "dns_bootstrap": [vp],
         "dns_step": [vp, i],
+        "dns_step_profiled": [vp, i, C.POINTER(C.c_double)],
         "dns_transform_3d_one": [vp, i, vp, sz, vp, sz, i],
         "dns_transform": [vp, i, i, C.POINTER(vp), sz, C.POINTER(vp), sz],
         "dns_cuda_transpose": [vp, i, vp, sz, vp, sz],
@@ -227,6 +231,12 @@ class Context:
 
     def step(self, n=1):
         self._call("dns_step", int(n))
+
+    def step_profiled(self, n=1):
+        """Run n un-graphed steps; returns {kernel name: mean ms per launch}."""
+        ms = (C.c_double * 6)()
+        self._call("dns_step_profiled", int(n), ms)
+        return {self.lib.dns_kernel_name(k).decode(): ms[k] for k in range(6)}
 
     # -- reference-layout entry points (device pointers as ints) -----------
     def transform_3d_one(self, direction, phys, pitch, spec, tpitch, pad=PADDING):

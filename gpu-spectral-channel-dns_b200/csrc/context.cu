@@ -135,9 +135,12 @@ dns_status build_inverses(dns_ctx* c) {
   return DNS_OK;
 }
 
+// Enqueue one step (boot = 0) or the history bootstrap (boot = 1).  With
+// `ev` (7 events) an event is recorded before the first and after every
+// kernel, for per-kernel timing on the launching stream.
 template <typename C>
 cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const DevFft<C>& fx,
-                             const DevFft<C>& fyP) {
+                             const DevFft<C>& fyP, cudaEvent_t* ev) {
   const DnsGeom& g = c->g;
   const long long H = g.H;
   PencilArr F6p{c->F6, c->PyS, H * c->PyS};
@@ -145,23 +148,33 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   RowArr G3r{c->F6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
   PencilArr F3p{c->G6, c->PyS, H * c->PyS};
   cudaError_t e;
+  int k = 0;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
+  mark();
   if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->st))) return e;
+  mark();
   if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st))) return e;
+  mark();
   if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->st))) return e;
+  mark();
   if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
+  mark();
   if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, c->Ut, c->ddUt, g, c->ph,
                         fyP.tab(), c->fy0_d.tab(), boot, c->st)))
     return e;
+  mark();
   if (!boot)
     if ((e = launch_y2(c->AT, c->V, c->O, c->rv, c->ro, c->dUt, g, c->ph, c->fy0_d.tab(),
                        c->status, c->st)))
       return e;
+  mark();
   return cudaSuccess;
 }
 
-cudaError_t enqueue(dns_ctx* c, int boot) {
-  if (c->P.precision == DNS_PREC_MIXED) return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f);
-  return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d);
+cudaError_t enqueue(dns_ctx* c, int boot, cudaEvent_t* ev = nullptr) {
+  if (c->P.precision == DNS_PREC_MIXED)
+    return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f, ev);
+  return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d, ev);
 }
 
 dns_status need_scratch(dns_ctx* c) {
@@ -372,7 +385,7 @@ dns_status dns_set_state(dns_ctx* c, const void* v, const void* o, size_t pitch,
   CK(cudaSetDevice(c->P.device));
   dns_status s = copy_pencils(c, c->V, v, nullptr, pitch, where, true);
   if (s == DNS_OK) s = copy_pencils(c, c->O, o, nullptr, pitch, where, true);
-  if (s == DNS_OK) { c->have_state = true; c->booted = false; }
+  if (s == DNS_OK) c->have_state = true;
   return s;
 }
 
@@ -433,6 +446,38 @@ dns_status dns_step(dns_ctx* c, int nsteps) {
   }
   for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
   return DNS_OK;
+}
+
+dns_status dns_step_profiled(dns_ctx* c, int nsteps, double kernel_ms[DNS_NUM_KERNELS]) {
+  if (!c || !kernel_ms) return fail(DNS_ERR_ARG, "null argument");
+  if (nsteps < 1) return fail(DNS_ERR_ARG, "nsteps < 1");
+  if (!c->have_state || !c->booted)
+    return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step_profiled");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = build_inverses(c);
+  if (s != DNS_OK) return s;
+  const int ne = DNS_NUM_KERNELS + 1;
+  std::vector<cudaEvent_t> ev((size_t)ne * nsteps);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  cudaError_t err = cudaSuccess;
+  for (int i = 0; i < nsteps && !err; ++i) err = enqueue(c, 0, &ev[(size_t)i * ne]);
+  if (!err) err = cudaStreamSynchronize(c->st);
+  for (int k = 0; k < DNS_NUM_KERNELS; ++k) kernel_ms[k] = 0.0;
+  for (int i = 0; i < nsteps && !err; ++i)
+    for (int k = 0; k < DNS_NUM_KERNELS; ++k) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[(size_t)i * ne + k], ev[(size_t)i * ne + k + 1]);
+      kernel_ms[k] += ms / nsteps;
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (err) return fail(DNS_ERR_CUDA, cudaGetErrorString(err));
+  return check_status(c);
+}
+
+const char* dns_kernel_name(int k) {
+  static const char* names[DNS_NUM_KERNELS] = {
+      "y3_uvw_s2p", "zb_span_inverse", "x_c2r_lamb_r2c", "zf_span_forward", "y1_p2s_rhs", "y2_solve"};
+  return (k >= 0 && k < DNS_NUM_KERNELS) ? names[k] : "";
 }
 
 // ---- reference-layout entry points ----------------------------------------

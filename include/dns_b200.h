@@ -106,7 +106,8 @@ dns_status dns_memory_bytes(const dns_ctx* ctx, size_t* bytes);
 /* State in the reference's host layout: rhs_v / rhs_omega_y after a solve
  * (source/solver.cpp:95-96): [Nz][Kx] pencils of `pitch` bytes, Ny complex
  * doubles used per pencil, pencil (0,0) = u0 / w0.  where = DNS_HOST or
- * DNS_DEVICE.  Synchronous. */
+ * DNS_DEVICE.  Synchronous.  Setting the state keeps the AB2 history (as a
+ * host-driven step of the reference does); call dns_bootstrap to restart it. */
 dns_status dns_set_state(dns_ctx* ctx, const void* v, const void* omega, size_t pitch, int where);
 dns_status dns_get_state(dns_ctx* ctx, void* v, void* omega, size_t pitch, int where);
 /* The AB2 history: nonlinear terms at the Ny collocation points
@@ -124,6 +125,15 @@ dns_status dns_bootstrap(dns_ctx* ctx);
  * side with the tilting term, omega solve -- one CUDA graph per step, no
  * host round trip. */
 dns_status dns_step(dns_ctx* ctx, int nsteps);
+
+/* The same steps without the graph, with CUDA events recorded around each
+ * of the DNS_NUM_KERNELS kernels of a step on the context stream;
+ * kernel_ms[k] = mean duration of kernel k (dns_kernel_name(k)).
+ * Synchronous.  Replaces the reference's CURPCF_CUDA_PROFILING timers
+ * (include/cuRPCF.h:14-15, source/nonlinear.cu:28-106). */
+#define DNS_NUM_KERNELS 6
+dns_status dns_step_profiled(dns_ctx* ctx, int nsteps, double kernel_ms[DNS_NUM_KERNELS]);
+const char* dns_kernel_name(int k);
 
 /* ---- reference-layout entry points (device pointers) ----------------- */
 
