@@ -1,0 +1,271 @@
+// Compile-time-length shared-memory FFT built from register codelets.
+//
+// L = R_1 * R_2 * ... * R_P with every radix R_p <= 16 (codelets 2, 3, 4, 6,
+// 8, 12, 16).  Pass p is a Stockham autosort step: with Ns = R_1 ... R_{p-1},
+// butterfly j in [0, L/R) reads x[j + r L/R] (r < R), multiplies by
+// W_{Ns R}^{r (j mod Ns)}, takes the R-point DFT in registers and writes
+// y[(j/Ns) Ns R + (j mod Ns) + r Ns].  Every thread reads all its butterfly
+// inputs, the block synchronises, then every thread writes, so one buffer
+// suffices.  Input and output are in natural order.
+//
+// Shared-memory positions go through fpos(i) = i + i/16 (one pad element
+// every 16) so the strided accesses of the early passes spread over banks.
+// Pass twiddles come from the table W_L^j (host long double); codelet
+// constants are the exact values cos, sin (2 pi m / R) for R <= 16.
+#pragma once
+#include "dns_common.cuh"
+
+DNS_HD int fpos(int i) { return i + (i >> 4); }
+DNS_HD int fpad_len(int L) { return L + (L >> 4) + 1; }
+
+template <int... Rs> struct Radices {};
+
+template <int L> struct FftPlanL;
+template <> struct FftPlanL<48> { typedef Radices<16, 3> R; };
+template <> struct FftPlanL<64> { typedef Radices<8, 8> R; };
+template <> struct FftPlanL<96> { typedef Radices<16, 6> R; };
+template <> struct FftPlanL<128> { typedef Radices<16, 8> R; };
+template <> struct FftPlanL<144> { typedef Radices<12, 12> R; };
+template <> struct FftPlanL<192> { typedef Radices<16, 12> R; };
+template <> struct FftPlanL<256> { typedef Radices<16, 16> R; };
+template <> struct FftPlanL<288> { typedef Radices<16, 6, 3> R; };
+template <> struct FftPlanL<384> { typedef Radices<16, 8, 3> R; };
+template <> struct FftPlanL<512> { typedef Radices<8, 8, 8> R; };
+template <> struct FftPlanL<576> { typedef Radices<16, 12, 3> R; };
+template <> struct FftPlanL<768> { typedef Radices<16, 16, 3> R; };
+
+#define FFT2_LENGTHS(X) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(288) X(384) X(512) X(576) X(768)
+
+// ---------------------------------------------------------------------------
+// register codelets: out-of-place R-point DFT, v[] -> v[] (forward sign -)
+// ---------------------------------------------------------------------------
+template <int R> struct CodeletConst;
+// cos / sin of 2 pi m / R
+template <> struct CodeletConst<8> {
+  DNS_HD static double c(int m) {
+    const double t[8] = {1.0, 0.70710678118654752440084436210485, 0.0, -0.70710678118654752440084436210485,
+                         -1.0, -0.70710678118654752440084436210485, 0.0, 0.70710678118654752440084436210485};
+    return t[m & 7];
+  }
+  DNS_HD static double s(int m) { return c((m + 6) & 7); }
+};
+template <> struct CodeletConst<16> {
+  DNS_HD static double c(int m) {
+    const double a = 0.92387953251128675612818318939679, b = 0.38268343236508977172845998403040,
+                 h = 0.70710678118654752440084436210485;
+    const double t[16] = {1.0, a, h, b, 0.0, -b, -h, -a, -1.0, -a, -h, -b, 0.0, b, h, a};
+    return t[m & 15];
+  }
+  DNS_HD static double s(int m) { return c((m + 12) & 15); }
+};
+template <> struct CodeletConst<12> {
+  DNS_HD static double c(int m) {
+    const double r = 0.86602540378443864676372317075294;
+    const double t[12] = {1.0, r, 0.5, 0.0, -0.5, -r, -1.0, -r, -0.5, 0.0, 0.5, r};
+    return t[m % 12];
+  }
+  DNS_HD static double s(int m) { return c((m + 9) % 12); }
+};
+template <> struct CodeletConst<6> {
+  DNS_HD static double c(int m) {
+    const double t[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
+    return t[m % 6];
+  }
+  DNS_HD static double s(int m) {
+    const double r = 0.86602540378443864676372317075294;
+    const double t[6] = {0.0, r, r, 0.0, -r, -r};
+    return t[m % 6];
+  }
+};
+
+// W_R^m (forward: exp(-2 pi i m / R)); INV conjugates
+template <int R, bool INV, typename C>
+DNS_HD C wconst(int m) {
+  typedef T_of<C> T;
+  const double cc = CodeletConst<R>::c(m);
+  const double ss = CodeletConst<R>::s(m);
+  C w;
+  w.x = (T)cc;
+  w.y = (T)(INV ? ss : -ss);
+  return w;
+}
+
+template <bool INV, typename C>
+DNS_HD void dft2(C& a, C& b) {
+  C t = a - b;
+  a = a + b;
+  b = t;
+}
+
+template <bool INV, typename C>
+DNS_HD void dft3(C& y0, C& y1, C& y2) {
+  typedef T_of<C> T;
+  const T c3 = (T)(-0.5);
+  const T s3 = (T)0.86602540378443864676372317075294;
+  C t1 = y1 + y2;
+  C t2 = y1 - y2;
+  C base = y0 + t1 * c3;
+  C its = muli(t2) * s3;
+  y0 = y0 + t1;
+  if (INV) { y1 = base + its; y2 = base - its; }
+  else { y1 = base - its; y2 = base + its; }
+}
+
+template <bool INV, typename C>
+DNS_HD void dft4(C& y0, C& y1, C& y2, C& y3) {
+  C a = y0 + y2, b = y0 - y2, c = y1 + y3, d = y1 - y3;
+  C id = muli(d);
+  y0 = a + c;
+  y2 = a - c;
+  if (INV) { y1 = b + id; y3 = b - id; }
+  else { y1 = b - id; y3 = b + id; }
+}
+
+// Generic R = R1 * R2 codelet: x[r2 + R2 r1] -> X[k1 + R1 k2]
+template <int R, bool INV, typename C> struct Codelet;
+
+template <bool INV, typename C> struct Codelet<2, INV, C> {
+  DNS_HD static void run(C* v) { dft2<INV>(v[0], v[1]); }
+};
+template <bool INV, typename C> struct Codelet<3, INV, C> {
+  DNS_HD static void run(C* v) { dft3<INV>(v[0], v[1], v[2]); }
+};
+template <bool INV, typename C> struct Codelet<4, INV, C> {
+  DNS_HD static void run(C* v) { dft4<INV>(v[0], v[1], v[2], v[3]); }
+};
+
+template <int R1, int R2, int R, bool INV, typename C>
+DNS_HD void codelet_split(C* v) {
+  // step 1: R2 DFTs of size R1 over r1 (stride R2), twiddle W_R^{r2 k1}
+  C t[R];
+#pragma unroll
+  for (int r2 = 0; r2 < R2; ++r2) {
+    C a[R1];
+#pragma unroll
+    for (int r1 = 0; r1 < R1; ++r1) a[r1] = v[r2 + R2 * r1];
+    Codelet<R1, INV, C>::run(a);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      C x = a[k1];
+      if (r2 * k1) x = cmul(x, wconst<R, INV, C>(r2 * k1));
+      t[k1 * R2 + r2] = x;
+    }
+  }
+  // step 2: R1 DFTs of size R2 over r2, output X[k1 + R1 k2]
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    C b[R2];
+#pragma unroll
+    for (int r2 = 0; r2 < R2; ++r2) b[r2] = t[k1 * R2 + r2];
+    Codelet<R2, INV, C>::run(b);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = b[k2];
+  }
+}
+
+template <bool INV, typename C> struct Codelet<6, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<2, 3, 6, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<8, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<2, 4, 8, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<12, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<4, 3, 12, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<16, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<4, 4, 16, INV, C>(v); }
+};
+
+// ---------------------------------------------------------------------------
+// one Stockham pass; Ns = product of the previous radices
+// ---------------------------------------------------------------------------
+template <int L, int R, int Ns, bool INV, typename C>
+struct FftPass {
+  static constexpr int NB = L / R;  // butterflies per line
+  // read inputs of butterfly j of one line into v, twiddled
+  DNS_HD static void load(const C* line, int j, C* v, const C* tw) {
+    const int k = j % Ns;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      C x = line[fpos(j + r * NB)];
+      if (Ns > 1 && r > 0 && k > 0) {
+        const C w = tw[(r * k) * (L / (Ns * R))];
+        x = INV ? cmulc(x, w) : cmul(x, w);
+      }
+      v[r] = x;
+    }
+    Codelet<R, INV, C>::run(v);
+  }
+  DNS_HD static void store(C* line, int j, const C* v) {
+    const int k = j % Ns;
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) line[fpos(base + r * Ns)] = v[r];
+  }
+};
+
+#ifdef __CUDACC__
+// One pass over nb lines (line stride ls >= fpad_len(L)) by the whole block.
+// A thread keeps KMAX butterflies in registers; a round covers whole lines,
+// so all reads of a line precede all writes to it.
+template <typename C, int L, bool INV, int R, int Ns>
+__device__ __forceinline__ void fft2_pass(C* buf, int nb, int ls, const C* __restrict__ tw) {
+  typedef FftPass<L, R, Ns, INV, C> P;
+  constexpr int KMAX = (16 / R) > 0 ? 16 / R : 1;
+  const int per_round = (KMAX * (int)blockDim.x) / P::NB;
+  for (int l0 = 0; l0 < nb; l0 += per_round) {
+    const int total = min(per_round, nb - l0) * P::NB;
+    C v[KMAX][R];
+#pragma unroll
+    for (int q = 0; q < KMAX; ++q) {
+      const int w = q * blockDim.x + threadIdx.x;
+      if (w < total) {
+        const int line = w / P::NB;
+        const int j = w - line * P::NB;
+        P::load(buf + (size_t)(l0 + line) * ls, j, v[q], tw);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < KMAX; ++q) {
+      const int w = q * blockDim.x + threadIdx.x;
+      if (w < total) {
+        const int line = w / P::NB;
+        const int j = w - line * P::NB;
+        P::store(buf + (size_t)(l0 + line) * ls, j, v[q]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename C, int L, bool INV, int Ns, int R, int... Rest>
+struct FftRun {
+  __device__ __forceinline__ static void go(C* buf, int nb, int ls, const C* tw) {
+    fft2_pass<C, L, INV, R, Ns>(buf, nb, ls, tw);
+    FftRun<C, L, INV, Ns * R, Rest...>::go(buf, nb, ls, tw);
+  }
+};
+template <typename C, int L, bool INV, int Ns, int R>
+struct FftRun<C, L, INV, Ns, R> {
+  __device__ __forceinline__ static void go(C* buf, int nb, int ls, const C* tw) {
+    fft2_pass<C, L, INV, R, Ns>(buf, nb, ls, tw);
+  }
+};
+
+template <typename C, int L, bool INV, typename RS> struct FftDo;
+template <typename C, int L, bool INV, int... Rs>
+struct FftDo<C, L, INV, Radices<Rs...>> {
+  __device__ __forceinline__ static void go(C* buf, int nb, int ls, const C* tw) {
+    FftRun<C, L, INV, 1, Rs...>::go(buf, nb, ls, tw);
+  }
+};
+
+// Entry: the lines must be written (at fpos positions) before the call;
+// a barrier is taken first, and the result is complete on return.
+template <typename C, int L, bool INV>
+__device__ __forceinline__ void fft2(C* buf, int nb, int ls, const C* __restrict__ tw) {
+  __syncthreads();
+  FftDo<C, L, INV, typename FftPlanL<L>::R>::go(buf, nb, ls, tw);
+}
+#endif

@@ -15,6 +15,7 @@
 // project's own FFT (fft.cuh).  Collocation-point values of v, v'', v'''',
 // omega, omega'' (the reference's T0/T2/T4 matrix products) are obtained the
 // same way: coefficient-space derivatives, then the no-pad DCT.
+#include "fftline.cuh"
 #include "kernels.cuh"
 #include "ypass.cuh"
 
@@ -289,12 +290,14 @@ __global__ void k_solve_eq(const double2* __restrict__ inv, double2* rhs, long l
 // then the padded s2p of all six fields, written pencil-major for the
 // spanwise pass.  Fields: u, v(span), w(wall), omega_x, omega_y, omega_z.
 // ---------------------------------------------------------------------------
-template <typename C>
-__global__ void k_y3(const double2* __restrict__ V, const double2* __restrict__ O,
+template <typename C, int LM>
+__global__ void __launch_bounds__(256, 2) k_y3(const double2* __restrict__ V, const double2* __restrict__ O,
                      PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab) {
+  typedef FLine<C, LM> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   const int M = tab.plan.L;  // 4 (Ny - 1)
+  const int ls = FL::stride(M);
   Carve cv(smem_raw);
   double2* w = cv.take<double2>(Ny);
   double2* oz = cv.take<double2>(Ny);
@@ -305,7 +308,7 @@ __global__ void k_y3(const double2* __restrict__ V, const double2* __restrict__ 
   double2* Dv = cv.take<double2>(Ny);
   double2* ox = cv.take<double2>(Ny);
   double2* oy = cv.take<double2>(Ny);
-  C* lines = cv.take<C>((size_t)6 * M);
+  C* lines = cv.take<C>((size_t)6 * ls);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -347,14 +350,14 @@ __global__ void k_y3(const double2* __restrict__ V, const double2* __restrict__ 
   for (int t = threadIdx.x; t < 6 * M; t += blockDim.x) {
     const int f = t / M;
     const int n = t - f * M;
-    lines[(size_t)f * M + tab.drev[n]] = from_d2<C>(ext_s2p_pad<C>(src[f], n, M, Ny));
+    lines[(size_t)f * ls + FL::in_pos(tab, n)] = from_d2<C>(ext_s2p_pad<C>(src[f], n, M, Ny));
   }
-  fft_batch<C, false>(lines, 6, M, tab.plan, tab.tw);
+  FL::template fft<false>(lines, 6, ls, tab);
   const int Py = g.Py;
   for (int t = threadIdx.x; t < 6 * Py; t += blockDim.x) {
     const int f = t / Py;
     const int j = t - f * Py;
-    pencil_ptr<C>(out, f, p)[j] = lines[(size_t)f * M + j];
+    pencil_ptr<C>(out, f, p)[j] = lines[(size_t)f * ls + FL::out_pos(j)];
   }
 }
 
@@ -365,17 +368,21 @@ __global__ void k_y3(const double2* __restrict__ V, const double2* __restrict__ 
 //   boot: only store the nonlinear terms as the AB2 history (the effect of
 //         the reference's "extra previous step", source/main_loop.cpp:39-52).
 // ---------------------------------------------------------------------------
-template <typename C>
-__global__ void k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
+template <typename C, int LM, int LM0>
+__global__ void __launch_bounds__(256, 2) k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
                      double2* Nvp, double2* Nop, double2* rv, double2* ro,
                      const double* __restrict__ Ut, const double* __restrict__ ddUt,
                      DnsGeom g, PhysParams ph, FftTab<C> tabP, FftTab<double2> tab0,
                      int boot) {
+  typedef FLine<C, LM> FP;
+  typedef FLine<double2, LM0> F0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   const int Py = g.Py;
   const int M = tabP.plan.L;   // 2 (Py - 1)
   const int M0 = tab0.plan.L;  // 2 (Ny - 1)
+  const int lsP = FP::stride(M);
+  const int ls0 = F0::stride(M0);
   Carve cv(smem_raw);
   double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients
   double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
@@ -391,8 +398,8 @@ __global__ void k_y1(PencilArr lam, const double2* __restrict__ V, const double2
   double2* D4V = cv.take<double2>(Ny);
   double2* nvp = cv.take<double2>(Ny);
   double2* nop = cv.take<double2>(Ny);
-  const size_t bytesP = (size_t)3 * M * sizeof(C);
-  const size_t bytes0 = (size_t)7 * M0 * sizeof(double2);
+  const size_t bytesP = (size_t)3 * lsP * sizeof(C);
+  const size_t bytes0 = (size_t)7 * ls0 * sizeof(double2);
   unsigned char* region = (unsigned char*)cv.take<unsigned char>(bytesP > bytes0 ? bytesP : bytes0);
   C* linesP = (C*)region;
   double2* lines0 = (double2*)region;
@@ -410,7 +417,7 @@ __global__ void k_y1(PencilArr lam, const double2* __restrict__ V, const double2
     const int f = t / M;
     const int n = t - f * M;
     const C* src = pencil_ptr<C>(lam, f, p);
-    linesP[(size_t)f * M + tabP.drev[n]] = (n < Py) ? src[n] : src[M - n];
+    linesP[(size_t)f * lsP + FP::in_pos(tabP, n)] = (n < Py) ? src[n] : src[M - n];
   }
   for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
     Vc[n] = V[p * Ny + n];
@@ -418,12 +425,12 @@ __global__ void k_y1(PencilArr lam, const double2* __restrict__ V, const double2
     nvp[n] = Nvp[p * Ny + n];
     nop[n] = Nop[p * Ny + n];
   }
-  fft_batch<C, false>(linesP, 3, M, tabP.plan, tabP.tw);
+  FP::template fft<false>(linesP, 3, lsP, tabP);
   const double sc = 1.0 / (Py - 1);
   for (int t = threadIdx.x; t < 3 * Ny; t += blockDim.x) {
     const int f = t / Ny;
     const int k = t - f * Ny;
-    double2 c = to_d2(linesP[(size_t)f * M + k]) * sc;
+    double2 c = to_d2(linesP[(size_t)f * lsP + FP::out_pos(k)]) * sc;
     if (k == 0) c = c * 0.5;
     lc[t] = c;
   }
@@ -462,55 +469,53 @@ __global__ void k_y1(PencilArr lam, const double2* __restrict__ V, const double2
   for (int t = threadIdx.x; t < nl * M0; t += blockDim.x) {
     const int f = t / M0;
     const int n = t - f * M0;
-    lines0[(size_t)f * M0 + tab0.drev[n]] = ext_s2p_nopad(srcs[f], n, M0, Ny);
+    lines0[(size_t)f * ls0 + F0::in_pos(tab0, n)] = ext_s2p_nopad(srcs[f], n, M0, Ny);
   }
-  fft_batch<double2, false>(lines0, nl, M0, tab0.plan, tab0.tw);
-  const double2* Nv = lines0;
-  const double2* No = lines0 + M0;
+  F0::template fft<false>(lines0, nl, ls0, tab0);
+  // collocation value at point m of line f (natural order)
+  auto col = [&](int f, int m) { return lines0[(size_t)f * ls0 + F0::out_pos(m)]; };
   if (boot) {
     for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-      Nvp[p * Ny + n] = Nv[n];
-      Nop[p * Ny + n] = No[n];
+      Nvp[p * Ny + n] = col(0, n);
+      Nop[p * Ny + n] = col(1, n);
     }
     return;
   }
-  const double2* P0 = lines0 + 2 * M0;
-  const double2* P2 = lines0 + 3 * M0;
-  const double2* P4 = lines0 + 4 * M0;
-  const double2* Q0 = lines0 + 5 * M0;
-  const double2* Q2 = lines0 + 6 * M0;
   const double dt = ph.dt, Re = ph.Re, al = ia;
   const int N = Ny - 1;
+  // lines: 0 Nv, 1 No, 2 v, 3 v'', 4 v(4), 5 omega, 6 omega''
   for (int i = threadIdx.x; i < Ny; i += blockDim.x) {
     double2 rvi = make_double2(0.0, 0.0), roi = make_double2(0.0, 0.0);
     if (zero) {
       // _get_linear_u0 / _w0: rows 2..N at point i-1
       if (i >= 2) {
         const int m = i - 1;
-        rvi = P0[m] + P2[m] * (dt * 0.5 / Re) - (Nv[m] * 1.5 - nvp[m] * 0.5) * dt;
-        roi = Q0[m] + Q2[m] * (dt * 0.5 / Re) - (No[m] * 1.5 - nop[m] * 0.5) * dt;
+        rvi = col(2, m) + col(3, m) * (dt * 0.5 / Re) - (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
+        roi = col(5, m) + col(6, m) * (dt * 0.5 / Re) - (col(1, m) * 1.5 - nop[m] * 0.5) * dt;
       }
     } else {
       if (i >= 4 && i <= N) {
         const int m = i - 2;
         const double Um = Ut[m];
-        const double2 re = P4[m] * (dt * 0.5 / Re) + P2[m] * (1 - kmn * dt / Re)
-                           - P0[m] * (kmn * (1 - kmn * dt * 0.5 / Re));
-        const double2 im = P2[m] * (-al * dt * 0.5 * Um)
-                           + P0[m] * (kmn * al * dt * 0.5 * Um + al * dt * 0.5 * ddUt[m]);
-        rvi = re + muli(im) + (Nv[m] * 1.5 - nvp[m] * 0.5) * dt;
+        const double2 P0 = col(2, m), P2 = col(3, m), P4 = col(4, m);
+        const double2 re = P4 * (dt * 0.5 / Re) + P2 * (1 - kmn * dt / Re)
+                           - P0 * (kmn * (1 - kmn * dt * 0.5 / Re));
+        const double2 im = P2 * (-al * dt * 0.5 * Um)
+                           + P0 * (kmn * al * dt * 0.5 * Um + al * dt * 0.5 * ddUt[m]);
+        rvi = re + muli(im) + (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
       }
       if (i >= 2) {
         const int m = i - 1;
-        const double2 re = Q2[m] * (0.5 / Re * dt) + Q0[m] * (1 - kmn * dt * 0.5 / Re);
-        const double2 im = Q0[m] * (-al * dt * 0.5 * Ut[m]);
-        roi = re + muli(im) + (No[m] * 1.5 - nop[m] * 0.5) * dt;
+        const double2 Q0 = col(5, m), Q2 = col(6, m);
+        const double2 re = Q2 * (0.5 / Re * dt) + Q0 * (1 - kmn * dt * 0.5 / Re);
+        const double2 im = Q0 * (-al * dt * 0.5 * Ut[m]);
+        roi = re + muli(im) + (col(1, m) * 1.5 - nop[m] * 0.5) * dt;
       }
     }
     rv[p * Ny + i] = rvi;
     ro[p * Ny + i] = roi;
-    Nvp[p * Ny + i] = Nv[i];
-    Nop[p * Ny + i] = No[i];
+    Nvp[p * Ny + i] = col(0, i);
+    Nop[p * Ny + i] = col(1, i);
   }
 }
 
@@ -564,13 +569,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 #define Y2_WAIT_LIMIT (1LL << 31)
 
+template <int LM0>
 __global__ void k_y2(const double2* __restrict__ AT, double2* V, double2* O,
                      const double2* __restrict__ rv, const double2* __restrict__ ro,
                      const double* __restrict__ dUt, DnsGeom g, PhysParams ph,
                      FftTab<double2> tab0, int CH, int NST, int* status) {
+  typedef FLine<double2, LM0> F0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   const int M0 = tab0.plan.L;
+  const int ls0 = F0::stride(M0);
   Carve cv(smem_raw);
   uint64_t* full = cv.take<uint64_t>(NST);
   double2* ring = cv.take<double2>((size_t)NST * CH * Ny);
@@ -578,7 +586,7 @@ __global__ void k_y2(const double2* __restrict__ AT, double2* V, double2* O,
   double2* ro_s = cv.take<double2>((size_t)2 * Ny); // omega right-hand sides
   double2* vold = cv.take<double2>((size_t)2 * Ny);
   double2* xv = cv.take<double2>((size_t)2 * Ny);
-  double2* lines = cv.take<double2>((size_t)2 * M0);
+  double2* lines = cv.take<double2>((size_t)2 * ls0);
 
   const int kx = blockIdx.x % g.Kx;
   const int kzs = blockIdx.x / g.Kx;  // slot kz' in [0, Nz/2]
@@ -642,16 +650,16 @@ __global__ void k_y2(const double2* __restrict__ AT, double2* V, double2* O,
           else if (n == Ny - 1) { src = n; sc = 1.0; }
           else { src = M0 - n; sc = 0.5; }
           const double2 sv = (xv[bb * Ny + src] + vold[bb * Ny + src]) * sc;
-          lines[(size_t)bb * M0 + tab0.drev[n]] = sv;
+          lines[(size_t)bb * ls0 + F0::in_pos(tab0, n)] = sv;
         }
-        fft_batch<double2, false>(lines, npen, M0, tab0.plan, tab0.tw);
+        F0::template fft<false>(lines, npen, ls0, tab0);
         if (active && i >= 2) {
           const int m = i - 1;
           const int kzp = (b == 0) ? kzs : g.Nz - kzs;
           double iab, ibb;
           wavenumbers(kx, kzp, g.Nz, ph.aphi, ph.beta, iab, ibb);
           const double coef = -0.5 * ibb * dUt[m] * ph.dt;
-          ro_s[b * Ny + i] = ro_s[b * Ny + i] + muli(lines[(size_t)b * M0 + m] * coef);
+          ro_s[b * Ny + i] = ro_s[b * Ny + i] + muli(lines[(size_t)b * ls0 + F0::out_pos(m)] * coef);
         }
       }
       __syncthreads();
@@ -694,20 +702,20 @@ __global__ void k_y2(const double2* __restrict__ AT, double2* V, double2* O,
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-size_t y3_smem(int Ny, int M, size_t csz) {
+size_t y3_smem(int Ny, int ls, size_t csz) {
   auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
-  return 9 * a((size_t)Ny * 16) + a((size_t)6 * M * csz);
+  return 9 * a((size_t)Ny * 16) + a((size_t)6 * ls * csz);
 }
-size_t y1_smem(int Ny, int M, int M0, size_t csz) {
+size_t y1_smem(int Ny, int lsP, int ls0, size_t csz) {
   auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
   size_t s = a((size_t)3 * Ny * 16) + a((size_t)2 * Ny * 16) + 12 * a((size_t)Ny * 16);
-  size_t bp = (size_t)3 * M * csz, b0 = (size_t)7 * M0 * 16;
+  size_t bp = (size_t)3 * lsP * csz, b0 = (size_t)7 * ls0 * 16;
   return s + a(bp > b0 ? bp : b0);
 }
-size_t y2_smem(int Ny, int M0, int CH, int NST) {
+size_t y2_smem(int Ny, int ls0, int CH, int NST) {
   auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
   return a((size_t)NST * 8) + a((size_t)NST * CH * Ny * 16) + 4 * a((size_t)2 * Ny * 16) +
-         a((size_t)2 * M0 * 16);
+         a((size_t)2 * ls0 * 16);
 }
 
 template <typename C>
@@ -755,10 +763,13 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
                       PhysParams ph, FftTab<C> tab, cudaStream_t st) {
-  const size_t sm = y3_smem(g.Ny, tab.plan.L, sizeof(C));
-  cudaFuncSetAttribute(k_y3<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_y3<C><<<(unsigned)g.H, 256, sm, st>>>(V, O, out, g, ph, tab);
-  return cudaGetLastError();
+  return with_len_m(tab.plan.L, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    const size_t sm = y3_smem(g.Ny, FLine<C, L>::stride(tab.plan.L), sizeof(C));
+    cudaFuncSetAttribute(k_y3<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_y3<C, L><<<(unsigned)g.H, 256, sm, st>>>(V, O, out, g, ph, tab);
+    return cudaGetLastError();
+  });
 }
 template cudaError_t launch_y3<double2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<double2>, cudaStream_t);
 template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<float2>, cudaStream_t);
@@ -768,11 +779,16 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
                       double2* Nop, double2* rv, double2* ro, const double* Ut,
                       const double* ddUt, DnsGeom g, PhysParams ph, FftTab<C> tabP,
                       FftTab<double2> tab0, int boot, cudaStream_t st) {
-  const size_t sm = y1_smem(g.Ny, tabP.plan.L, tab0.plan.L, sizeof(C));
-  cudaFuncSetAttribute(k_y1<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_y1<C><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, rv, ro, Ut, ddUt, g, ph, tabP,
-                                          tab0, boot);
-  return cudaGetLastError();
+  return with_len_m(tabP.plan.L, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    constexpr int L0 = L / 2;  // the no-pad extension is half the padded one
+    const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L),
+                              FLine<double2, L0>::stride(tab0.plan.L), sizeof(C));
+    cudaFuncSetAttribute(k_y1<C, L, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_y1<C, L, L0><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, rv, ro, Ut, ddUt, g, ph,
+                                                   tabP, tab0, boot);
+    return cudaGetLastError();
+  });
 }
 template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, const double*, const double*, DnsGeom, PhysParams, FftTab<double2>, FftTab<double2>, int, cudaStream_t);
 template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, const double*, const double*, DnsGeom, PhysParams, FftTab<float2>, FftTab<double2>, int, cudaStream_t);
@@ -782,11 +798,16 @@ cudaError_t launch_y2(const double2* AT, double2* V, double2* O, const double2* 
                       FftTab<double2> tab0, int* status, cudaStream_t st) {
   const int CH = 8;
   const int NST = 4;
-  const size_t sm = y2_smem(g.Ny, tab0.plan.L, CH, NST);
-  cudaFuncSetAttribute(k_y2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  int threads = ((2 * g.Ny + 31) / 32) * 32;
-  if (threads < 64) threads = 64;
-  const unsigned nslots = (unsigned)(g.Kx * g.Kh);
-  k_y2<<<nslots, threads, sm, st>>>(AT, V, O, rv, ro, dUt, g, ph, tab0, CH, NST, status);
-  return cudaGetLastError();
+  // the tilting transform is a small part of this kernel: the runtime-length
+  // FFT keeps its register footprint (and so the occupancy) low
+  return with_len_m0(0, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    const size_t sm = y2_smem(g.Ny, FLine<double2, L>::stride(tab0.plan.L), CH, NST);
+    cudaFuncSetAttribute(k_y2<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int threads = ((2 * g.Ny + 31) / 32) * 32;
+    if (threads < 64) threads = 64;
+    const unsigned nslots = (unsigned)(g.Kx * g.Kh);
+    k_y2<L><<<nslots, threads, sm, st>>>(AT, V, O, rv, ro, dUt, g, ph, tab0, CH, NST, status);
+    return cudaGetLastError();
+  });
 }

@@ -15,6 +15,7 @@
 // the zeroing of both Nyquist modes are folded into the one pass.
 //
 // Streamwise pass: two real rows share one complex FFT (a + i b).
+#include "fftline.cuh"
 #include "kernels.cuh"
 #include "zxpass.cuh"
 
@@ -32,11 +33,13 @@ __device__ __forceinline__ C* ppen(const PencilArr& a, int f, long long p) {
 // ---------------------------------------------------------------------------
 // spanwise backward: pencils [f][kz*Kx+kx][y] -> rows [f][y][zp][kx]
 // ---------------------------------------------------------------------------
-template <typename C, int TX, int TY>
+template <typename C, int TX, int TY, int L>
 __global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
+  typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
   const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int ls = FL::stride(Pz);
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
@@ -47,7 +50,7 @@ __global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
   for (int t = threadIdx.x; t < NL * nzero; t += blockDim.x) {
     const int li = t / nzero;
     const int n = hz + (t - li * nzero);
-    lines[(size_t)li * Pz + tab.drev[n]] = cmk<C>(0.0, 0.0);
+    lines[(size_t)li * ls + FL::in_pos(tab, n)] = cmk<C>(0.0, 0.0);
   }
   for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
     const int yl = t % TY;
@@ -59,9 +62,9 @@ __global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
     const int y = y0 + yl;
     C v = cmk<C>(0.0, 0.0);
     if (kx < Kx - 1 && y < Py) v = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
-    lines[(size_t)(kxl * TY + yl) * Pz + tab.drev[n]] = v;
+    lines[(size_t)(kxl * TY + yl) * ls + FL::in_pos(tab, n)] = v;
   }
-  fft_batch<C, true>(lines, NL, Pz, tab.plan, tab.tw);
+  FL::template fft<true>(lines, NL, ls, tab);
   for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
     const int kxl = t % TX;
     const int zp = (t / TX) % Pz;
@@ -69,18 +72,20 @@ __global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
     const int kx = kx0 + kxl;
     const int y = y0 + yl;
     if (kx < Kx && y < Py)
-      prow<C>(out, f, (long long)y * Pz + zp)[kx] = lines[(size_t)(kxl * TY + yl) * Pz + zp];
+      prow<C>(out, f, (long long)y * Pz + zp)[kx] = lines[(size_t)(kxl * TY + yl) * ls + FL::out_pos(zp)];
   }
 }
 
 // ---------------------------------------------------------------------------
 // spanwise forward: rows [f][y][zp][kx] -> pencils [f][kz*Kx+kx][y]
 // ---------------------------------------------------------------------------
-template <typename C, int TX, int TY>
+template <typename C, int TX, int TY, int L>
 __global__ void k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
+  typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
   const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int ls = FL::stride(Pz);
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
@@ -93,9 +98,9 @@ __global__ void k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
     const int y = y0 + yl;
     C v = cmk<C>(0.0, 0.0);
     if (kx < Kx && y < Py) v = prow<C>(in, f, (long long)y * Pz + zp)[kx];
-    lines[(size_t)(kxl * TY + yl) * Pz + tab.drev[zp]] = v;
+    lines[(size_t)(kxl * TY + yl) * ls + FL::in_pos(tab, zp)] = v;
   }
-  fft_batch<C, false>(lines, NL, Pz, tab.plan, tab.tw);
+  FL::template fft<false>(lines, NL, ls, tab);
   const int hz = Nz / 2;
   for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
     const int yl = t % TY;
@@ -105,7 +110,7 @@ __global__ void k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
     const int y = y0 + yl;
     const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
     if (kx < Kx && y < Py)
-      ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * Pz + n];
+      ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * ls + FL::out_pos(n)];
   }
 }
 
@@ -146,15 +151,17 @@ __device__ __forceinline__ C unpack_r2c(const C* Z, int k, int Px, bool imag_par
 // lambda_x, lambda_y(span), lambda_z(wall).  RB rows per CTA (even, rows of
 // one wall-normal plane).
 // ---------------------------------------------------------------------------
-template <typename C>
+template <typename C, int L>
 __global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
                           const double* __restrict__ Uy, double Ro, int RB) {
+  typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  typedef decltype(C().x) T;
+  typedef T_of<C> T;
   const int Px = g.Px;
   const int hx = g.Nx / 2;
-  C* zin = (C*)smem_raw;               // 3*RB lines
-  C* zout = zin + (size_t)3 * RB * Px; // RB lines (lx + i ly) then RB/2 (lz pairs)
+  const int ls = FL::stride(Px);
+  C* zin = (C*)smem_raw;                // 3*RB lines
+  C* zout = zin + (size_t)3 * RB * ls;  // RB lines (lx + i ly) then RB/2 (lz pairs)
   const long long r0 = (long long)blockIdx.x * RB;
   const long long nrows = (long long)g.Py * g.Pz;
   for (int t = threadIdx.x; t < RB * 3 * Px; t += blockDim.x) {
@@ -165,13 +172,17 @@ __global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
     const long long row = r0 + rl;
     C z = cmk<C>(0.0, 0.0);
     if (row < nrows) {
-      const C* a = prow<C>(in, 2 * q, row);
-      const C* b = prow<C>(in, 2 * q + 1, row);
+      // fields of similar magnitude share a transform (the smaller one's
+      // rounding error is relative to the larger): (u, v), (ox, oy), (w, oz)
+      const int fa = (q == 0) ? 0 : (q == 1 ? 3 : 2);
+      const int fb = (q == 0) ? 1 : (q == 1 ? 4 : 5);
+      const C* a = prow<C>(in, fa, row);
+      const C* b = prow<C>(in, fb, row);
       z = pack_c2r<C>(a, b, n, Px, hx);
     }
-    zin[(size_t)(rl * 3 + q) * Px + tab.drev[n]] = z;
+    zin[(size_t)(rl * 3 + q) * ls + FL::in_pos(tab, n)] = z;
   }
-  fft_batch<C, true>(zin, 3 * RB, Px, tab.plan, tab.tw);
+  FL::template fft<true>(zin, 3 * RB, ls, tab);
   const T ro = (T)Ro;
   for (int t = threadIdx.x; t < RB * Px; t += blockDim.x) {
     const int rl = t / Px;
@@ -179,20 +190,21 @@ __global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
     const long long row = r0 + rl;
     const int y = (int)(row / g.Pz);
     const T Ub = (row < nrows) ? (T)Uy[y] : (T)0;
-    const C z0 = zin[(size_t)(rl * 3 + 0) * Px + j];
-    const C z1 = zin[(size_t)(rl * 3 + 1) * Px + j];
-    const C z2 = zin[(size_t)(rl * 3 + 2) * Px + j];
-    const T u = z0.x, v = z0.y, w = z1.x, ox = z1.y, oy = z2.x, oz = z2.y;
+    const int op = FL::out_pos(j);
+    const C z0 = zin[(size_t)(rl * 3 + 0) * ls + op];
+    const C z1 = zin[(size_t)(rl * 3 + 1) * ls + op];
+    const C z2 = zin[(size_t)(rl * 3 + 2) * ls + op];
+    const T u = z0.x, v = z0.y, ox = z1.x, oy = z1.y, w = z2.x, oz = z2.y;
     const T lx = oz * v - oy * w - ro * w;
     const T ly = ox * w - oz * u;
     const T lz = oy * u - ox * v + ro * (u + Ub);
-    const int pos = tab.drev[j];
+    const int pos = FL::in_pos(tab, j);
     C A; A.x = lx; A.y = ly;
-    zout[(size_t)rl * Px + pos] = A;
-    T* B = (T*)(zout + (size_t)(RB + rl / 2) * Px + pos);
+    zout[(size_t)rl * ls + pos] = A;
+    T* B = (T*)(zout + (size_t)(RB + rl / 2) * ls + pos);
     B[rl & 1] = lz;
   }
-  fft_batch<C, false>(zout, RB + RB / 2, Px, tab.plan, tab.tw);
+  FL::template fft<false>(zout, RB + RB / 2, ls, tab);
   const int Kx = g.Kx;
   const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
   for (int t = threadIdx.x; t < RB * 3 * Kx; t += blockDim.x) {
@@ -201,9 +213,13 @@ __global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
     const int rl = t / (3 * Kx);
     const long long row = r0 + rl;
     if (row >= nrows) continue;
+    const C* Z = (fl < 2) ? zout + (size_t)rl * ls : zout + (size_t)(RB + rl / 2) * ls;
+    const bool im = (fl < 2) ? (fl == 1) : ((rl & 1) != 0);
+    const C zk = Z[FL::out_pos(k)];
+    const C zm = Z[FL::out_pos((Px - k) % Px)];
     C v;
-    if (fl < 2) v = unpack_r2c<C>(zout + (size_t)rl * Px, k, Px, fl == 1);
-    else v = unpack_r2c<C>(zout + (size_t)(RB + rl / 2) * Px, k, Px, (rl & 1) != 0);
+    if (!im) { v.x = zk.x + zm.x; v.y = zk.y - zm.y; }
+    else { v.x = zk.y + zm.y; v.y = zm.x - zk.x; }
     prow<C>(out, fl, row)[k] = v * sc;
   }
 }
@@ -304,30 +320,39 @@ template <> struct ZTile<float2> { enum { TX = 8, TY = 4 }; };
 template <typename C>
 cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
-  const size_t sm = (size_t)TX * TY * g.Pz * sizeof(C);
-  cudaFuncSetAttribute(k_zb<C, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
-  k_zb<C, TX, TY><<<grid, 256, sm, st>>>(in, out, g, tab);
-  return cudaGetLastError();
+  return with_len_xz(g.Pz, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
+    cudaFuncSetAttribute(k_zb<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
+    k_zb<C, TX, TY, L><<<grid, 256, sm, st>>>(in, out, g, tab);
+    return cudaGetLastError();
+  });
 }
 template <typename C>
 cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
-  const size_t sm = (size_t)TX * TY * g.Pz * sizeof(C);
-  cudaFuncSetAttribute(k_zf<C, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
-  k_zf<C, TX, TY><<<grid, 256, sm, st>>>(in, out, g, tab);
-  return cudaGetLastError();
+  return with_len_xz(g.Pz, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
+    cudaFuncSetAttribute(k_zf<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
+    k_zf<C, TX, TY, L><<<grid, 256, sm, st>>>(in, out, g, tab);
+    return cudaGetLastError();
+  });
 }
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
                            double Ro, cudaStream_t st) {
   const int RB = 2;
-  const size_t sm = (size_t)(3 * RB + RB + RB / 2) * g.Px * sizeof(C);
-  cudaFuncSetAttribute(k_x_fused<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  const long long nrows = (long long)g.Py * g.Pz;
-  k_x_fused<C><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(in, out, g, tab, Uy, Ro, RB);
-  return cudaGetLastError();
+  return with_len_xz(g.Px, [&](auto LL) {
+    constexpr int L = decltype(LL)::value;
+    const size_t sm = (size_t)(3 * RB + RB + RB / 2) * FLine<C, L>::stride(g.Px) * sizeof(C);
+    cudaFuncSetAttribute(k_x_fused<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const long long nrows = (long long)g.Py * g.Pz;
+    k_x_fused<C, L><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(in, out, g, tab, Uy, Ro, RB);
+    return cudaGetLastError();
+  });
 }
 template <typename C>
 cudaError_t launch_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
