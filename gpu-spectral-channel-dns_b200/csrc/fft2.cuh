@@ -20,19 +20,35 @@ DNS_HD int fpad_len(int L) { return L + (L >> 4) + 1; }
 
 template <int... Rs> struct Radices {};
 
-template <int L> struct FftPlanL;
-template <> struct FftPlanL<48> { typedef Radices<16, 3> R; };
-template <> struct FftPlanL<64> { typedef Radices<8, 8> R; };
-template <> struct FftPlanL<96> { typedef Radices<16, 6> R; };
-template <> struct FftPlanL<128> { typedef Radices<16, 8> R; };
-template <> struct FftPlanL<144> { typedef Radices<12, 12> R; };
-template <> struct FftPlanL<192> { typedef Radices<16, 12> R; };
-template <> struct FftPlanL<256> { typedef Radices<16, 16> R; };
-template <> struct FftPlanL<288> { typedef Radices<16, 6, 3> R; };
-template <> struct FftPlanL<384> { typedef Radices<16, 8, 3> R; };
-template <> struct FftPlanL<512> { typedef Radices<8, 8, 8> R; };
-template <> struct FftPlanL<576> { typedef Radices<16, 12, 3> R; };
-template <> struct FftPlanL<768> { typedef Radices<16, 16, 3> R; };
+// Radix plans: MAXR 16 (fewer passes, FP32 data) or 8 (fewer registers per
+// butterfly, FP64 data).
+template <int L, int MAXR> struct FftPlanL;
+template <> struct FftPlanL<48, 16> { typedef Radices<16, 3> R; };
+template <> struct FftPlanL<64, 16> { typedef Radices<8, 8> R; };
+template <> struct FftPlanL<96, 16> { typedef Radices<16, 6> R; };
+template <> struct FftPlanL<128, 16> { typedef Radices<16, 8> R; };
+template <> struct FftPlanL<144, 16> { typedef Radices<12, 12> R; };
+template <> struct FftPlanL<192, 16> { typedef Radices<16, 12> R; };
+template <> struct FftPlanL<256, 16> { typedef Radices<16, 16> R; };
+template <> struct FftPlanL<288, 16> { typedef Radices<16, 6, 3> R; };
+template <> struct FftPlanL<384, 16> { typedef Radices<16, 8, 3> R; };
+template <> struct FftPlanL<512, 16> { typedef Radices<8, 8, 8> R; };
+template <> struct FftPlanL<576, 16> { typedef Radices<16, 12, 3> R; };
+template <> struct FftPlanL<768, 16> { typedef Radices<16, 16, 3> R; };
+template <> struct FftPlanL<48, 8> { typedef Radices<8, 6> R; };
+template <> struct FftPlanL<64, 8> { typedef Radices<8, 8> R; };
+template <> struct FftPlanL<96, 8> { typedef Radices<8, 4, 3> R; };
+template <> struct FftPlanL<128, 8> { typedef Radices<8, 4, 4> R; };
+template <> struct FftPlanL<144, 8> { typedef Radices<8, 6, 3> R; };
+template <> struct FftPlanL<192, 8> { typedef Radices<8, 8, 3> R; };
+template <> struct FftPlanL<256, 8> { typedef Radices<8, 8, 4> R; };
+template <> struct FftPlanL<288, 8> { typedef Radices<8, 6, 6> R; };
+template <> struct FftPlanL<384, 8> { typedef Radices<8, 8, 6> R; };
+template <> struct FftPlanL<512, 8> { typedef Radices<8, 8, 8> R; };
+template <> struct FftPlanL<576, 8> { typedef Radices<8, 6, 4, 3> R; };
+template <> struct FftPlanL<768, 8> { typedef Radices<8, 8, 4, 3> R; };
+template <typename C> struct FftMaxRadix { enum { v = 16 }; };
+template <> struct FftMaxRadix<double2> { enum { v = 8 }; };
 
 #define FFT2_LENGTHS(X) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(288) X(384) X(512) X(576) X(768)
 
@@ -211,7 +227,8 @@ struct FftPass {
 template <typename C, int L, bool INV, int R, int Ns>
 __device__ __forceinline__ void fft2_pass(C* buf, int nb, int ls, const C* __restrict__ tw) {
   typedef FftPass<L, R, Ns, INV, C> P;
-  constexpr int KMAX = (16 / R) > 0 ? 16 / R : 1;
+  // complex values a thread keeps in registers per round: the max radix
+  constexpr int KMAX = (FftMaxRadix<C>::v / R) > 0 ? FftMaxRadix<C>::v / R : 1;
   const int per_round = (KMAX * (int)blockDim.x) / P::NB;
   for (int l0 = 0; l0 < nb; l0 += per_round) {
     const int total = min(per_round, nb - l0) * P::NB;
@@ -266,6 +283,6 @@ struct FftDo<C, L, INV, Radices<Rs...>> {
 template <typename C, int L, bool INV>
 __device__ __forceinline__ void fft2(C* buf, int nb, int ls, const C* __restrict__ tw) {
   __syncthreads();
-  FftDo<C, L, INV, typename FftPlanL<L>::R>::go(buf, nb, ls, tw);
+  FftDo<C, L, INV, typename FftPlanL<L, FftMaxRadix<C>::v>::R>::go(buf, nb, ls, tw);
 }
 #endif

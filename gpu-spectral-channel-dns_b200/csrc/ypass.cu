@@ -291,7 +291,7 @@ __global__ void k_solve_eq(const double2* __restrict__ inv, double2* rhs, long l
 // spanwise pass.  Fields: u, v(span), w(wall), omega_x, omega_y, omega_z.
 // ---------------------------------------------------------------------------
 template <typename C, int LM>
-__global__ void __launch_bounds__(256, 2) k_y3(const double2* __restrict__ V, const double2* __restrict__ O,
+__global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, const double2* __restrict__ O,
                      PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab) {
   typedef FLine<C, LM> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256, 2) k_y3(const double2* __restrict__ V, co
 //         the reference's "extra previous step", source/main_loop.cpp:39-52).
 // ---------------------------------------------------------------------------
 template <typename C, int LM, int LM0>
-__global__ void __launch_bounds__(256, 2) k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
+__global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
                      double2* Nvp, double2* Nop, double2* rv, double2* ro,
                      const double* __restrict__ Ut, const double* __restrict__ ddUt,
                      DnsGeom g, PhysParams ph, FftTab<C> tabP, FftTab<double2> tab0,

@@ -34,7 +34,7 @@ __device__ __forceinline__ C* ppen(const PencilArr& a, int f, long long p) {
 // spanwise backward: pencils [f][kz*Kx+kx][y] -> rows [f][y][zp][kx]
 // ---------------------------------------------------------------------------
 template <typename C, int TX, int TY, int L>
-__global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
+__global__ void __launch_bounds__(256, 3) k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
@@ -80,7 +80,7 @@ __global__ void k_zb(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
 // spanwise forward: rows [f][y][zp][kx] -> pencils [f][kz*Kx+kx][y]
 // ---------------------------------------------------------------------------
 template <typename C, int TX, int TY, int L>
-__global__ void k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
+__global__ void __launch_bounds__(256, 3) k_zf(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
@@ -152,7 +152,7 @@ __device__ __forceinline__ C unpack_r2c(const C* Z, int k, int Px, bool imag_par
 // one wall-normal plane).
 // ---------------------------------------------------------------------------
 template <typename C, int L>
-__global__ void k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+__global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
                           const double* __restrict__ Uy, double Ro, int RB) {
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -314,8 +314,11 @@ __global__ void k_lamb_rows(const double* u, const double* v, const double* w,
 // host launchers
 // ---------------------------------------------------------------------------
 template <typename C> struct ZTile;
-template <> struct ZTile<double2> { enum { TX = 4, TY = 4 }; };
-template <> struct ZTile<float2> { enum { TX = 8, TY = 4 }; };
+// TX x TY lines per CTA: TX runs of the streamwise index (64 B) on the row
+// side, TY runs of the wall-normal index on the pencil side; small enough
+// for three CTAs per SM.
+template <> struct ZTile<double2> { enum { TX = 4, TY = 2 }; };
+template <> struct ZTile<float2> { enum { TX = 8, TY = 2 }; };
 
 template <typename C>
 cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {

@@ -39,8 +39,9 @@ void run(bool inv) {
     tw[j] = cmk<C>((double)cosl(a), (double)sinl(a));
     line[fpos(j)] = cmk<C>(std::sin(0.37 * j * j + 1.0), std::cos(1.3 * j) - 0.25);
   }
-  if (inv) HostDo<C, L, true, typename FftPlanL<L>::R>::go(line, tw);
-  else HostDo<C, L, false, typename FftPlanL<L>::R>::go(line, tw);
+  typedef typename FftPlanL<L, FftMaxRadix<C>::v>::R RS;
+  if (inv) HostDo<C, L, true, RS>::go(line, tw);
+  else HostDo<C, L, false, RS>::go(line, tw);
   for (int k = 0; k < L; ++k) printf("%.17g %.17g\n", (double)line[fpos(k)].x, (double)line[fpos(k)].y);
 }
 
