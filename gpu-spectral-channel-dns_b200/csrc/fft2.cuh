@@ -202,13 +202,22 @@ struct FftPass {
   DNS_HD static void load(const C* line, int j, C* v, const C* tw) {
     const int k = j % Ns;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      C x = line[fpos(j + r * NB)];
-      if (Ns > 1 && r > 0 && k > 0) {
-        const C w = tw[(r * k) * (L / (Ns * R))];
-        x = INV ? cmulc(x, w) : cmul(x, w);
+    for (int r = 0; r < R; ++r) v[r] = line[fpos(j + r * NB)];
+    if (Ns > 1 && k > 0) {
+      // FP64: W^r from one table load by products (error ~ r eps, far below
+      // the FP64 budget, and cheaper than R-1 loads through L1); FP32: exact
+      // table values for every r.
+      const C w1 = tw[k * (L / (Ns * R))];
+      C wr = w1;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        if (FftMaxRadix<C>::v == 8) {
+          if (r > 1) wr = cmul(wr, w1);
+        } else {
+          wr = tw[(r * k) * (L / (Ns * R))];
+        }
+        v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
       }
-      v[r] = x;
     }
     Codelet<R, INV, C>::run(v);
   }

@@ -38,7 +38,8 @@ __global__ void __launch_bounds__(256, 3) k_zb(PencilArr in, RowArr out, DnsGeom
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
-  const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int Pz = L > 0 ? L : g.Pz;
+  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
   const int ls = FL::stride(Pz);
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
@@ -84,7 +85,8 @@ __global__ void __launch_bounds__(256, 3) k_zf(RowArr in, PencilArr out, DnsGeom
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* lines = (C*)smem_raw;
-  const int Pz = g.Pz, Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int Pz = L > 0 ? L : g.Pz;
+  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
   const int ls = FL::stride(Pz);
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
@@ -153,68 +155,80 @@ __device__ __forceinline__ C unpack_r2c(const C* Z, int k, int Px, bool imag_par
 // ---------------------------------------------------------------------------
 template <typename C, int L>
 __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
-                          const double* __restrict__ Uy, double Ro, int RB) {
+                                                   const double* __restrict__ Uy, double Ro) {
+  // two rows per CTA: lines 0-2 hold row 0's packed fields (u,v) (ox,oy)
+  // (w,oz), lines 3-5 row 1's; after the inverse transform a thread owning
+  // point j of both rows writes lambda_x + i lambda_y of row 0 / row 1 into
+  // lines 0 / 1 and lambda_z(row 0) + i lambda_z(row 1) into line 2 at the
+  // same position, then lines 0-2 are transformed forward.
   typedef FLine<C, L> FL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
-  const int Px = g.Px;
+  const int Px = L > 0 ? L : g.Px;
   const int hx = g.Nx / 2;
   const int ls = FL::stride(Px);
-  C* zin = (C*)smem_raw;                // 3*RB lines
-  C* zout = zin + (size_t)3 * RB * ls;  // RB lines (lx + i ly) then RB/2 (lz pairs)
-  const long long r0 = (long long)blockIdx.x * RB;
+  C* z = (C*)smem_raw;  // 6 lines (9 for the runtime-length FFT)
+  const long long r0 = (long long)blockIdx.x * 2;
   const long long nrows = (long long)g.Py * g.Pz;
-  for (int t = threadIdx.x; t < RB * 3 * Px; t += blockDim.x) {
+  for (int t = threadIdx.x; t < 2 * 3 * Px; t += blockDim.x) {
     const int rl = t / (3 * Px);
     const int rem = t - rl * 3 * Px;
     const int q = rem / Px;
     const int n = rem - q * Px;
     const long long row = r0 + rl;
-    C z = cmk<C>(0.0, 0.0);
+    C zz = cmk<C>(0.0, 0.0);
     if (row < nrows) {
       // fields of similar magnitude share a transform (the smaller one's
       // rounding error is relative to the larger): (u, v), (ox, oy), (w, oz)
       const int fa = (q == 0) ? 0 : (q == 1 ? 3 : 2);
       const int fb = (q == 0) ? 1 : (q == 1 ? 4 : 5);
-      const C* a = prow<C>(in, fa, row);
-      const C* b = prow<C>(in, fb, row);
-      z = pack_c2r<C>(a, b, n, Px, hx);
+      zz = pack_c2r<C>(prow<C>(in, fa, row), prow<C>(in, fb, row), n, Px, hx);
     }
-    zin[(size_t)(rl * 3 + q) * ls + FL::in_pos(tab, n)] = z;
+    z[(size_t)(rl * 3 + q) * ls + FL::in_pos(tab, n)] = zz;
   }
-  FL::template fft<true>(zin, 3 * RB, ls, tab);
+  FL::template fft<true>(z, 6, ls, tab);
   const T ro = (T)Ro;
-  for (int t = threadIdx.x; t < RB * Px; t += blockDim.x) {
-    const int rl = t / Px;
-    const int j = t - rl * Px;
-    const long long row = r0 + rl;
-    const int y = (int)(row / g.Pz);
-    const T Ub = (row < nrows) ? (T)Uy[y] : (T)0;
+  const int y = (int)(r0 / g.Pz);  // both rows lie in one wall-normal plane
+  const T Ub = (T)Uy[y < g.Py ? y : 0];
+  for (int j = threadIdx.x; j < Px; j += blockDim.x) {
     const int op = FL::out_pos(j);
-    const C z0 = zin[(size_t)(rl * 3 + 0) * ls + op];
-    const C z1 = zin[(size_t)(rl * 3 + 1) * ls + op];
-    const C z2 = zin[(size_t)(rl * 3 + 2) * ls + op];
-    const T u = z0.x, v = z0.y, ox = z1.x, oy = z1.y, w = z2.x, oz = z2.y;
-    const T lx = oz * v - oy * w - ro * w;
-    const T ly = ox * w - oz * u;
-    const T lz = oy * u - ox * v + ro * (u + Ub);
-    const int pos = FL::in_pos(tab, j);
-    C A; A.x = lx; A.y = ly;
-    zout[(size_t)rl * ls + pos] = A;
-    T* B = (T*)(zout + (size_t)(RB + rl / 2) * ls + pos);
-    B[rl & 1] = lz;
+    T lz[2];
+    C A[2];
+#pragma unroll
+    for (int rl = 0; rl < 2; ++rl) {
+      const C z0 = z[(size_t)(rl * 3 + 0) * ls + op];
+      const C z1 = z[(size_t)(rl * 3 + 1) * ls + op];
+      const C z2 = z[(size_t)(rl * 3 + 2) * ls + op];
+      const T u = z0.x, v = z0.y, ox = z1.x, oy = z1.y, w = z2.x, oz = z2.y;
+      A[rl].x = oz * v - oy * w - ro * w;
+      A[rl].y = ox * w - oz * u;
+      lz[rl] = oy * u - ox * v + ro * (u + Ub);
+    }
+    if (L > 0) {  // natural order: write in place
+      z[(size_t)0 * ls + op] = A[0];
+      z[(size_t)1 * ls + op] = A[1];
+      C B; B.x = lz[0]; B.y = lz[1];
+      z[(size_t)2 * ls + op] = B;
+    } else {      // digit-reversed input order: separate lines 6-8
+      const int pos = FL::in_pos(tab, j);
+      z[(size_t)6 * ls + pos] = A[0];
+      z[(size_t)7 * ls + pos] = A[1];
+      C B; B.x = lz[0]; B.y = lz[1];
+      z[(size_t)8 * ls + pos] = B;
+    }
   }
-  FL::template fft<false>(zout, RB + RB / 2, ls, tab);
+  C* zf = (L > 0) ? z : z + (size_t)6 * ls;
+  FL::template fft<false>(zf, 3, ls, tab);
   const int Kx = g.Kx;
   const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
-  for (int t = threadIdx.x; t < RB * 3 * Kx; t += blockDim.x) {
+  for (int t = threadIdx.x; t < 2 * 3 * Kx; t += blockDim.x) {
     const int k = t % Kx;
     const int fl = (t / Kx) % 3;
     const int rl = t / (3 * Kx);
     const long long row = r0 + rl;
     if (row >= nrows) continue;
-    const C* Z = (fl < 2) ? zout + (size_t)rl * ls : zout + (size_t)(RB + rl / 2) * ls;
-    const bool im = (fl < 2) ? (fl == 1) : ((rl & 1) != 0);
+    const C* Z = (fl < 2) ? zf + (size_t)rl * ls : zf + (size_t)2 * ls;
+    const bool im = (fl < 2) ? (fl == 1) : (rl == 1);
     const C zk = Z[FL::out_pos(k)];
     const C zm = Z[FL::out_pos((Px - k) % Px)];
     C v;
@@ -347,13 +361,12 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
                            double Ro, cudaStream_t st) {
-  const int RB = 2;
   return with_len_xz(g.Px, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
-    const size_t sm = (size_t)(3 * RB + RB + RB / 2) * FLine<C, L>::stride(g.Px) * sizeof(C);
+    const size_t sm = (size_t)(L > 0 ? 6 : 9) * FLine<C, L>::stride(g.Px) * sizeof(C);
     cudaFuncSetAttribute(k_x_fused<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    const long long nrows = (long long)g.Py * g.Pz;
-    k_x_fused<C, L><<<(unsigned)((nrows + RB - 1) / RB), 256, sm, st>>>(in, out, g, tab, Uy, Ro, RB);
+    const long long nrows = (long long)g.Py * g.Pz;  // Pz is even: row pairs share a plane
+    k_x_fused<C, L><<<(unsigned)((nrows + 1) / 2), 256, sm, st>>>(in, out, g, tab, Uy, Ro);
     return cudaGetLastError();
   });
 }
