@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/dns_b200.h"
+#include "context_impl.cuh"
 #include "kernels.cuh"
 #include "setup.cuh"
 #include "ypass.cuh"
@@ -39,19 +40,6 @@ dns_status fail(dns_status s, const std::string& m) {
     cudaError_t e_ = (x);                                                                  \
     if (e_ != cudaSuccess) return fail(DNS_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
-
-template <typename C> struct DevFft {
-  FftPlan plan;
-  C* tw = nullptr;
-  short* drev = nullptr;
-  FftTab<C> tab() const {
-    FftTab<C> t;
-    t.plan = plan;
-    t.tw = tw;
-    t.drev = drev;
-    return t;
-  }
-};
 
 template <typename C> cudaError_t make_fft(int L, DevFft<C>& f) {
   if (!fft_make_plan(L, &f.plan)) return cudaErrorInvalidValue;
@@ -85,34 +73,6 @@ bool fft_len_ok(int L) {
 
 long long roundup(long long a, long long b) { return (a + b - 1) / b * b; }
 }  // namespace
-
-struct dns_ctx {
-  dns_params P;
-  DnsGeom g;
-  PhysParams ph;
-  cudaStream_t st = nullptr;
-  size_t bytes = 0;
-  long long PyS = 0, KxS = 0, RS = 0;
-  // tables
-  DevFft<double2> fz_d, fx_d, fyP_d, fy0_d;
-  DevFft<float2> fz_f, fx_f, fyP_f;
-  double *T0 = nullptr, *T2 = nullptr, *T4 = nullptr;
-  double *Ut = nullptr, *dUt = nullptr, *ddUt = nullptr, *Uy = nullptr;
-  // state
-  double2 *V = nullptr, *O = nullptr, *Nvp = nullptr, *Nop = nullptr, *rv = nullptr, *ro = nullptr;
-  double2* AT = nullptr;
-  void* F6 = nullptr;
-  void* G6 = nullptr;
-  double2* scratch = nullptr;
-  int* status = nullptr;
-  bool have_state = false, booted = false, inverses = false;
-  cudaGraphExec_t graph = nullptr;
-
-  template <typename T> cudaError_t alloc(T** p, size_t n) {
-    bytes += n * sizeof(T);
-    return cudaMalloc((void**)p, n * sizeof(T));
-  }
-};
 
 namespace {
 dns_status check_status(dns_ctx* c) {

@@ -1,0 +1,47 @@
+// Internal layout of dns_ctx, shared by the translation units that implement
+// the C ABI (context.cu, noalloc.cu).  Not part of the public interface.
+#pragma once
+#include "../../include/dns_b200.h"
+#include "kernels.cuh"
+
+template <typename C> struct DevFft {
+  FftPlan plan;
+  C* tw = nullptr;
+  short* drev = nullptr;
+  FftTab<C> tab() const {
+    FftTab<C> t;
+    t.plan = plan;
+    t.tw = tw;
+    t.drev = drev;
+    return t;
+  }
+};
+
+struct dns_ctx {
+  dns_params P;
+  DnsGeom g;
+  PhysParams ph;
+  cudaStream_t st = nullptr;
+  size_t bytes = 0;
+  long long PyS = 0, KxS = 0, RS = 0;
+  // tables
+  DevFft<double2> fz_d, fx_d, fyP_d, fy0_d;
+  DevFft<float2> fz_f, fx_f, fyP_f;
+  double *T0 = nullptr, *T2 = nullptr, *T4 = nullptr;
+  double *Ut = nullptr, *dUt = nullptr, *ddUt = nullptr, *Uy = nullptr;
+  // state
+  double2 *V = nullptr, *O = nullptr, *Nvp = nullptr, *Nop = nullptr, *rv = nullptr, *ro = nullptr;
+  double2* AT = nullptr;
+  void* F6 = nullptr;
+  void* G6 = nullptr;
+  double2* scratch = nullptr;
+  int* status = nullptr;
+  bool have_state = false, booted = false, inverses = false;
+  cudaGraphExec_t graph = nullptr;
+
+  template <typename T> cudaError_t alloc(T** p, size_t n) {
+    bytes += n * sizeof(T);
+    return cudaMalloc((void**)p, n * sizeof(T));
+  }
+};
+
