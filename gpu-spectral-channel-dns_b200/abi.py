@@ -27,7 +27,7 @@ EXPORTS = [
     "dns_kernel_name",
     "dns_transform_3d_one", "dns_transform", "dns_cuda_transpose", "dns_cheby_s2p",
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
-    "dns_init_aux_matrix",
+    "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
 ]
 
 
@@ -94,6 +94,7 @@ def load_library(path: str | None = None):
         "dns_step": [vp, i],
         "dns_step_profiled": [vp, i, C.POINTER(C.c_double)],
         "dns_transform_3d_one": [vp, i, vp, sz, vp, sz, i],
+        "dns_transform_3d_one_noalloc": [vp, i, vp, sz, vp, sz, i],
         "dns_transform": [vp, i, i, C.POINTER(vp), sz, C.POINTER(vp), sz],
         "dns_cuda_transpose": [vp, i, vp, sz, vp, sz],
         "dns_cheby_s2p": [vp, vp, sz, i],
@@ -241,6 +242,12 @@ class Context:
     # -- reference-layout entry points (device pointers as ints) -----------
     def transform_3d_one(self, direction, phys, pitch, spec, tpitch, pad=PADDING):
         self._call("dns_transform_3d_one", int(direction), C.c_void_p(phys), pitch,
+                   C.c_void_p(spec), tpitch, int(pad))
+
+    def transform_3d_one_noalloc(self, direction, phys, pitch, spec, tpitch, pad=PADDING):
+        """transform_3d_one without device allocation at call time (see the
+        header): same results, work buffer in a 16 MiB static device array."""
+        self._call("dns_transform_3d_one_noalloc", int(direction), C.c_void_p(phys), pitch,
                    C.c_void_p(spec), tpitch, int(pad))
 
     def transform(self, direction, phys, pitch, spec, tpitch):

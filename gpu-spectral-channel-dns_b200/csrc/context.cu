@@ -149,6 +149,8 @@ cudaMemcpyKind kind_of(int where, bool to_device) {
 }
 }  // namespace
 
+dns_status dns_internal_fail(dns_status s, const char* msg) { return fail(s, msg); }
+
 extern "C" {
 
 const char* dns_status_string(dns_status s) {

@@ -45,3 +45,6 @@ struct dns_ctx {
   }
 };
 
+
+// record an error message for dns_last_error() and return the status
+dns_status dns_internal_fail(dns_status s, const char* msg);

@@ -144,6 +144,19 @@ const char* dns_kernel_name(int k);
  * wall-normal points, DNS_NO_PADDING the nz points. */
 dns_status dns_transform_3d_one(dns_ctx* ctx, int dir, void* phys, size_t pitch, void* spec,
                                 size_t tpitch, int pad);
+/* No counterpart in the reference.  dns_transform_3d_one for callers that
+ * must not allocate device memory at call time (dns_transform_3d_one
+ * cudaMallocs a work buffer on first use; an application that has reserved
+ * nearly all device memory for itself, or a loop that cannot take the
+ * implicit device synchronisation of cudaMalloc, cannot allow that).  Same
+ * arguments and identical results; the work buffer is a 16 MiB static device
+ * array per GPU, so one wall-normal plane of streamwise rows
+ * (my * roundup(mx/2+1, 8) complex doubles) must fit, else DNS_ERR_ARG.
+ * Calls on one device share that buffer: calls that overlap on the GPU race.
+ * The first call on a device looks up the buffer's address; make it before
+ * any stream capture. */
+dns_status dns_transform_3d_one_noalloc(dns_ctx* ctx, int dir, void* phys, size_t pitch, void* spec,
+                                        size_t tpitch, int pad);
 /* transform (source/transform.cu:321-351): BACKWARD on six fields
  * (u, v, w, omega_x, omega_y, omega_z), FORWARD on three (lamb_z, lamb_y,
  * lamb_x order of the reference is immaterial). */
