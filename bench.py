@@ -303,8 +303,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
 
     if args.impl == "reference":
-        from oracle.ref_build import ref_arm  # noqa: WPS433 (test/baseline infrastructure)
+        # the reference's algorithm on the host (oracle port): rank 0 only
         if rank == 0:
+            sys.path.insert(0, ROOT)
+            from oracle import ref_arm
             print(json.dumps(ref_arm.run(args, CFG, METRIC)))
         return
 
