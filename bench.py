@@ -62,20 +62,36 @@ def load_pkg():
 # algorithmic bytes per kernel launch (one step), element size c (16 FP64 /
 # 8 FP32 complex); s = 16 (FP64 state / operator complex)
 # ---------------------------------------------------------------------------
-def kernel_bytes(g, c):
+WALL_BANDS = {0: (4, 8, 2, 4), 1: (5, 9, 3, 6), 2: (6, 10, 4, 8)}  # v kl, ku; omega kl, ku
+
+
+def wall_dims(g, U):
+    """Rows per pencil of the banded systems and bytes of the packed factors
+    (groups of 16 operator slots; v rows: kl + 1 + ku + 2 entries, omega
+    rows: kl + 1 + ku entries, complex FP64)."""
+    delta = 2 if U[2] else (1 if U[1] else 0)
+    klv, kuv, klo, kuo = WALL_BANDS[delta]
+    n = g["Ny"] + delta
+    slots = g["Kx"] * (g["Nz"] // 2 + 1)
+    groups = (slots + 15) // 16
+    per_group = 16 * (n * (klv + 1 + kuv + 2) + n * (klo + 1 + kuo))
+    return n, groups * per_group * 16
+
+
+def kernel_bytes(g, c, U=(0.5, 0.5, 0.0)):
     Kx, Nz, Ny, Py, Pz = g["Kx"], g["Nz"], g["Ny"], g["Py"], g["Pz"]
     H = Kx * Nz
     s = 16
-    slots = Kx * (Nz // 2 + 1)
+    n, fac = wall_dims(g, U)
     return {
         "y3_uvw_s2p": s * 2 * H * Ny + c * 6 * H * Py,
         "zb_span_inverse": c * 6 * H * Py + c * 6 * Kx * Pz * Py,
         "x_c2r_lamb_r2c": c * 6 * Kx * Pz * Py + c * 3 * Kx * Pz * Py,
         "zf_span_forward": c * 3 * Kx * Pz * Py + c * 3 * H * Py,
-        # lambda in; v, omega, history in; rhs and history out
-        "y1_p2s_rhs": c * 3 * H * Py + s * 4 * H * Ny + s * 4 * H * Ny,
-        # explicit inverses (v and omega, shared by +-kz), rhs and v^n in, state out
-        "y2_solve": s * 2 * slots * Ny * Ny + s * 3 * H * Ny + s * 2 * H * Ny,
+        # lambda in; v, omega, history in; history and the two integrated rhs out
+        "y1_p2s_rhs": c * 3 * H * Py + s * 4 * H * Ny + s * 2 * H * Ny + s * 2 * H * n,
+        # banded factors and the two integrated rhs in, v and omega out
+        "y2_solve": fac + s * 2 * H * n + s * 2 * H * Ny,
     }
 
 

@@ -1,7 +1,7 @@
 """Build libdnsb200.so in-tree for sm_100a with nvcc.
 
-``python build.py`` (or ``build()`` from Python) compiles every CUDA source
-under ``csrc/`` into ``libdnsb200.so`` next to this file.  The CUDA runtime
+``python build.py`` (or ``build()`` from Python) compiles every CUDA and C++
+source under ``csrc/`` into ``libdnsb200.so`` next to this file.  The CUDA runtime
 is linked statically, so the library needs only the driver at run time.
 """
 from __future__ import annotations
@@ -28,7 +28,7 @@ def _nvcc():
 
 
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def _stale():

@@ -1,4 +1,4 @@
-// dns_ctx: device buffers, FFT tables, operator inverses and the C ABI of
+// dns_ctx: device buffers, FFT tables, wall-normal solver factors and the C ABI of
 // libdnsb200.so (include/dns_b200.h).
 //
 // One context = one problem on one device, one CUDA stream, no host threads.
@@ -11,19 +11,23 @@
 //   x   streamwise C2R -> Lamb vector + rotation -> R2C
 //   zf  spanwise forward FFT with truncation, transpose back to pencils
 //   y1  p2s -> rhsNonlinear -> collocation values -> CN/AB2 right-hand sides
-//   y2  v solve, tilting term, omega solve (explicit inverses streamed)
+//       -> integrated right-hand sides of the banded systems
+//   y2  banded v solve, tilting term, banded omega solve (factors streamed)
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dns_b200.h"
 #include "context_impl.cuh"
 #include "kernels.cuh"
 #include "setup.cuh"
+#include "wallsolve.h"
 #include "ypass.cuh"
 #include "zxpass.cuh"
 
@@ -84,14 +88,36 @@ dns_status check_status(dns_ctx* c) {
   return DNS_OK;
 }
 
-dns_status build_inverses(dns_ctx* c) {
-  if (c->inverses) return DNS_OK;
-  const long long nunits = (long long)c->g.Kx * c->g.Kh;
-  CK(launch_gj_invert(0, 0, nunits, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt, c->AT,
-                      nullptr, nullptr, c->status, c->st));
-  dns_status s = check_status(c);
-  if (s != DNS_OK) return s;
-  c->inverses = true;
+// Factor the banded wall-normal systems of every operator slot on the host
+// threads and upload them (once per context, before the first step).
+dns_status build_wall_solver(dns_ctx* c) {
+  if (c->wall_ready) return DNS_OK;
+  const DnsGeom& g = c->g;
+  const int N = g.Ny - 1;
+  if (N < 8) return fail(DNS_ERR_ARG, "the time step needs Ny >= 9 (mz >= 32)");
+  WallDims& wd = c->wd;
+  int klv, kuv, klo, kuo;
+  if (!wall_band_of(wd.delta, &klv, &kuv, &klo, &kuo)) return fail(DNS_ERR_ARG, "base flow degree");
+  const wall::Shape sv{wd.nv, klv, kuv, 2}, so{wd.no, klo, kuo, 0};
+  const wall::Packing pk = wall::make_packing(sv, so);
+  wall::Grid gr{N, g.Kx, g.Nz, g.Kh, c->ph.aphi, c->ph.beta, c->ph.Re, c->ph.dt,
+                c->ph.U0, c->ph.U1, c->ph.U2};
+  std::vector<wall::cx> fac;
+  unsigned nt = std::thread::hardware_concurrency();
+  const std::string err = wall::pack_grid(gr, sv, so, fac, (int)std::min(32u, std::max(1u, nt)));
+  if (!err.empty()) return fail(DNS_ERR_SINGULAR, err);
+  std::vector<double> Q((size_t)7 * wd.no);
+  if (!wall::tilting_table(N, wd.no, c->ph.U1, c->ph.U2, Q.data()))
+    return fail(DNS_ERR_ARG, "tilting table outside its band");
+  wd.group_complex = pk.group_complex;
+  wd.nslots = (long long)g.Kx * g.Kh;
+  wd.ngroups = (wd.nslots + 15) / 16;
+  if (wall_smem_bytes(wd) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
+  CK(c->alloc(&c->wfac, fac.size()));
+  CK(c->alloc(&c->wQ, Q.size()));
+  CK(cudaMemcpy(c->wfac, fac.data(), fac.size() * 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->wQ, Q.data(), Q.size() * 8, cudaMemcpyHostToDevice));
+  c->wall_ready = true;
   return DNS_OK;
 }
 
@@ -119,13 +145,14 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   mark();
   if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
   mark();
-  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, c->Ut, c->ddUt, g, c->ph,
-                        fyP.tab(), c->fy0_d.tab(), boot, c->st)))
+  const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
+  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, c->Ut, c->dUt, c->ddUt,
+                        g, c->ph, fyP.tab(), c->fy0_d.tab(), boot, c->st)))
     return e;
   mark();
   if (!boot)
-    if ((e = launch_y2(c->AT, c->V, c->O, c->rv, c->ro, c->dUt, g, c->ph, c->fy0_d.tab(),
-                       c->status, c->st)))
+    if ((e = launch_wall_solve(c->wfac, c->V, c->O, c->rv, c->ro, c->wQ, c->wd, g, c->ph,
+                               c->status, c->st)))
       return e;
   mark();
   return cudaSuccess;
@@ -220,8 +247,6 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   if (!fft_len_ok(g.Px) || !fft_len_ok(g.Pz) || !fft_len_ok(p->mz) || !fft_len_ok(p->mz / 2))
     return fail(DNS_ERR_ARG, "mx, my, mz and mz/2 must be products of 2 and 3 (2^a 3^b)");
   if (g.Px < g.Nx || g.Pz < g.Nz) return fail(DNS_ERR_ARG, "padded sizes below mode counts");
-  if (gj_cluster_size(g.Ny) < 0) return fail(DNS_ERR_ARG, "Ny too large for the operator inversion");
-  if (2 * g.Ny > 1024) return fail(DNS_ERR_ARG, "Ny too large for the solve kernel");
 
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
@@ -265,14 +290,20 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   const size_t f6 = std::max((size_t)6 * g.H * c->PyS, (size_t)3 * g.Py * g.Pz * c->KxS);
   const size_t g6 = std::max((size_t)6 * g.Py * g.Pz * c->KxS, (size_t)3 * g.H * c->PyS);
   const size_t hn = (size_t)g.H * Ny;
+  // integrated right-hand sides: N + deg(U) + 1 rows per pencil
+  c->wd.delta = wall::base_degree(p->U1, p->U2);
+  c->wd.nv = c->wd.no = Ny + c->wd.delta;
+  c->wd.gp = c->wd.nv;
+  c->wd.SP = (std::max(c->wd.nv, c->wd.no) | 1);
+  c->wd.qbytes = (int)((7 * (size_t)c->wd.no * 8 + 15) & ~(size_t)15);
+  const size_t gn = (size_t)g.H * c->wd.gp;
   if ((e = c->alloc(&c->T0, NN)) || (e = c->alloc(&c->T2, NN)) || (e = c->alloc(&c->T4, NN)) ||
       (e = c->alloc(&c->Ut, Ny)) || (e = c->alloc(&c->dUt, Ny)) || (e = c->alloc(&c->ddUt, Ny)) ||
       (e = c->alloc(&c->Uy, g.Py)) || (e = c->alloc(&c->V, hn)) || (e = c->alloc(&c->O, hn)) ||
-      (e = c->alloc(&c->Nvp, hn)) || (e = c->alloc(&c->Nop, hn)) || (e = c->alloc(&c->rv, hn)) ||
-      (e = c->alloc(&c->ro, hn)) || (e = c->alloc(&c->status, 1)) ||
+      (e = c->alloc(&c->Nvp, hn)) || (e = c->alloc(&c->Nop, hn)) || (e = c->alloc(&c->rv, gn)) ||
+      (e = c->alloc(&c->ro, gn)) || (e = c->alloc(&c->status, 1)) ||
       (e = c->alloc((unsigned char**)&c->F6, f6 * csz)) ||
-      (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
-      (e = c->alloc(&c->AT, (size_t)g.Kx * g.Kh * 2 * NN)))
+      (e = c->alloc((unsigned char**)&c->G6, g6 * csz)))
     return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
   cudaMemcpy(c->T0, T0.data(), NN * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->T2, T2.data(), NN * 8, cudaMemcpyHostToDevice);
@@ -296,7 +327,7 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->AT, c->F6, c->G6, c->scratch, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->F6, c->G6, c->scratch, c->status};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -380,10 +411,8 @@ dns_status dns_bootstrap(dns_ctx* c) {
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (!c->have_state) return fail(DNS_ERR_STATE, "dns_set_state must precede dns_bootstrap");
   CK(cudaSetDevice(c->P.device));
-  dns_status s = build_inverses(c);
-  if (s != DNS_OK) return s;
   CK(enqueue(c, 1));
-  s = check_status(c);
+  dns_status s = check_status(c);
   if (s == DNS_OK) c->booted = true;
   return s;
 }
@@ -394,7 +423,7 @@ dns_status dns_step(dns_ctx* c, int nsteps) {
   if (!c->have_state || !c->booted)
     return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step");
   CK(cudaSetDevice(c->P.device));
-  dns_status s = build_inverses(c);
+  dns_status s = build_wall_solver(c);
   if (s != DNS_OK) return s;
   if (!c->graph) {
     cudaGraph_t gr;
@@ -416,7 +445,7 @@ dns_status dns_step_profiled(dns_ctx* c, int nsteps, double kernel_ms[DNS_NUM_KE
   if (!c->have_state || !c->booted)
     return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step_profiled");
   CK(cudaSetDevice(c->P.device));
-  dns_status s = build_inverses(c);
+  dns_status s = build_wall_solver(c);
   if (s != DNS_OK) return s;
   const int ne = DNS_NUM_KERNELS + 1;
   std::vector<cudaEvent_t> ev((size_t)ne * nsteps);
@@ -567,6 +596,7 @@ dns_status dns_init_aux_matrix(dns_ctx* c, void* inv_v, void* inv_o, int where) 
   if (!c || !inv_v || !inv_o) return fail(DNS_ERR_ARG, "null argument");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
   CK(cudaSetDevice(c->P.device));
+  if (gj_cluster_size(c->g.Ny) < 0) return fail(DNS_ERR_ARG, "Ny too large for the operator inversion");
   const long long NN = (long long)c->g.Ny * c->g.Ny;
   if (where == DNS_DEVICE) {
     CK(launch_gj_invert(1, 0, c->g.H, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt, nullptr,

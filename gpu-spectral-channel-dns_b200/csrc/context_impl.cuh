@@ -3,6 +3,7 @@
 #pragma once
 #include "../../include/dns_b200.h"
 #include "kernels.cuh"
+#include "wallsolve_dev.cuh"
 
 template <typename C> struct DevFft {
   FftPlan plan;
@@ -31,12 +32,15 @@ struct dns_ctx {
   double *Ut = nullptr, *dUt = nullptr, *ddUt = nullptr, *Uy = nullptr;
   // state
   double2 *V = nullptr, *O = nullptr, *Nvp = nullptr, *Nop = nullptr, *rv = nullptr, *ro = nullptr;
-  double2* AT = nullptr;
+  // banded wall-normal solve: packed factors, tilting table, dimensions
+  double2* wfac = nullptr;
+  double* wQ = nullptr;
+  WallDims wd{};
   void* F6 = nullptr;
   void* G6 = nullptr;
   double2* scratch = nullptr;
   int* status = nullptr;
-  bool have_state = false, booted = false, inverses = false;
+  bool have_state = false, booted = false, wall_ready = false;
   cudaGraphExec_t graph = nullptr;
 
   template <typename T> cudaError_t alloc(T** p, size_t n) {

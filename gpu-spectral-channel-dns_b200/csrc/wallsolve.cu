@@ -1,0 +1,350 @@
+// Per-step wall-normal solves (the y2 kernel): v solve, tilting term,
+// omega_y solve, for every Fourier mode, on the banded integrated systems of
+// wallsolve.h.  Replaces the reference's explicit-inverse products
+// (source/solver.cpp:107-123, matrix_op.cpp:68-78) and the tilting term of
+// _get_linear_omega_y (source/linear.cpp:147-151).
+//
+// One CTA = one warp = a group of 16 operator slots; lane 2q + b handles
+// pencil b (kz' or Nz - kz') of slot q, both pencils sharing the slot's
+// factors.  The factors of a group are stored as one contiguous stream in
+// the order the solve reads them (v forward rows, v backward rows, omega
+// forward rows, omega backward rows; each row holds its entries for the 16
+// slots side by side), and are streamed through a shared-memory ring with
+// cp.async.bulk and mbarriers.  Each lane keeps its right-hand side, the
+// intermediate solution and the tilting term in one shared-memory row.
+//
+// Inputs from the y1 kernel: g_v, g_o (rows K.. of the integrated
+// collocation right-hand sides, the v^n part of the tilting term included).
+// Outputs: V, O (Chebyshev coefficients of v^{n+1}, omega_y^{n+1}).
+#include "kernels.cuh"
+#include "mbar.cuh"
+#include "wallsolve_dev.cuh"
+
+#define WALL_WAIT_LIMIT (1LL << 31)
+
+namespace {
+
+constexpr int WALL_NST = 3;          // ring stages
+constexpr int WALL_STG = 12288;      // bytes per stage
+constexpr int WALL_HDR = 128;        // mbarriers
+
+__host__ __device__ constexpr int rows_per_chunk(int entries, int cap) {
+  return (WALL_STG / (entries * 256)) < cap ? (WALL_STG / (entries * 256)) : cap;
+}
+
+__device__ __forceinline__ double2 sel(bool p, double2 a) { return p ? a : make_double2(0.0, 0.0); }
+
+template <int KLV, int KUV, int KLO, int KUO>
+struct WallCfg {
+  static constexpr int E0 = KLV, E1 = 1 + KUV + 2, E2 = KLO, E3 = 1 + KUO;
+  static constexpr int R0 = rows_per_chunk(E0, 64), R1 = rows_per_chunk(E1, 64);
+  static constexpr int R2 = rows_per_chunk(E2, 16), R3 = rows_per_chunk(E3, 64);
+};
+
+// chunk c of a group's stream: byte count and offset (complex values)
+template <class CF>
+__device__ __forceinline__ void chunk_of(int c, const WallDims& wd, uint32_t& bytes, long long& off) {
+  const int n0 = (wd.nv + CF::R0 - 1) / CF::R0, n1 = (wd.nv + CF::R1 - 1) / CF::R1;
+  const int n2 = (wd.no + CF::R2 - 1) / CF::R2;
+  long long base;
+  int r0, rows, E;
+  if (c < n0) {
+    base = 0; E = CF::E0; r0 = c * CF::R0; rows = min(CF::R0, wd.nv - r0);
+  } else if (c < n0 + n1) {
+    base = 16LL * wd.nv * CF::E0; E = CF::E1; r0 = (c - n0) * CF::R1; rows = min(CF::R1, wd.nv - r0);
+  } else if (c < n0 + n1 + n2) {
+    base = 16LL * wd.nv * (CF::E0 + CF::E1); E = CF::E2; r0 = (c - n0 - n1) * CF::R2;
+    rows = min(CF::R2, wd.no - r0);
+  } else {
+    base = 16LL * (wd.nv * (CF::E0 + CF::E1) + wd.no * CF::E2); E = CF::E3;
+    r0 = (c - n0 - n1 - n2) * CF::R3; rows = min(CF::R3, wd.no - r0);
+  }
+  off = base + 16LL * r0 * E;
+  bytes = (uint32_t)(rows * E * 256);
+}
+
+}  // namespace
+
+template <int KLV, int KUV, int KLO, int KUO>
+__global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ fac, double2* V,
+                                                   double2* O, const double2* __restrict__ gv,
+                                                   const double2* __restrict__ go,
+                                                   const double* __restrict__ Qg, WallDims wd,
+                                                   DnsGeom g, PhysParams ph, int* status) {
+  typedef WallCfg<KLV, KUV, KLO, KUO> CF;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* full = (uint64_t*)smem_raw;
+  uint64_t* gbar = full + WALL_NST;
+  double2* ring = (double2*)(smem_raw + WALL_HDR);
+  double* Qs = (double*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG);
+  double2* S = (double2*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG + wd.qbytes);
+
+  const int lane = threadIdx.x;
+  const int q = lane >> 1, b = lane & 1;
+  const long long slot = (long long)blockIdx.x * 16 + q;
+  const bool valid = slot < wd.nslots;
+  const int kx = valid ? (int)(slot % g.Kx) : 0;
+  const int kzs = valid ? (int)(slot / g.Kx) : 0;
+  const int npen = (kzs == 0 || kzs == g.Nz / 2) ? 1 : 2;
+  const bool active = valid && b < npen;
+  const int kz = (b == 0) ? kzs : g.Nz - kzs;
+  const long long pen = (long long)kz * g.Kx + kx;
+  const bool zero = valid && slot == 0;
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kap = zero ? 0.0 : -0.5 * ib * ph.dt;  // tilting weight of this pencil
+  const int N = g.Ny - 1, Ny = g.Ny;
+  double2* Sr = S + (size_t)lane * wd.SP;
+  const double2* gfac = fac + (long long)blockIdx.x * wd.group_complex;
+  const int nch0 = (wd.nv + CF::R0 - 1) / CF::R0, nch1 = (wd.nv + CF::R1 - 1) / CF::R1;
+  const int nch2 = (wd.no + CF::R2 - 1) / CF::R2, nch3 = (wd.no + CF::R3 - 1) / CF::R3;
+  const int total = nch0 + nch1 + nch2 + nch3;
+
+  auto issue = [&](int c) {
+    uint32_t bytes;
+    long long off;
+    chunk_of<CF>(c, wd, bytes, off);
+    uint64_t* bar = &full[c % WALL_NST];
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(ring + (size_t)(c % WALL_NST) * (WALL_STG / 16), gfac + off, bytes, bar);
+  };
+  // on a timed-out wait: report, let the copies in flight land, leave
+  auto abort_at = [&](int c) {
+    if (lane == 0) {
+      atomicOr(status, 1);
+      for (int cc = c; cc < min(c + WALL_NST, total); ++cc)
+        mbar_wait_bounded(&full[cc % WALL_NST], (uint32_t)((cc / WALL_NST) & 1), WALL_WAIT_LIMIT, nullptr);
+    }
+  };
+  auto wait_chunk = [&](int c) {
+    const bool ok = mbar_wait_bounded(&full[c % WALL_NST], (uint32_t)((c / WALL_NST) & 1),
+                                      WALL_WAIT_LIMIT, status);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto release = [&](int c) {
+    __syncwarp();
+    if (lane == 0 && c + WALL_NST < total) {
+      fence_proxy_async();
+      issue(c + WALL_NST);
+    }
+  };
+
+  // ---- start: barriers, ring prefetch, right-hand sides of v -------------
+  const unsigned amask = __ballot_sync(0xffffffffu, active);
+  if (lane == 0) {
+    for (int s = 0; s < WALL_NST; ++s) mbar_init(&full[s], 1);
+    mbar_init(gbar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  for (int k = lane; k < 7 * wd.no; k += 32) Qs[k] = Qg[k];
+  if (lane == 0) {
+    mbar_expect_tx(gbar, (uint32_t)(__popc(amask) * wd.nv * 16));
+    for (int c = 0; c < min(WALL_NST, total); ++c) issue(c);
+  }
+  __syncwarp();
+  if (active) bulk_g2s(Sr, gv + pen * wd.gp, (uint32_t)(wd.nv * 16), gbar);
+  else
+    for (int i = 0; i < wd.nv; ++i) Sr[i] = make_double2(0.0, 0.0);
+  {
+    const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(gbar, 0, WALL_WAIT_LIMIT, status));
+    if (!ok) {
+      if (lane == 0) mbar_wait_bounded(gbar, 0, WALL_WAIT_LIMIT, nullptr);
+      abort_at(0);
+      return;
+    }
+  }
+  __syncwarp();
+
+  int c = 0;
+  // ---- v: forward substitution (unit lower band) -------------------------
+  {
+    double2 yw[KLV];
+#pragma unroll
+    for (int e = 0; e < KLV; ++e) yw[e] = make_double2(0.0, 0.0);
+    for (int r0 = 0; r0 < wd.nv; r0 += CF::R0, ++c) {
+      if (!wait_chunk(c)) { abort_at(c); return; }
+      const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
+      const int rows = min(CF::R0, wd.nv - r0);
+      for (int rr = 0; rr < rows; ++rr) {
+        const int i = r0 + rr;
+        const double2* Lr = ch + rr * CF::E0 * 16;
+        double2 acc = Sr[i];
+#pragma unroll
+        for (int e = 0; e < KLV; ++e) acc = acc - cmul(Lr[e * 16], yw[e]);
+        Sr[i] = acc;
+#pragma unroll
+        for (int e = 0; e < KLV - 1; ++e) yw[e] = yw[e + 1];
+        yw[KLV - 1] = acc;
+      }
+      release(c);
+    }
+  }
+  // ---- v: back substitution, recombination, tilting term -----------------
+  {
+    double2 xw[KUV];
+#pragma unroll
+    for (int e = 0; e < KUV; ++e) xw[e] = make_double2(0.0, 0.0);
+    double2 xd0 = make_double2(0.0, 0.0), xd1 = make_double2(0.0, 0.0);
+    double2 P[7];  // P[j]: partial tilting sum of row k+1-j, k = next coefficient emitted
+#pragma unroll
+    for (int j = 0; j < 7; ++j) P[j] = make_double2(0.0, 0.0);
+    const int nbv = zero ? N - 1 : N - 3;
+    auto emit = [&](int k, double2 a) {
+      if (active) V[pen * Ny + k] = a;
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        const int r = k + 1 - j;
+        if (r >= 0 && r < wd.no) P[j] = P[j] + a * Qs[7 * r + j];
+      }
+      if (k + 1 < wd.no) Sr[k + 1] = muli(P[0] * kap);
+#pragma unroll
+      for (int j = 0; j < 6; ++j) P[j] = P[j + 1];
+      P[6] = make_double2(0.0, 0.0);
+    };
+    for (int r0 = 0; r0 < wd.nv; r0 += CF::R1, ++c) {
+      if (!wait_chunk(c)) { abort_at(c); return; }
+      const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
+      const int rows = min(CF::R1, wd.nv - r0);
+      for (int rr = 0; rr < rows; ++rr) {
+        const int i = wd.nv - 1 - (r0 + rr);
+        const double2* Ur = ch + rr * CF::E1 * 16;
+        double2 acc = Sr[i];
+        if (i >= N + 2) Sr[i] = make_double2(0.0, 0.0);  // no tilting term above row N+1
+        acc = acc - cmul(Ur[(KUV + 1) * 16], xd0) - cmul(Ur[(KUV + 2) * 16], xd1);
+#pragma unroll
+        for (int e = KUV; e >= 1; --e) acc = acc - cmul(Ur[e * 16], xw[e - 1]);
+        const double2 x = cmul(Ur[0], acc);
+        if (i == wd.nv - 1) xd1 = x;
+        if (i == wd.nv - 2) xd0 = x;
+#pragma unroll
+        for (int e = KUV - 1; e >= 1; --e) xw[e] = xw[e - 1];
+        xw[0] = x;
+        if (i < nbv) {
+          if (!zero) {
+            const int k = i + 4;
+            emit(k, sel(i + 4 < nbv, xw[4]) - sel(i + 2 < nbv, xw[2]) * (2.0 * k / (k + 1)) +
+                        x * ((double)(i + 1) / (double)(i + 3)));
+          } else {
+            emit(i + 2, x - sel(i + 2 < nbv, xw[2]));
+          }
+        }
+      }
+      release(c);
+    }
+    if (!zero) {
+      emit(3, xw[3] - xw[1] * 1.5);
+      emit(2, xw[2] - xw[0] * (4.0 / 3.0));
+      emit(1, xw[1]);
+      emit(0, xw[0]);
+    } else {
+      emit(1, make_double2(-xw[1].x, -xw[1].y));
+      emit(0, make_double2(-xw[0].x, -xw[0].y));
+    }
+    Sr[0] = muli(P[0] * kap);
+  }
+  // ---- omega: forward substitution (adds g_o to the tilting term) --------
+  {
+    constexpr int R2 = CF::R2;
+    double2 ow[KLO];
+#pragma unroll
+    for (int e = 0; e < KLO; ++e) ow[e] = make_double2(0.0, 0.0);
+    const double2* gop = go + pen * wd.gp;
+    double2 gnext[R2];
+#pragma unroll
+    for (int rr = 0; rr < R2; ++rr)
+      gnext[rr] = (active && rr < wd.no) ? __ldg(gop + rr) : make_double2(0.0, 0.0);
+    for (int r0 = 0; r0 < wd.no; r0 += R2, ++c) {
+      double2 gcur[R2];
+#pragma unroll
+      for (int rr = 0; rr < R2; ++rr) gcur[rr] = gnext[rr];
+#pragma unroll
+      for (int rr = 0; rr < R2; ++rr) {
+        const int i = r0 + R2 + rr;
+        gnext[rr] = (active && i < wd.no) ? __ldg(gop + i) : make_double2(0.0, 0.0);
+      }
+      if (!wait_chunk(c)) { abort_at(c); return; }
+      const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
+      const int rows = min(R2, wd.no - r0);
+#pragma unroll
+      for (int rr = 0; rr < R2; ++rr) {
+        if (rr < rows) {
+          const int i = r0 + rr;
+          const double2* Lr = ch + rr * CF::E2 * 16;
+          double2 acc = Sr[i] + gcur[rr];
+#pragma unroll
+          for (int e = 0; e < KLO; ++e) acc = acc - cmul(Lr[e * 16], ow[e]);
+          Sr[i] = acc;
+#pragma unroll
+          for (int e = 0; e < KLO - 1; ++e) ow[e] = ow[e + 1];
+          ow[KLO - 1] = acc;
+        }
+      }
+      release(c);
+    }
+  }
+  // ---- omega: back substitution and recombination ------------------------
+  {
+    double2 zw[KUO];
+#pragma unroll
+    for (int e = 0; e < KUO; ++e) zw[e] = make_double2(0.0, 0.0);
+    const int nbo = N - 1;
+    for (int r0 = 0; r0 < wd.no; r0 += CF::R3, ++c) {
+      if (!wait_chunk(c)) { abort_at(c); return; }
+      const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
+      const int rows = min(CF::R3, wd.no - r0);
+      for (int rr = 0; rr < rows; ++rr) {
+        const int i = wd.no - 1 - (r0 + rr);
+        const double2* Ur = ch + rr * CF::E3 * 16;
+        double2 acc = Sr[i];
+#pragma unroll
+        for (int e = KUO; e >= 1; --e) acc = acc - cmul(Ur[e * 16], zw[e - 1]);
+        const double2 x = cmul(Ur[0], acc);
+#pragma unroll
+        for (int e = KUO - 1; e >= 1; --e) zw[e] = zw[e - 1];
+        zw[0] = x;
+        if (i < nbo && active) O[pen * Ny + i + 2] = x - sel(i + 2 < nbo, zw[2]);
+      }
+      release(c);
+    }
+    if (active) {
+      O[pen * Ny + 1] = make_double2(-zw[1].x, -zw[1].y);
+      O[pen * Ny + 0] = make_double2(-zw[0].x, -zw[0].y);
+    }
+  }
+}
+
+size_t wall_smem_bytes(const WallDims& wd) {
+  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)32 * wd.SP * 16;
+}
+
+// band instances: base-flow degree 0, 1, 2
+bool wall_band_of(int delta, int* klv, int* kuv, int* klo, int* kuo) {
+  static const int tab[3][4] = {{4, 8, 2, 4}, {5, 9, 3, 6}, {6, 10, 4, 8}};
+  if (delta < 0 || delta > 2) return false;
+  *klv = tab[delta][0]; *kuv = tab[delta][1]; *klo = tab[delta][2]; *kuo = tab[delta][3];
+  return true;
+}
+
+template <int A, int B, int C, int D>
+static cudaError_t launch_inst(const double2* fac, double2* V, double2* O, const double2* gv,
+                               const double2* go, const double* Q, const WallDims& wd,
+                               const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
+  const size_t sm = wall_smem_bytes(wd);
+  cudaError_t e = cudaFuncSetAttribute(k_wall_solve<A, B, C, D>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e) return e;
+  k_wall_solve<A, B, C, D><<<(unsigned)wd.ngroups, 32, sm, st>>>(fac, V, O, gv, go, Q, wd, g, ph, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const double2* gv,
+                              const double2* go, const double* Q, const WallDims& wd,
+                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
+  switch (wd.delta) {
+    case 0: return launch_inst<4, 8, 2, 4>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
+    case 1: return launch_inst<5, 9, 3, 6>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
+    case 2: return launch_inst<6, 10, 4, 8>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
+  }
+  return cudaErrorInvalidValue;
+}

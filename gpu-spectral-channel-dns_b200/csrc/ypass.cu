@@ -9,6 +9,8 @@
 //   _get_linear_v / _omega_y / u0  source/linear.cpp:86-205
 //   AB2 add ...................... source/rhs.cpp:205-215
 //   solveEq / m_multi_v .......... source/solver.cpp:107-123, matrix_op.cpp:68-78
+//                                  (reference-layout op; the time step solves
+//                                  the banded systems of wallsolve.cu)
 //
 // The Chebyshev transforms are DCT-I evaluated as complex FFTs of the even
 // extension, as the reference does with cuFFT, but in shared memory with the
@@ -364,14 +366,20 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
 // ---------------------------------------------------------------------------
 // Fused forward wall-normal pass: padded p2s of the three Lamb components,
 // rhsNonlinear, no-pad s2p to collocation values, then (unless boot) the
-// CN explicit operators and AB2 for v, omega_y and the mean modes.
+// CN explicit operators, AB2 and the v^n half of the tilting term for v,
+// omega_y and the mean modes at the collocation points; finally the values
+// (zero at the points an equation does not use) go back to coefficients
+// (no-pad p2s) and are integrated K times (K = 4 for v, 2 for omega_y and
+// the mean modes): the right-hand sides of the banded systems of
+// wallsolve.h, rows K .. K+n-1.
 //   boot: only store the nonlinear terms as the AB2 history (the effect of
 //         the reference's "extra previous step", source/main_loop.cpp:39-52).
 // ---------------------------------------------------------------------------
 template <typename C, int LM, int LM0>
 __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
-                     double2* Nvp, double2* Nop, double2* rv, double2* ro,
-                     const double* __restrict__ Ut, const double* __restrict__ ddUt,
+                     double2* Nvp, double2* Nop, double2* gv, double2* go, RhsDims rd,
+                     const double* __restrict__ Ut, const double* __restrict__ dUt,
+                     const double* __restrict__ ddUt,
                      DnsGeom g, PhysParams ph, FftTab<C> tabP, FftTab<double2> tab0,
                      int boot) {
   typedef FLine<C, LM> FP;
@@ -384,18 +392,21 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   const int lsP = FP::stride(M);
   const int ls0 = F0::stride(M0);
   Carve cv(smem_raw);
-  double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients
-  double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
-  double2* Hv = cv.take<double2>(Ny);
-  double2* Ho = cv.take<double2>(Ny);
-  double2* Vc = cv.take<double2>(Ny);
-  double2* Oc = cv.take<double2>(Ny);
-  double2* t1 = cv.take<double2>(Ny);
-  double2* t3 = cv.take<double2>(Ny);
-  double2* D2V = cv.take<double2>(Ny);
-  double2* D2O = cv.take<double2>(Ny);
-  double2* t2 = cv.take<double2>(Ny);
-  double2* D4V = cv.take<double2>(Ny);
+  // work region of 15 Ny: coefficient-space arrays, reused at the end for the
+  // right-hand-side values and their integration
+  double2* wk = cv.take<double2>((size_t)15 * Ny);
+  double2* lc = wk;              // lambda coefficients (3 Ny)
+  double2* D1 = wk + 3 * Ny;     // D lambda_x, D lambda_y (2 Ny)
+  double2* Hv = wk + 5 * Ny;
+  double2* Ho = wk + 6 * Ny;
+  double2* Vc = wk + 7 * Ny;
+  double2* Oc = wk + 8 * Ny;
+  double2* t1 = wk + 9 * Ny;
+  double2* t3 = wk + 10 * Ny;
+  double2* D2V = wk + 11 * Ny;
+  double2* D2O = wk + 12 * Ny;
+  double2* t2 = wk + 13 * Ny;
+  double2* D4V = wk + 14 * Ny;
   double2* nvp = cv.take<double2>(Ny);
   double2* nop = cv.take<double2>(Ny);
   const size_t bytesP = (size_t)3 * lsP * sizeof(C);
@@ -483,6 +494,9 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   }
   const double dt = ph.dt, Re = ph.Re, al = ia;
   const int N = Ny - 1;
+  const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
+  double2* vv = wk;        // collocation values of the v (mean: u0) right-hand side
+  double2* vo = wk + Ny;   // ... of the omega_y (mean: w0) right-hand side
   // lines: 0 Nv, 1 No, 2 v, 3 v'', 4 v(4), 5 omega, 6 omega''
   for (int i = threadIdx.x; i < Ny; i += blockDim.x) {
     double2 rvi = make_double2(0.0, 0.0), roi = make_double2(0.0, 0.0);
@@ -492,6 +506,8 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
         const int m = i - 1;
         rvi = col(2, m) + col(3, m) * (dt * 0.5 / Re) - (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
         roi = col(5, m) + col(6, m) * (dt * 0.5 / Re) - (col(1, m) * 1.5 - nop[m] * 0.5) * dt;
+        vv[m] = rvi;
+        vo[m] = roi;
       }
     } else {
       if (i >= 4 && i <= N) {
@@ -503,200 +519,75 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
         const double2 im = P2 * (-al * dt * 0.5 * Um)
                            + P0 * (kmn * al * dt * 0.5 * Um + al * dt * 0.5 * ddUt[m]);
         rvi = re + muli(im) + (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
+        vv[m] = rvi;
       }
       if (i >= 2) {
         const int m = i - 1;
         const double2 Q0 = col(5, m), Q2 = col(6, m);
         const double2 re = Q2 * (0.5 / Re * dt) + Q0 * (1 - kmn * dt * 0.5 / Re);
         const double2 im = Q0 * (-al * dt * 0.5 * Ut[m]);
-        roi = re + muli(im) + (col(1, m) * 1.5 - nop[m] * 0.5) * dt;
+        roi = re + muli(im) + (col(1, m) * 1.5 - nop[m] * 0.5) * dt + muli(col(2, m) * (kap * dUt[m]));
+        vo[m] = roi;
       }
     }
-    rv[p * Ny + i] = rvi;
-    ro[p * Ny + i] = roi;
     Nvp[p * Ny + i] = col(0, i);
     Nop[p * Ny + i] = col(1, i);
   }
-}
-
-// ---------------------------------------------------------------------------
-// Per-mode solves.  One CTA per operator slot (kx, kz'), kz' in [0, Nz/2];
-// the operator depends on kz only through beta^2, so pencils kz' and Nz-kz'
-// share it.  Explicit inverses are stored transposed, AT[slot][eq][j][i],
-// and streamed through a shared-memory ring with cp.async.bulk + mbarrier.
-// Between the v and omega solves the tilting term -i beta U' dt/2 (v^{n+1}
-// + v^n) of source/linear.cpp:147-151 is added at the collocation points.
-// ---------------------------------------------------------------------------
-namespace {
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-// Bounded wait: gives up after `limit` SM clock cycles (about a second), or
-// at once when another CTA has already reported a timeout in *status
-// (status == nullptr: no early exit, used to drain copies in flight).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit,
-                                                  const int* status) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > limit) return false;
-    if (status && (*(volatile const int*)status & 1)) return false;
-  }
-  return true;
-}
-}  // namespace
-
-#define Y2_WAIT_LIMIT (1LL << 31)
-
-template <int LM0>
-__global__ void k_y2(const double2* __restrict__ AT, double2* V, double2* O,
-                     const double2* __restrict__ rv, const double2* __restrict__ ro,
-                     const double* __restrict__ dUt, DnsGeom g, PhysParams ph,
-                     FftTab<double2> tab0, int CH, int NST, int* status) {
-  typedef FLine<double2, LM0> F0;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Ny = g.Ny;
-  const int M0 = tab0.plan.L;
-  const int ls0 = F0::stride(M0);
-  Carve cv(smem_raw);
-  uint64_t* full = cv.take<uint64_t>(NST);
-  double2* ring = cv.take<double2>((size_t)NST * CH * Ny);
-  double2* r = cv.take<double2>((size_t)2 * Ny);    // current right-hand sides
-  double2* ro_s = cv.take<double2>((size_t)2 * Ny); // omega right-hand sides
-  double2* vold = cv.take<double2>((size_t)2 * Ny);
-  double2* xv = cv.take<double2>((size_t)2 * Ny);
-  double2* lines = cv.take<double2>((size_t)2 * ls0);
-
-  const int kx = blockIdx.x % g.Kx;
-  const int kzs = blockIdx.x / g.Kx;  // slot kz' in [0, Nz/2]
-  const long long slot = blockIdx.x;
-  const int npen = (kzs == 0 || kzs == g.Nz / 2) ? 1 : 2;
-  long long pen[2];
-  pen[0] = (long long)kzs * g.Kx + kx;
-  pen[1] = (long long)(g.Nz - kzs) * g.Kx + kx;
-  const bool zero = (kx == 0 && kzs == 0);
-  const long long NN = (long long)Ny * Ny;
-  const double2* Av = AT + slot * 2 * NN;
-  const double2* Ao = Av + NN;
-  const int nch = (Ny + CH - 1) / CH;
-  const int nchunks = 2 * nch;
-  const int tid = threadIdx.x;
-
-  if (tid == 0) {
-    for (int s = 0; s < NST; ++s) mbar_init(&full[s], 1);
-    fence_mbar_init();
-  }
-  for (int t = tid; t < npen * Ny; t += blockDim.x) {
-    const int b = t / Ny;
-    const int n = t - b * Ny;
-    r[t] = rv[pen[b] * Ny + n];
-    ro_s[t] = ro[pen[b] * Ny + n];
-    vold[t] = V[pen[b] * Ny + n];
+  if (threadIdx.x == 0) {
+    const double2 z = make_double2(0.0, 0.0);
+    vv[0] = z; vv[N] = z; vo[0] = z; vo[N] = z;
+    if (!zero) { vv[1] = z; vv[N - 1] = z; }
   }
   __syncthreads();
-  auto issue = [&](int c) {
-    const int s = c % NST;
-    const int e = c / nch;
-    const int j0 = (c - e * nch) * CH;
-    const int ncol = min(CH, Ny - j0);
-    const uint32_t bytes = (uint32_t)(ncol * Ny * sizeof(double2));
-    const double2* src = (e == 0 ? Av : Ao) + (long long)j0 * Ny;
-    mbar_expect_tx(&full[s], bytes);
-    bulk_g2s(ring + (size_t)s * CH * Ny, src, bytes, &full[s]);
-  };
-  if (tid == 0)
-    for (int c = 0; c < min(NST, nchunks); ++c) issue(c);
-
-  const int b = tid / Ny;        // right-hand side handled by this thread
-  const int i = tid - b * Ny;    // output row
-  const bool active = (b < npen);
-  double2 acc = make_double2(0.0, 0.0);
-  for (int c = 0; c < nchunks; ++c) {
-    if (c == nch) {
-      // v solved: keep it, then add the tilting term to the omega rhs
-      if (active) xv[b * Ny + i] = acc;
-      acc = make_double2(0.0, 0.0);
-      __syncthreads();
-      if (!zero) {
-        for (int t = tid; t < npen * M0; t += blockDim.x) {
-          const int bb = t / M0;
-          const int n = t - bb * M0;
-          // S = v^{n+1} + v^n, even extension for the no-pad s2p
-          int src;
-          double sc;
-          if (n == 0) { src = 0; sc = 1.0; }
-          else if (n < Ny - 1) { src = n; sc = 0.5; }
-          else if (n == Ny - 1) { src = n; sc = 1.0; }
-          else { src = M0 - n; sc = 0.5; }
-          const double2 sv = (xv[bb * Ny + src] + vold[bb * Ny + src]) * sc;
-          lines[(size_t)bb * ls0 + F0::in_pos(tab0, n)] = sv;
-        }
-        F0::template fft<false>(lines, npen, ls0, tab0);
-        if (active && i >= 2) {
-          const int m = i - 1;
-          const int kzp = (b == 0) ? kzs : g.Nz - kzs;
-          double iab, ibb;
-          wavenumbers(kx, kzp, g.Nz, ph.aphi, ph.beta, iab, ibb);
-          const double coef = -0.5 * ibb * dUt[m] * ph.dt;
-          ro_s[b * Ny + i] = ro_s[b * Ny + i] + muli(lines[(size_t)b * ls0 + F0::out_pos(m)] * coef);
-        }
-      }
-      __syncthreads();
-    }
-    const int s = c % NST;
-    const uint32_t par = (uint32_t)((c / NST) & 1);
-    const bool ok = mbar_wait_bounded(&full[s], par, Y2_WAIT_LIMIT, status);
-    const int e = c / nch;
-    const int j0 = (c - e * nch) * CH;
-    const int ncol = min(CH, Ny - j0);
-    if (ok && active) {
-      const double2* rr = (e == 0 ? r : ro_s) + b * Ny + j0;
-      const double2* A = ring + (size_t)s * CH * Ny;
-      double ar = acc.x, ai = acc.y;
-      for (int jj = 0; jj < ncol; ++jj) {
-        const double2 a = A[jj * Ny + i];
-        const double2 x = rr[jj];
-        ar += a.x * x.x - a.y * x.y;
-        ai += a.x * x.y + a.y * x.x;
-      }
-      acc = make_double2(ar, ai);
-    }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicOr(status, 1);
-        // let the copies already in flight land before the CTA exits
-        for (int cc = c; cc < min(c + NST, nchunks); ++cc)
-          mbar_wait_bounded(&full[cc % NST], (uint32_t)((cc / NST) & 1), Y2_WAIT_LIMIT, nullptr);
-      }
-      return;
-    }
-    if (tid == 0 && c + NST < nchunks) issue(c + NST);
+  // no-pad p2s of the two value vectors (even extension, FFT, 1/N, ends halved)
+  for (int t = threadIdx.x; t < 2 * M0; t += blockDim.x) {
+    const int f = t / M0;
+    const int n = t - f * M0;
+    const double2* src = f ? vo : vv;
+    lines0[(size_t)f * ls0 + F0::in_pos(tab0, n)] = (n <= N) ? src[n] : src[M0 - n];
   }
-  if (active) {
-    V[pen[b] * Ny + i] = xv[b * Ny + i];
-    O[pen[b] * Ny + i] = acc;
+  F0::template fft<false>(lines0, 2, ls0, tab0);
+  const int LB = Ny + 8;
+  double2* av = wk + 2 * Ny;
+  double2* bv = av + LB;
+  double2* ao = bv + LB;
+  double2* bo = ao + LB;
+  for (int t = threadIdx.x; t < 2 * LB; t += blockDim.x) {
+    const int f = t / LB;
+    const int k = t - f * LB;
+    double2 cval = make_double2(0.0, 0.0);
+    if (k <= N) {
+      cval = lines0[(size_t)f * ls0 + F0::out_pos(k)] * (1.0 / N);
+      if (k == 0 || k == N) cval = cval * 0.5;
+    }
+    (f ? ao : av)[k] = cval;
   }
+  __syncthreads();
+  // Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  const int Kv = zero ? 2 : 4;
+  for (int it = 0; it < Kv; ++it) {
+    const int nf = (it < 2) ? 2 : 1;
+    for (int t = threadIdx.x; t < nf * LB; t += blockDim.x) {
+      const int f = t / LB;
+      const int k = t - f * LB;
+      const double2* x = f ? ao : av;
+      double2* y = f ? bo : bv;
+      double2 r = make_double2(0.0, 0.0);
+      if (k >= 1) {
+        const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
+        const double2 xp = (k + 1 < LB) ? x[k + 1] : make_double2(0.0, 0.0);
+        r = (xm - xp) * (1.0 / (2.0 * k));
+      }
+      y[k] = r;
+    }
+    __syncthreads();
+    double2* tmp = av; av = bv; bv = tmp;
+    if (it < 2) { tmp = ao; ao = bo; bo = tmp; }
+  }
+  for (int r = threadIdx.x; r < rd.nv; r += blockDim.x)
+    gv[p * rd.gp + r] = (Kv + r < LB) ? av[Kv + r] : make_double2(0.0, 0.0);
+  for (int r = threadIdx.x; r < rd.no; r += blockDim.x)
+    go[p * rd.gp + r] = (2 + r < LB) ? ao[2 + r] : make_double2(0.0, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -712,12 +603,6 @@ size_t y1_smem(int Ny, int lsP, int ls0, size_t csz) {
   size_t bp = (size_t)3 * lsP * csz, b0 = (size_t)7 * ls0 * 16;
   return s + a(bp > b0 ? bp : b0);
 }
-size_t y2_smem(int Ny, int ls0, int CH, int NST) {
-  auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
-  return a((size_t)NST * 8) + a((size_t)NST * CH * Ny * 16) + 4 * a((size_t)2 * Ny * 16) +
-         a((size_t)2 * ls0 * 16);
-}
-
 template <typename C>
 cudaError_t launch_cheby_inplace(PencilArr arr, long long npencils, int mode, int Ny,
                                  FftTab<C> tab, cudaStream_t st) {
@@ -776,38 +661,19 @@ template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr
 
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
-                      double2* Nop, double2* rv, double2* ro, const double* Ut,
-                      const double* ddUt, DnsGeom g, PhysParams ph, FftTab<C> tabP,
-                      FftTab<double2> tab0, int boot, cudaStream_t st) {
+                      double2* Nop, double2* gv, double2* go, RhsDims rd, const double* Ut,
+                      const double* dUt, const double* ddUt, DnsGeom g, PhysParams ph,
+                      FftTab<C> tabP, FftTab<double2> tab0, int boot, cudaStream_t st) {
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     constexpr int L0 = L / 2;  // the no-pad extension is half the padded one
     const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L),
                               FLine<double2, L0>::stride(tab0.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y1<C, L, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_y1<C, L, L0><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, rv, ro, Ut, ddUt, g, ph,
-                                                   tabP, tab0, boot);
+    k_y1<C, L, L0><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, Ut, dUt, ddUt,
+                                                   g, ph, tabP, tab0, boot);
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, const double*, const double*, DnsGeom, PhysParams, FftTab<double2>, FftTab<double2>, int, cudaStream_t);
-template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, const double*, const double*, DnsGeom, PhysParams, FftTab<float2>, FftTab<double2>, int, cudaStream_t);
-
-cudaError_t launch_y2(const double2* AT, double2* V, double2* O, const double2* rv,
-                      const double2* ro, const double* dUt, DnsGeom g, PhysParams ph,
-                      FftTab<double2> tab0, int* status, cudaStream_t st) {
-  const int CH = 8;
-  const int NST = 4;
-  // the tilting transform is a small part of this kernel: the runtime-length
-  // FFT keeps its register footprint (and so the occupancy) low
-  return with_len_m0(0, [&](auto LL) {
-    constexpr int L = decltype(LL)::value;
-    const size_t sm = y2_smem(g.Ny, FLine<double2, L>::stride(tab0.plan.L), CH, NST);
-    cudaFuncSetAttribute(k_y2<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    int threads = ((2 * g.Ny + 31) / 32) * 32;
-    if (threads < 64) threads = 64;
-    const unsigned nslots = (unsigned)(g.Kx * g.Kh);
-    k_y2<L><<<nslots, threads, sm, st>>>(AT, V, O, rv, ro, dUt, g, ph, tab0, CH, NST, status);
-    return cudaGetLastError();
-  });
-}
+template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, const double*, const double*, const double*, DnsGeom, PhysParams, FftTab<double2>, FftTab<double2>, int, cudaStream_t);
+template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, const double*, const double*, const double*, DnsGeom, PhysParams, FftTab<float2>, FftTab<double2>, int, cudaStream_t);

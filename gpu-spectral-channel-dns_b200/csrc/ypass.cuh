@@ -14,11 +14,13 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
                       PhysParams ph, FftTab<C> tab, cudaStream_t st);
+// rows of the integrated right-hand sides written by y1 for the wall solve
+struct RhsDims {
+  int nv, no;       // rows per pencil (v / omega systems)
+  long long gp;     // pencil pitch (complex)
+};
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
-                      double2* Nop, double2* rv, double2* ro, const double* Ut,
-                      const double* ddUt, DnsGeom g, PhysParams ph, FftTab<C> tabP,
-                      FftTab<double2> tab0, int boot, cudaStream_t st);
-cudaError_t launch_y2(const double2* AT, double2* V, double2* O, const double2* rv,
-                      const double2* ro, const double* dUt, DnsGeom g, PhysParams ph,
-                      FftTab<double2> tab0, int* status, cudaStream_t st);
+                      double2* Nop, double2* gv, double2* go, RhsDims rd, const double* Ut,
+                      const double* dUt, const double* ddUt, DnsGeom g, PhysParams ph,
+                      FftTab<C> tabP, FftTab<double2> tab0, int boot, cudaStream_t st);
