@@ -146,8 +146,9 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
   mark();
   const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
-  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, c->Ut, c->dUt, c->ddUt,
-                        g, c->ph, fyP.tab(), c->fy0_d.tab(), boot, c->st)))
+  const RhsTabs tb{c->rtab, c->rtab + 4 * (size_t)c->wd.nv, c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no};
+  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
+                        boot, c->st)))
     return e;
   mark();
   if (!boot)
@@ -303,7 +304,8 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
       (e = c->alloc(&c->Nvp, hn)) || (e = c->alloc(&c->Nop, hn)) || (e = c->alloc(&c->rv, gn)) ||
       (e = c->alloc(&c->ro, gn)) || (e = c->alloc(&c->status, 1)) ||
       (e = c->alloc((unsigned char**)&c->F6, f6 * csz)) ||
-      (e = c->alloc((unsigned char**)&c->G6, g6 * csz)))
+      (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
+      (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny)))
     return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
   cudaMemcpy(c->T0, T0.data(), NN * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->T2, T2.data(), NN * 8, cudaMemcpyHostToDevice);
@@ -312,6 +314,18 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   cudaMemcpy(c->dUt, dU.data(), Ny * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->ddUt, ddU.data(), Ny * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->Uy, Uy.data(), g.Py * 8, cudaMemcpyHostToDevice);
+  {
+    // y1 tables (integrated cardinal corrections, cos(k pi/N))
+    const int N = Ny - 1, nv = c->wd.nv, no = c->wd.no;
+    std::vector<double> tab(4 * (size_t)nv + 2 * (size_t)no + Ny);
+    const int mv[4] = {0, 1, N - 1, N};
+    for (int m = 0; m < 4; ++m) wall::cardinal_rows(N, mv[m], 4, nv, &tab[(size_t)m * nv]);
+    wall::cardinal_rows(N, 0, 2, no, &tab[4 * (size_t)nv]);
+    wall::cardinal_rows(N, N, 2, no, &tab[4 * (size_t)nv + no]);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k <= N; ++k) tab[4 * (size_t)nv + 2 * (size_t)no + k] = (double)cosl(PI * k / N);
+    cudaMemcpy(c->rtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice);
+  }
   cudaMemset(c->status, 0, sizeof(int));
   cudaMemset(c->Nvp, 0, hn * 16);
   cudaMemset(c->Nop, 0, hn * 16);
@@ -327,7 +341,7 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->F6, c->G6, c->scratch, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->status};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -390,19 +404,51 @@ dns_status dns_get_state(dns_ctx* c, void* v, void* o, size_t pitch, int where) 
   return s;
 }
 
+// The AB2 history is held as Chebyshev coefficients; the ABI exchanges it
+// as values at the Gauss-Lobatto points (the reference's rhs_v_p /
+// rhs_omega_y_p), converted here with the no-pad s2p / p2s.
+// (k_cheby_inplace writes whole FFT lines, so the scratch pencils have
+// pitch mz/2 >= the no-pad FFT length.)
+static dns_status history_out(dns_ctx* c, const double2* src, void* dst, size_t pitch, int where) {
+  dns_status s = need_scratch(c);
+  if (s) return s;
+  const size_t w = (size_t)c->g.Ny * 16, ps = (size_t)(c->P.mz / 2);
+  CK(cudaMemcpy2DAsync(c->scratch, ps * 16, src, w, w, (size_t)c->g.H, cudaMemcpyDeviceToDevice, c->st));
+  PencilArr a{c->scratch, (long long)ps, 0};
+  CK(launch_cheby_inplace<double2>(a, c->g.H, 1, c->g.Ny, c->fy0_d.tab(), c->st));
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
+  if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
+  CK(cudaMemcpy2DAsync(dst, pitch, c->scratch, ps * 16, w, (size_t)c->g.H, kind_of(where, false), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DNS_OK;
+}
+static dns_status history_in(dns_ctx* c, double2* dst, const void* src, size_t pitch, int where) {
+  dns_status s = need_scratch(c);
+  if (s) return s;
+  const size_t w = (size_t)c->g.Ny * 16, ps = (size_t)(c->P.mz / 2);
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
+  if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
+  CK(cudaMemcpy2DAsync(c->scratch, ps * 16, src, pitch, w, (size_t)c->g.H, kind_of(where, true), c->st));
+  PencilArr a{c->scratch, (long long)ps, 0};
+  CK(launch_cheby_inplace<double2>(a, c->g.H, 3, c->g.Ny, c->fy0_d.tab(), c->st));
+  CK(cudaMemcpy2DAsync(dst, w, c->scratch, ps * 16, w, (size_t)c->g.H, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return DNS_OK;
+}
+
 dns_status dns_get_history(dns_ctx* c, void* nv, void* no, size_t pitch, int where) {
   if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
-  dns_status s = copy_pencils(c, c->Nvp, nullptr, nv, pitch, where, false);
-  if (s == DNS_OK) s = copy_pencils(c, c->Nop, nullptr, no, pitch, where, false);
+  dns_status s = history_out(c, c->Nvp, nv, pitch, where);
+  if (s == DNS_OK) s = history_out(c, c->Nop, no, pitch, where);
   return s;
 }
 
 dns_status dns_set_history(dns_ctx* c, const void* nv, const void* no, size_t pitch, int where) {
   if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
-  dns_status s = copy_pencils(c, c->Nvp, nv, nullptr, pitch, where, true);
-  if (s == DNS_OK) s = copy_pencils(c, c->Nop, no, nullptr, pitch, where, true);
+  dns_status s = history_in(c, c->Nvp, nv, pitch, where);
+  if (s == DNS_OK) s = history_in(c, c->Nop, no, pitch, where);
   if (s == DNS_OK) c->booted = true;
   return s;
 }

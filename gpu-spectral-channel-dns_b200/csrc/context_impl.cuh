@@ -36,6 +36,7 @@ struct dns_ctx {
   double2* wfac = nullptr;
   double* wQ = nullptr;
   WallDims wd{};
+  double* rtab = nullptr;  // y1 tables: B^4 C_m (4 x nv), B^2 C_m (2 x no), cos(k pi/N)
   void* F6 = nullptr;
   void* G6 = nullptr;
   double2* scratch = nullptr;

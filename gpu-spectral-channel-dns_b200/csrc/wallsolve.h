@@ -91,6 +91,10 @@ void solve(const Shape& sh, const cx* L, const cx* U, const cx* g, cx* x);
 // rows K .. K+n-1 of B^K rho, rho of length N+1 (B: Chebyshev integration)
 void integrate_rows(int K, int N, const cx* rho, int n, cx* g);
 
+// rows K .. K+n-1 of B^K C_m, C_m the coefficients of the cardinal
+// polynomial of the Gauss-Lobatto point y_m (1 at y_m, 0 at the others)
+void cardinal_rows(int N, int m, int K, int n, double* out);
+
 // Chebyshev coefficients (N+1) from basis unknowns: v or Dirichlet recombination
 void recombine(int eq, int N, const cx* x, cx* a);
 

@@ -313,6 +313,20 @@ void integrate_rows(int K, int N, const cx* rho, int n, cx* g) {
   for (int r = 0; r < n; ++r) g[r] = cx{re[K + r], im[K + r]};
 }
 
+void cardinal_rows(int N, int m, int K, int n, double* out) {
+  const long double PI = 3.141592653589793238462643383279502884L;
+  std::vector<cx> rho(N + 1), g(n);
+  const long double wm = (m == 0 || m == N) ? 0.5L : 1.0L;
+  for (int k = 0; k <= N; ++k) {
+    const long long r = ((long long)m * k) % (2LL * N);
+    long double c = 2.0L / N * wm * cosl(PI * r / N);
+    if (k == 0 || k == N) c *= 0.5L;
+    rho[k] = cx{(double)c, 0.0};
+  }
+  integrate_rows(K, N, rho.data(), n, g.data());
+  for (int r = 0; r < n; ++r) out[r] = g[r].re;
+}
+
 void recombine(int eq, int N, const cx* x, cx* a) {
   const int nb = (eq == EQ_V) ? N - 3 : N - 1;
   auto b = [&](int j) { return (j >= 0 && j < nb) ? x[j] : cx{0, 0}; };

@@ -79,15 +79,6 @@ __device__ __forceinline__ double2 ext_s2p_pad(const double2* c, int n, int M, i
   return make_double2(0.0, 0.0);
 }
 
-// even extension for the no-pad s2p (cheby_pre_s2p_noPad): M0 = 2(Ny-1);
-// e[0] = c0, e[Ny-1] = c_{Ny-1}, e[k] = e[M0-k] = c_k/2 otherwise.
-__device__ __forceinline__ double2 ext_s2p_nopad(const double2* c, int n, int M0, int Ny) {
-  if (n == 0) return c[0];
-  if (n < Ny - 1) return c[n] * 0.5;
-  if (n == Ny - 1) return c[n];
-  return c[M0 - n] * 0.5;
-}
-
 template <typename C>
 __device__ __forceinline__ C* pencil_ptr(const PencilArr& a, int f, long long p) {
   return (C*)a.base + (long long)f * a.fs + p * a.ps;
@@ -365,55 +356,97 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
 
 // ---------------------------------------------------------------------------
 // Fused forward wall-normal pass: padded p2s of the three Lamb components,
-// rhsNonlinear, no-pad s2p to collocation values, then (unless boot) the
-// CN explicit operators, AB2 and the v^n half of the tilting term for v,
-// omega_y and the mean modes at the collocation points; finally the values
-// (zero at the points an equation does not use) go back to coefficients
-// (no-pad p2s) and are integrated K times (K = 4 for v, 2 for omega_y and
-// the mean modes): the right-hand sides of the banded systems of
-// wallsolve.h, rows K .. K+n-1.
+// rhsNonlinear, then (unless boot) the right-hand sides of the banded
+// wall-normal systems (wallsolve.h), all in Chebyshev coefficient space:
+//
+//   f = interpolant, at the Gauss-Lobatto points, of the reference's
+//       collocation right-hand side (CN explicit operators, AB2 of the
+//       nonlinear terms, v^n half of the tilting term; source/linear.cpp:
+//       86-205, rhs.cpp:205-215).  Every term is a polynomial: derivatives
+//       come from the coefficient recurrence, products with U(y), U'(y)
+//       from multiplication by y, and the degrees above N fold back
+//       (T_{N+j} = T_{N-j} at the Gauss-Lobatto points);
+//   the equations do not use the walls (and, for v, the points next to
+//       them): the interpolant with those values set to zero is f minus
+//       f(y_m) times the cardinal polynomial of each such point y_m;
+//   g = rows K .. K+n-1 of the K-fold Chebyshev integral (K = 4 for v, 2
+//       for omega_y and the mean modes), the cardinal corrections taken from
+//       precomputed integrated tables.
+//
+// The AB2 history is kept as Chebyshev coefficients of the nonlinear terms.
 //   boot: only store the nonlinear terms as the AB2 history (the effect of
 //         the reference's "extra previous step", source/main_loop.cpp:39-52).
 // ---------------------------------------------------------------------------
-template <typename C, int LM, int LM0>
-__global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __restrict__ V, const double2* __restrict__ O,
-                     double2* Nvp, double2* Nop, double2* gv, double2* go, RhsDims rd,
-                     const double* __restrict__ Ut, const double* __restrict__ dUt,
-                     const double* __restrict__ ddUt,
-                     DnsGeom g, PhysParams ph, FftTab<C> tabP, FftTab<double2> tab0,
-                     int boot) {
+namespace {
+__device__ __forceinline__ double2 cget(const double2* X, int j, int N) {
+  return (j >= 0 && j <= N) ? X[j] : make_double2(0.0, 0.0);
+}
+// coefficient j of y X (y T_0 = T_1, y T_i = (T_{i+1} + T_{i-1}) / 2)
+__device__ __forceinline__ double2 ymul(const double2* X, int j, int N) {
+  if (j < 0) return make_double2(0.0, 0.0);
+  if (j == 0) return cget(X, 1, N) * 0.5;
+  return (cget(X, j - 1, N) * (j == 1 ? 2.0 : 1.0) + cget(X, j + 1, N)) * 0.5;
+}
+__device__ __forceinline__ double2 y2mul(const double2* X, int j, int N) {
+  if (j < 0) return make_double2(0.0, 0.0);
+  if (j == 0) return ymul(X, 1, N) * 0.5;
+  return (ymul(X, j - 1, N) * (j == 1 ? 2.0 : 1.0) + ymul(X, j + 1, N)) * 0.5;
+}
+// coefficient k of the Gauss-Lobatto interpolant of U(y) X(y)
+__device__ __forceinline__ double2 umul_gl(const double2* X, int k, int N, const PhysParams& ph) {
+  auto u = [&](int j) { return cget(X, j, N) * ph.U0 + ymul(X, j, N) * ph.U1 + y2mul(X, j, N) * ph.U2; };
+  double2 r = u(k);
+  if (k == N - 1 || k == N - 2) r = r + u(2 * N - k);
+  return r;
+}
+// ... of U'(y) X(y)
+__device__ __forceinline__ double2 upmul_gl(const double2* X, int k, int N, const PhysParams& ph) {
+  auto u = [&](int j) { return cget(X, j, N) * ph.U1 + ymul(X, j, N) * (2.0 * ph.U2); };
+  double2 r = u(k);
+  if (k == N - 1) r = r + u(N + 1);
+  return r;
+}
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, d);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, d);
+  }
+  return v;
+}
+}  // namespace
+
+template <typename C, int LM>
+__global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __restrict__ V,
+                                                const double2* __restrict__ O, double2* Nvp,
+                                                double2* Nop, double2* gv, double2* go, RhsDims rd,
+                                                RhsTabs tb, DnsGeom g, PhysParams ph,
+                                                FftTab<C> tabP, int boot) {
   typedef FLine<C, LM> FP;
-  typedef FLine<double2, LM0> F0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   const int Py = g.Py;
-  const int M = tabP.plan.L;   // 2 (Py - 1)
-  const int M0 = tab0.plan.L;  // 2 (Ny - 1)
+  const int N = Ny - 1;
+  const int M = tabP.plan.L;  // 2 (Py - 1)
   const int lsP = FP::stride(M);
-  const int ls0 = F0::stride(M0);
+  const int LB = Ny + 8;
   Carve cv(smem_raw);
-  // work region of 15 Ny: coefficient-space arrays, reused at the end for the
-  // right-hand-side values and their integration
-  double2* wk = cv.take<double2>((size_t)15 * Ny);
-  double2* lc = wk;              // lambda coefficients (3 Ny)
-  double2* D1 = wk + 3 * Ny;     // D lambda_x, D lambda_y (2 Ny)
-  double2* Hv = wk + 5 * Ny;
-  double2* Ho = wk + 6 * Ny;
-  double2* Vc = wk + 7 * Ny;
-  double2* Oc = wk + 8 * Ny;
-  double2* t1 = wk + 9 * Ny;
-  double2* t3 = wk + 10 * Ny;
-  double2* D2V = wk + 11 * Ny;
-  double2* D2O = wk + 12 * Ny;
-  double2* t2 = wk + 13 * Ny;
-  double2* D4V = wk + 14 * Ny;
-  double2* nvp = cv.take<double2>(Ny);
-  double2* nop = cv.take<double2>(Ny);
-  const size_t bytesP = (size_t)3 * lsP * sizeof(C);
-  const size_t bytes0 = (size_t)7 * ls0 * sizeof(double2);
-  unsigned char* region = (unsigned char*)cv.take<unsigned char>(bytesP > bytes0 ? bytesP : bytes0);
+  double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients, then fv, fo
+  double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
+  double2* Vc = cv.take<double2>(Ny);
+  double2* Oc = cv.take<double2>(Ny);
+  double2* nvc = cv.take<double2>(Ny);
+  double2* noc = cv.take<double2>(Ny);
+  double2* DV = cv.take<double2>(Ny);
+  double2* D2V = cv.take<double2>(Ny);
+  double2* D3V = cv.take<double2>(Ny);
+  double2* D4V = cv.take<double2>(Ny);
+  double2* DO = cv.take<double2>(Ny);
+  double2* D2O = cv.take<double2>(Ny);
+  double2* red = cv.take<double2>(8);  // values of fv, fo at the unused points
+  const size_t bytesP = (size_t)3 * lsP * sizeof(C), bytesI = (size_t)4 * LB * 16;
+  unsigned char* region = cv.take<unsigned char>(bytesP > bytesI ? bytesP : bytesI);
   C* linesP = (C*)region;
-  double2* lines0 = (double2*)region;
 
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
@@ -423,19 +456,20 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
   const double kmn = kmn_of(ia, ib);
 
-  // 1. load Lamb pencils as even extensions (DCT-I of Py points); state
+  // 1. Lamb pencils as even extensions (DCT-I of Py points); state, history
   for (int t = threadIdx.x; t < 3 * M; t += blockDim.x) {
     const int f = t / M;
     const int n = t - f * M;
     const C* src = pencil_ptr<C>(lam, f, p);
     linesP[(size_t)f * lsP + FP::in_pos(tabP, n)] = (n < Py) ? src[n] : src[M - n];
   }
-  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    Vc[n] = V[p * Ny + n];
-    Oc[n] = O[p * Ny + n];
-    nvp[n] = Nvp[p * Ny + n];
-    nop[n] = Nop[p * Ny + n];
-  }
+  if (!boot)
+    for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
+      Vc[n] = V[p * Ny + n];
+      Oc[n] = O[p * Ny + n];
+      nvc[n] = Nvp[p * Ny + n];
+      noc[n] = Nop[p * Ny + n];
+    }
   FP::template fft<false>(linesP, 3, lsP, tabP);
   const double sc = 1.0 / (Py - 1);
   for (int t = threadIdx.x; t < 3 * Ny; t += blockDim.x) {
@@ -451,119 +485,96 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   if (warp == 0) ddz_warp(lc, D1, Ny);
   if (warp == 1) ddz_warp(lc + Ny, D1 + Ny, Ny);
   if (!boot) {
-    if (warp == 2) ddz_warp(Vc, t1, Ny);
-    if (warp == 3) ddz_warp(Oc, t3, Ny);
-  }
-  __syncthreads();
-  if (!boot) {
-    if (warp == 0) ddz_warp(t1, D2V, Ny);
-    if (warp == 1) ddz_warp(t3, D2O, Ny);
-    __syncthreads();
-    if (warp == 0) ddz_warp(D2V, t2, Ny);
-    __syncthreads();
-    if (warp == 0) ddz_warp(t2, D4V, Ny);
-  }
-  // 3. nonlinear terms in coefficient space
-  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    if (zero) {
-      Hv[n] = lc[n];
-      Ho[n] = lc[Ny + n];
-    } else {
-      Hv[n] = lc[2 * Ny + n] * kmn + muli(D1[n] * ia) + muli(D1[Ny + n] * ib);
-      Ho[n] = muli(lc[Ny + n] * ia) - muli(lc[n] * ib);
+    if (warp == 2) {
+      ddz_warp(Vc, DV, Ny);
+      __syncwarp();
+      ddz_warp(DV, D2V, Ny);
+      __syncwarp();
+      ddz_warp(D2V, D3V, Ny);
+      __syncwarp();
+      ddz_warp(D3V, D4V, Ny);
+    }
+    if (warp == 3) {
+      ddz_warp(Oc, DO, Ny);
+      __syncwarp();
+      ddz_warp(DO, D2O, Ny);
     }
   }
   __syncthreads();
-  // 4. no-pad s2p: collocation values of Hv, Ho, V, V'', V'''', O, O''
-  const int nl = boot ? 2 : 7;
-  const double2* srcs[7] = {Hv, Ho, Vc, D2V, D4V, Oc, D2O};
-  for (int t = threadIdx.x; t < nl * M0; t += blockDim.x) {
-    const int f = t / M0;
-    const int n = t - f * M0;
-    lines0[(size_t)f * ls0 + F0::in_pos(tab0, n)] = ext_s2p_nopad(srcs[f], n, M0, Ny);
-  }
-  F0::template fft<false>(lines0, nl, ls0, tab0);
-  // collocation value at point m of line f (natural order)
-  auto col = [&](int f, int m) { return lines0[(size_t)f * ls0 + F0::out_pos(m)]; };
-  if (boot) {
-    for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-      Nvp[p * Ny + n] = col(0, n);
-      Nop[p * Ny + n] = col(1, n);
-    }
-    return;
-  }
-  const double dt = ph.dt, Re = ph.Re, al = ia;
-  const int N = Ny - 1;
+  // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
+  const double dt = ph.dt, Re = ph.Re, gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
-  double2* vv = wk;        // collocation values of the v (mean: u0) right-hand side
-  double2* vo = wk + Ny;   // ... of the omega_y (mean: w0) right-hand side
-  // lines: 0 Nv, 1 No, 2 v, 3 v'', 4 v(4), 5 omega, 6 omega''
-  for (int i = threadIdx.x; i < Ny; i += blockDim.x) {
-    double2 rvi = make_double2(0.0, 0.0), roi = make_double2(0.0, 0.0);
+  double2* fv = lc;
+  double2* fo = lc + Ny;
+  for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
+    double2 hv, ho;
     if (zero) {
-      // _get_linear_u0 / _w0: rows 2..N at point i-1
-      if (i >= 2) {
-        const int m = i - 1;
-        rvi = col(2, m) + col(3, m) * (dt * 0.5 / Re) - (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
-        roi = col(5, m) + col(6, m) * (dt * 0.5 / Re) - (col(1, m) * 1.5 - nop[m] * 0.5) * dt;
-        vv[m] = rvi;
-        vo[m] = roi;
-      }
+      hv = lc[k];
+      ho = lc[Ny + k];
     } else {
-      if (i >= 4 && i <= N) {
-        const int m = i - 2;
-        const double Um = Ut[m];
-        const double2 P0 = col(2, m), P2 = col(3, m), P4 = col(4, m);
-        const double2 re = P4 * (dt * 0.5 / Re) + P2 * (1 - kmn * dt / Re)
-                           - P0 * (kmn * (1 - kmn * dt * 0.5 / Re));
-        const double2 im = P2 * (-al * dt * 0.5 * Um)
-                           + P0 * (kmn * al * dt * 0.5 * Um + al * dt * 0.5 * ddUt[m]);
-        rvi = re + muli(im) + (col(0, m) * 1.5 - nvp[m] * 0.5) * dt;
-        vv[m] = rvi;
-      }
-      if (i >= 2) {
-        const int m = i - 1;
-        const double2 Q0 = col(5, m), Q2 = col(6, m);
-        const double2 re = Q2 * (0.5 / Re * dt) + Q0 * (1 - kmn * dt * 0.5 / Re);
-        const double2 im = Q0 * (-al * dt * 0.5 * Ut[m]);
-        roi = re + muli(im) + (col(1, m) * 1.5 - nop[m] * 0.5) * dt + muli(col(2, m) * (kap * dUt[m]));
-        vo[m] = roi;
-      }
+      hv = lc[2 * Ny + k] * kmn + muli(D1[k] * ia) + muli(D1[Ny + k] * ib);
+      ho = muli(lc[Ny + k] * ia) - muli(lc[k] * ib);
     }
-    Nvp[p * Ny + i] = col(0, i);
-    Nop[p * Ny + i] = col(1, i);
+    Nvp[p * Ny + k] = hv;
+    Nop[p * Ny + k] = ho;
+    if (boot) continue;
+    double2 a, b;
+    if (zero) {
+      // _get_linear_u0 / _w0
+      a = Vc[k] + D2V[k] * (dt * 0.5 / Re) - (hv * 1.5 - nvc[k] * 0.5) * dt;
+      b = Oc[k] + D2O[k] * (dt * 0.5 / Re) - (ho * 1.5 - noc[k] * 0.5) * dt;
+    } else {
+      const double2 re = D4V[k] * (dt * 0.5 / Re) + D2V[k] * (1 - kmn * dt / Re)
+                         - Vc[k] * (kmn * (1 - kmn * dt * 0.5 / Re));
+      const double2 im = umul_gl(D2V, k, N, ph) * (-gam) + umul_gl(Vc, k, N, ph) * (kmn * gam)
+                         + Vc[k] * (gam * 2.0 * ph.U2);
+      a = re + muli(im) + (hv * 1.5 - nvc[k] * 0.5) * dt;
+      const double2 ro = D2O[k] * (0.5 / Re * dt) + Oc[k] * (1 - kmn * dt * 0.5 / Re);
+      b = ro + muli(umul_gl(Oc, k, N, ph) * (-gam)) + (ho * 1.5 - noc[k] * 0.5) * dt
+          + muli(upmul_gl(Vc, k, N, ph) * kap);
+    }
+    fv[k] = a;
+    fo[k] = b;
   }
-  if (threadIdx.x == 0) {
-    const double2 z = make_double2(0.0, 0.0);
-    vv[0] = z; vv[N] = z; vo[0] = z; vo[N] = z;
-    if (!zero) { vv[1] = z; vv[N - 1] = z; }
-  }
+  if (boot) return;
   __syncthreads();
-  // no-pad p2s of the two value vectors (even extension, FFT, 1/N, ends halved)
-  for (int t = threadIdx.x; t < 2 * M0; t += blockDim.x) {
-    const int f = t / M0;
-    const int n = t - f * M0;
-    const double2* src = f ? vo : vv;
-    lines0[(size_t)f * ls0 + F0::in_pos(tab0, n)] = (n <= N) ? src[n] : src[M0 - n];
-  }
-  F0::template fft<false>(lines0, 2, ls0, tab0);
-  const int LB = Ny + 8;
-  double2* av = wk + 2 * Ny;
+  // 4. values at the points the equations leave out; integration buffers
+  double2* av = (double2*)region;
   double2* bv = av + LB;
   double2* ao = bv + LB;
   double2* bo = ao + LB;
-  for (int t = threadIdx.x; t < 2 * LB; t += blockDim.x) {
-    const int f = t / LB;
-    const int k = t - f * LB;
-    double2 cval = make_double2(0.0, 0.0);
-    if (k <= N) {
-      cval = lines0[(size_t)f * ls0 + F0::out_pos(k)] * (1.0 / N);
-      if (k == 0 || k == N) cval = cval * 0.5;
+  const int lane = threadIdx.x & 31;
+  if (warp < 2) {
+    const double2* f = warp ? fo : fv;
+    double2 s0 = make_double2(0.0, 0.0), sN = s0, s1 = s0, sN1 = s0;
+    for (int k = lane; k < Ny; k += 32) {
+      const double2 v = f[k];
+      const double cs = __ldg(tb.cosk + k);
+      const double sg = (k & 1) ? -1.0 : 1.0;
+      s0 = s0 + v;
+      sN = sN + v * sg;
+      s1 = s1 + v * cs;
+      sN1 = sN1 + v * (sg * cs);
     }
-    (f ? ao : av)[k] = cval;
+    s0 = warp_sum(s0);
+    sN = warp_sum(sN);
+    s1 = warp_sum(s1);
+    sN1 = warp_sum(sN1);
+    if (lane == 0) {
+      red[4 * warp + 0] = s0;   // y = 1
+      red[4 * warp + 1] = s1;   // y_1
+      red[4 * warp + 2] = sN1;  // y_{N-1}
+      red[4 * warp + 3] = sN;   // y = -1
+    }
+  } else {
+    for (int t = threadIdx.x - 64; t < 2 * LB; t += blockDim.x - 64) {
+      const int f = t / LB;
+      const int k = t - f * LB;
+      (f ? ao : av)[k] = (k <= N) ? (f ? fo : fv)[k] : make_double2(0.0, 0.0);
+    }
   }
   __syncthreads();
-  // Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  // 5. Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
   const int Kv = zero ? 2 : 4;
   for (int it = 0; it < Kv; ++it) {
     const int nf = (it < 2) ? 2 : 1;
@@ -584,10 +595,22 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
     double2* tmp = av; av = bv; bv = tmp;
     if (it < 2) { tmp = ao; ao = bo; bo = tmp; }
   }
-  for (int r = threadIdx.x; r < rd.nv; r += blockDim.x)
-    gv[p * rd.gp + r] = (Kv + r < LB) ? av[Kv + r] : make_double2(0.0, 0.0);
-  for (int r = threadIdx.x; r < rd.no; r += blockDim.x)
-    go[p * rd.gp + r] = (2 + r < LB) ? ao[2 + r] : make_double2(0.0, 0.0);
+  // 6. rows K .. K+n-1 minus the integrated cardinal corrections
+  for (int r = threadIdx.x; r < rd.nv; r += blockDim.x) {
+    double2 v = (Kv + r < LB) ? av[Kv + r] : make_double2(0.0, 0.0);
+    if (zero) {
+      v = v - red[0] * __ldg(tb.bkco + r) - red[3] * __ldg(tb.bkco + rd.no + r);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) v = v - red[m] * __ldg(tb.bkcv + (size_t)m * rd.nv + r);
+    }
+    gv[p * rd.gp + r] = v;
+  }
+  for (int r = threadIdx.x; r < rd.no; r += blockDim.x) {
+    double2 v = (2 + r < LB) ? ao[2 + r] : make_double2(0.0, 0.0);
+    v = v - red[4] * __ldg(tb.bkco + r) - red[7] * __ldg(tb.bkco + rd.no + r);
+    go[p * rd.gp + r] = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -597,11 +620,11 @@ size_t y3_smem(int Ny, int ls, size_t csz) {
   auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
   return 9 * a((size_t)Ny * 16) + a((size_t)6 * ls * csz);
 }
-size_t y1_smem(int Ny, int lsP, int ls0, size_t csz) {
+size_t y1_smem(int Ny, int lsP, size_t csz) {
   auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
-  size_t s = a((size_t)3 * Ny * 16) + a((size_t)2 * Ny * 16) + 12 * a((size_t)Ny * 16);
-  size_t bp = (size_t)3 * lsP * csz, b0 = (size_t)7 * ls0 * 16;
-  return s + a(bp > b0 ? bp : b0);
+  size_t s = a((size_t)3 * Ny * 16) + a((size_t)2 * Ny * 16) + 10 * a((size_t)Ny * 16) + a(8 * 16);
+  size_t bp = (size_t)3 * lsP * csz, bi = (size_t)4 * (Ny + 8) * 16;
+  return s + a(bp > bi ? bp : bi);
 }
 template <typename C>
 cudaError_t launch_cheby_inplace(PencilArr arr, long long npencils, int mode, int Ny,
@@ -661,19 +684,15 @@ template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr
 
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
-                      double2* Nop, double2* gv, double2* go, RhsDims rd, const double* Ut,
-                      const double* dUt, const double* ddUt, DnsGeom g, PhysParams ph,
-                      FftTab<C> tabP, FftTab<double2> tab0, int boot, cudaStream_t st) {
+                      double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
+                      PhysParams ph, FftTab<C> tabP, int boot, cudaStream_t st) {
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
-    constexpr int L0 = L / 2;  // the no-pad extension is half the padded one
-    const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L),
-                              FLine<double2, L0>::stride(tab0.plan.L), sizeof(C));
-    cudaFuncSetAttribute(k_y1<C, L, L0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_y1<C, L, L0><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, Ut, dUt, ddUt,
-                                                   g, ph, tabP, tab0, boot);
+    const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L), sizeof(C));
+    cudaFuncSetAttribute(k_y1<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_y1<C, L><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, const double*, const double*, const double*, DnsGeom, PhysParams, FftTab<double2>, FftTab<double2>, int, cudaStream_t);
-template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, const double*, const double*, const double*, DnsGeom, PhysParams, FftTab<float2>, FftTab<double2>, int, cudaStream_t);
+template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<double2>, int, cudaStream_t);
+template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<float2>, int, cudaStream_t);

@@ -19,8 +19,13 @@ struct RhsDims {
   int nv, no;       // rows per pencil (v / omega systems)
   long long gp;     // pencil pitch (complex)
 };
+// device tables for the integrated right-hand sides (y1)
+struct RhsTabs {
+  const double* bkcv;  // 4 x nv: rows 4.. of B^4 C_m, m = 0, 1, N-1, N (C_m cardinal polynomial of y_m)
+  const double* bkco;  // 2 x no: rows 2.. of B^2 C_m, m = 0, N
+  const double* cosk;  // cos(k pi / N), k = 0..N
+};
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
-                      double2* Nop, double2* gv, double2* go, RhsDims rd, const double* Ut,
-                      const double* dUt, const double* ddUt, DnsGeom g, PhysParams ph,
-                      FftTab<C> tabP, FftTab<double2> tab0, int boot, cudaStream_t st);
+                      double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
+                      PhysParams ph, FftTab<C> tabP, int boot, cudaStream_t st);
