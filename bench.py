@@ -294,6 +294,25 @@ def run_ours(args, rank, world):
                 state_bytes=2 * geo["Kx"] * geo["Nz"] * geo["Ny"] * 16)
 
 
+def run_one(args):
+    """One context of one precision: bootstrap, W warm-up steps, K steps,
+    per-kernel CUDA-event times (profiling runs; no comparison, no e2e)."""
+    import torch
+    pkg = load_pkg()
+    torch.cuda.set_device(0)
+    V0, O0 = pkg.seeded_state(CFG["Nx"], CFG["Ny"], CFG["Nz"], 4.0, 2.0, CFG["amplitude"], CFG["seed"])
+    prec = pkg.PREC_MIXED if args.only == "mixed" else pkg.PREC_FP64
+    ctx = pkg.Context(pkg.make_params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"],
+                                      dt=CFG["dt"], precision=prec, device=0))
+    ctx.set_state(V0, O0)
+    ctx.bootstrap()
+    ctx.step(args.warmup)
+    kms = ctx.step_profiled(args.steps)
+    ctx.synchronize()
+    ctx.close()
+    return {"only": args.only, "config": args.config, "kernel_ms": {k: round(v, 4) for k, v in kms.items()}}
+
+
 def roofline(kms, geo, c, peak):
     kb = kernel_bytes(geo, c)
     top = max(kms, key=kms.get)
@@ -311,6 +330,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", default="256x129x256", choices=sorted(CONFIGS))
+    ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
+                    help="run one precision only (bootstrap + warm-up + timed steps), for "
+                         "profiling captures; prints per-kernel times, not the bench line")
     args = ap.parse_args()
     global CFG
     CFG = CONFIGS[args.config]
@@ -330,6 +352,9 @@ def main():
         import datetime
         import torch
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.only:
+        print(json.dumps(run_one(args)))
+        return
     r = run_ours(args, rank, world)
     peak, peak_kind = measured_peaks()
     top64, roof64 = roofline(r["kms64"], r["geo"], 16, peak)

@@ -94,6 +94,46 @@ template <> struct CodeletConst<6> {
   }
 };
 
+// radices 24, 32, 48: quarter-wave tables (correctly rounded) and symmetry
+template <int R> struct CodeletQuarter;
+template <> struct CodeletQuarter<24> {
+  DNS_HD static double q(int m) {
+    const double t[7] = {1.0, 0.9659258262890683, 0.8660254037844386, 0.7071067811865476, 0.5,
+                         0.25881904510252074, 0.0};
+    return t[m];
+  }
+};
+template <> struct CodeletQuarter<32> {
+  DNS_HD static double q(int m) {
+    const double t[9] = {1.0, 0.9807852804032304, 0.9238795325112867, 0.8314696123025452,
+                         0.7071067811865476, 0.5555702330196022, 0.3826834323650898,
+                         0.19509032201612828, 0.0};
+    return t[m];
+  }
+};
+template <> struct CodeletQuarter<48> {
+  DNS_HD static double q(int m) {
+    const double t[13] = {1.0, 0.9914448613738104, 0.9659258262890683, 0.9238795325112867,
+                          0.8660254037844386, 0.7933533402912352, 0.7071067811865476,
+                          0.6087614290087207, 0.5, 0.3826834323650898, 0.25881904510252074,
+                          0.1305261922200516, 0.0};
+    return t[m];
+  }
+};
+template <int R> struct CodeletConstQ {
+  DNS_HD static double c(int m) {
+    m %= R;
+    if (m <= R / 4) return CodeletQuarter<R>::q(m);
+    if (m <= R / 2) return -CodeletQuarter<R>::q(R / 2 - m);
+    if (m <= 3 * R / 4) return -CodeletQuarter<R>::q(m - R / 2);
+    return CodeletQuarter<R>::q(R - m);
+  }
+  DNS_HD static double s(int m) { return c(m + 3 * R / 4); }
+};
+template <> struct CodeletConst<24> : CodeletConstQ<24> {};
+template <> struct CodeletConst<32> : CodeletConstQ<32> {};
+template <> struct CodeletConst<48> : CodeletConstQ<48> {};
+
 // W_R^m (forward: exp(-2 pi i m / R)); INV conjugates
 template <int R, bool INV, typename C>
 DNS_HD C wconst(int m) {
@@ -190,6 +230,15 @@ template <bool INV, typename C> struct Codelet<12, INV, C> {
 };
 template <bool INV, typename C> struct Codelet<16, INV, C> {
   DNS_HD static void run(C* v) { codelet_split<4, 4, 16, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<24, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<8, 3, 24, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<32, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<4, 8, 32, INV, C>(v); }
+};
+template <bool INV, typename C> struct Codelet<48, INV, C> {
+  DNS_HD static void run(C* v) { codelet_split<16, 3, 48, INV, C>(v); }
 };
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,205 @@
+// Warp-synchronous line FFT: one warp transforms NL lines of length L held
+// in shared memory, with no block-wide barrier.
+//
+// Each pass is a Stockham autosort step (as in fft2.cuh): with Ns = product
+// of the previous radices, butterfly j in [0, L/R) reads x[j + r L/R],
+// applies W_{Ns R}^{r (j mod Ns)}, takes the R-point DFT in registers and
+// writes y[(j/Ns) Ns R + (j mod Ns) + r Ns].  The NL L / R butterflies of a
+// pass are spread evenly over the 32 lanes (every radix of a plan divides
+// NL L / 32), a lane loads all its inputs before the warp synchronises and
+// writes, so the transform runs in place.  Input and output are in natural
+// order at swizzled positions wsw(i): the low bits of the index are XORed
+// with the next ones, which makes the strided accesses of the early passes
+// bank-conflict free without padding within a line; the line stride is a
+// parameter (padded where several lines are addressed at one position).
+#pragma once
+#include "fft2.cuh"
+
+// swizzle within aligned blocks: 16 elements (FP32 complex, 128 B) or 8
+// elements (FP64 complex)
+template <typename C> struct WSwz { enum { S = 4 }; };
+template <> struct WSwz<double2> { enum { S = 3 }; };
+template <typename C> DNS_HD int wsw(int i) {
+  constexpr int S = WSwz<C>::S;
+  return i ^ ((i >> S) & ((1 << S) - 1));
+}
+
+// plans: radices (up to 48 FP32, 8 FP64 for register pressure), each
+// dividing NL L / 32
+template <int L, int NL, int MAXR> struct WPlan { enum { ok = 0 }; };
+#define WPLAN(L, NL, MAXR, ...) \
+  template <> struct WPlan<L, NL, MAXR> { enum { ok = 1 }; typedef Radices<__VA_ARGS__> R; };
+// FP32
+WPLAN(128, 1, 16, 4, 4, 4, 2)
+WPLAN(256, 1, 16, 8, 8, 4)
+WPLAN(384, 1, 16, 12, 4, 4, 2)
+WPLAN(512, 1, 16, 8, 8, 8)
+WPLAN(768, 1, 16, 8, 8, 12)
+WPLAN(128, 2, 16, 8, 4, 4)
+WPLAN(192, 2, 16, 12, 4, 4)
+WPLAN(256, 2, 16, 16, 16)
+WPLAN(384, 2, 16, 8, 8, 6)
+WPLAN(512, 2, 16, 32, 16)
+WPLAN(768, 2, 16, 16, 48)
+WPLAN(384, 3, 16, 12, 4, 4, 2)
+WPLAN(384, 4, 16, 16, 24)
+// FP64
+WPLAN(128, 1, 8, 4, 4, 4, 2)
+WPLAN(256, 1, 8, 8, 8, 4)
+WPLAN(384, 1, 8, 6, 4, 4, 4)
+WPLAN(512, 1, 8, 8, 8, 8)
+WPLAN(768, 1, 8, 8, 8, 4, 3)
+WPLAN(128, 2, 8, 8, 4, 4)
+WPLAN(192, 2, 8, 4, 4, 4, 3)
+WPLAN(256, 2, 8, 8, 8, 4)
+WPLAN(384, 2, 8, 8, 8, 6)
+WPLAN(512, 2, 8, 8, 8, 8)
+WPLAN(768, 2, 8, 8, 8, 4, 3)
+WPLAN(384, 3, 8, 6, 4, 4, 4)
+#undef WPLAN
+
+// One pass, split into the load (inputs of the lane's butterfly q, twiddled,
+// transformed) and the store of its outputs, so that host code can run the
+// same index arithmetic lane by lane.
+template <typename C, int L, int NL, bool INV, int R, int Ns>
+struct WPass {
+  static constexpr int NB = L / R;        // butterflies per line
+  static constexpr int B = NL * NB / 32;  // butterflies per lane
+  static_assert((NL * NB) % 32 == 0, "radix does not divide the lane share");
+  DNS_HD static void load(const C* buf, int ls, const C* tw, int lane, int q, C* v) {
+    const int w = lane + 32 * q;
+    const int line = w / NB;
+    const int j = w - line * NB;
+    const C* x = buf + line * ls;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = x[wsw<C>(j + r * NB)];
+    if (Ns > 1) {
+      const int k = j % Ns;
+      if (k > 0) {
+        constexpr int step = L / (Ns * R);
+        const C w1 = tw[k * step];
+        C wr = w1;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          if (FftMaxRadix<C>::v == 8) {
+            if (r > 1) wr = cmul(wr, w1);
+          } else {
+            wr = tw[r * k * step];
+          }
+          v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+        }
+      }
+    }
+    Codelet<R, INV, C>::run(v);
+  }
+  // first pass (Ns = 1, no twiddles) reading element n of line l from ld(l, n)
+  template <class LD> DNS_HD static void load_fn(LD& ld, int lane, int q, C* v) {
+    const int w = lane + 32 * q;
+    const int line = w / NB;
+    const int j = w - line * NB;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ld(line, j + r * NB);
+    Codelet<R, INV, C>::run(v);
+  }
+  // last pass handing output k of line l to st(l, k, value)
+  template <class ST> DNS_HD static void store_fn(ST& st, int lane, int q, const C* v) {
+    const int w = lane + 32 * q;
+    const int line = w / NB;
+    const int j = w - line * NB;
+    const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+    for (int r = 0; r < R; ++r) st(line, base + r * Ns, v[r]);
+  }
+  DNS_HD static void store(C* buf, int ls, int lane, int q, const C* v) {
+    const int w = lane + 32 * q;
+    const int line = w / NB;
+    const int j = w - line * NB;
+    C* y = buf + line * ls;
+    const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+    for (int r = 0; r < R; ++r) y[wsw<C>(base + r * Ns)] = v[r];
+  }
+};
+
+#ifdef __CUDACC__
+template <typename C, int L, int NL, bool INV, int R, int Ns>
+__device__ __forceinline__ void wfft_pass(C* buf, int ls, const C* __restrict__ tw, int lane) {
+  typedef WPass<C, L, NL, INV, R, Ns> P;
+  C v[P::B][R];
+#pragma unroll
+  for (int q = 0; q < P::B; ++q) P::load(buf, ls, tw, lane, q, v[q]);
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < P::B; ++q) P::store(buf, ls, lane, q, v[q]);
+  __syncwarp();
+}
+
+template <typename C, int L, int NL, bool INV, int Ns, int R, int... Rest>
+struct WRun {
+  __device__ __forceinline__ static void go(C* buf, int ls, const C* tw, int lane) {
+    wfft_pass<C, L, NL, INV, R, Ns>(buf, ls, tw, lane);
+    WRun<C, L, NL, INV, Ns * R, Rest...>::go(buf, ls, tw, lane);
+  }
+};
+template <typename C, int L, int NL, bool INV, int Ns, int R>
+struct WRun<C, L, NL, INV, Ns, R> {
+  __device__ __forceinline__ static void go(C* buf, int ls, const C* tw, int lane) {
+    wfft_pass<C, L, NL, INV, R, Ns>(buf, ls, tw, lane);
+  }
+};
+template <typename C, int L, int NL, bool INV, typename RS> struct WDo;
+template <typename C, int L, int NL, bool INV, int... Rs>
+struct WDo<C, L, NL, INV, Radices<Rs...>> {
+  __device__ __forceinline__ static void go(C* buf, int ls, const C* tw, int lane) {
+    WRun<C, L, NL, INV, 1, Rs...>::go(buf, ls, tw, lane);
+  }
+};
+
+// Variant with the input and output fused into the first and last passes:
+// the first pass reads ld(line, n), the last hands st(line, k, value) every
+// output; buf (NL lines of L) holds the intermediate passes only.
+template <typename C, int L, int NL, bool INV, int Ns, bool FIRST, int R, int... Rest>
+struct WRunIO {
+  template <class LD, class ST>
+  __device__ __forceinline__ static void go(C* buf, const C* tw, int lane, LD& ld, ST& st) {
+    typedef WPass<C, L, NL, INV, R, Ns> P;
+    constexpr bool LAST = sizeof...(Rest) == 0;
+    C v[P::B][R];
+#pragma unroll
+    for (int q = 0; q < P::B; ++q) {
+      if constexpr (FIRST) P::template load_fn<LD>(ld, lane, q, v[q]);
+      else P::load(buf, L, tw, lane, q, v[q]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < P::B; ++q) {
+      if constexpr (LAST) P::template store_fn<ST>(st, lane, q, v[q]);
+      else P::store(buf, L, lane, q, v[q]);
+    }
+    __syncwarp();
+    if constexpr (!LAST) WRunIO<C, L, NL, INV, Ns * R, false, Rest...>::go(buf, tw, lane, ld, st);
+  }
+};
+template <typename C, int L, int NL, bool INV, typename RS> struct WDoIO;
+template <typename C, int L, int NL, bool INV, int... Rs>
+struct WDoIO<C, L, NL, INV, Radices<Rs...>> {
+  template <class LD, class ST>
+  __device__ __forceinline__ static void go(C* buf, const C* tw, int lane, LD& ld, ST& st) {
+    WRunIO<C, L, NL, INV, 1, true, Rs...>::go(buf, tw, lane, ld, st);
+  }
+};
+template <typename C, int L, int NL, bool INV, class LD, class ST>
+__device__ __forceinline__ void wfft_io(C* buf, const C* __restrict__ tw, LD ld, ST st) {
+  WDoIO<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, tw, threadIdx.x & 31, ld, st);
+}
+
+// Transform the NL lines at buf (line stride ls >= L, positions wsw(i)) by
+// the calling warp.  The lines must have been written by this warp (or be
+// visible to it after a barrier); a __syncwarp is taken first.
+// tw: W_L^j, j < L.
+template <typename C, int L, int NL, bool INV>
+__device__ __forceinline__ void wfft(C* buf, const C* __restrict__ tw, int ls = L) {
+  __syncwarp();
+  WDo<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, ls, tw, threadIdx.x & 31);
+}
+#endif

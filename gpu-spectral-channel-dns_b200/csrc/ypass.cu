@@ -19,6 +19,7 @@
 // same way: coefficient-space derivatives, then the no-pad DCT.
 #include "fftline.cuh"
 #include "kernels.cuh"
+#include "wfft.cuh"
 #include "ypass.cuh"
 
 namespace {
@@ -354,6 +355,90 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
   }
 }
 
+// Same pass with the warp FFT: three warps per pencil, two of the six lines
+// per warp, no block barrier inside the transforms; the twiddle table is
+// staged in shared memory.
+template <typename C, int M>
+__global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const double2* __restrict__ O,
+                                           PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Ny = g.Ny;
+  Carve cv(smem_raw);
+  C* tws = cv.take<C>(M);
+  double2* w = cv.take<double2>(Ny);
+  double2* oz = cv.take<double2>(Ny);
+  double2* Dw = cv.take<double2>(Ny);
+  double2* u = cv.take<double2>(Ny);
+  double2* v = cv.take<double2>(Ny);
+  double2* Du = cv.take<double2>(Ny);
+  double2* Dv = cv.take<double2>(Ny);
+  double2* ox = cv.take<double2>(Ny);
+  double2* oy = cv.take<double2>(Ny);
+  C* lines = cv.take<C>((size_t)6 * M);
+  const long long p = blockIdx.x;
+  const int kx = (int)(p % g.Kx);
+  const int kz = (int)(p / g.Kx);
+  const bool zero = (kx == 0 && kz == 0);
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = kmn_of(ia, ib);
+  const double kmn1 = zero ? 0.0 : 1.0 / kmn;
+  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
+    w[n] = V[p * Ny + n];
+    oz[n] = O[p * Ny + n];
+  }
+  for (int n = threadIdx.x; n < M; n += blockDim.x) tws[n] = tab.tw[n];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  if (!zero && warp == 0) ddz_warp(w, Dw, Ny);
+  __syncthreads();
+  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
+    if (zero) {
+      u[n] = w[n];
+      v[n] = oz[n];
+    } else {
+      const double2 d = Dw[n], o = oz[n];
+      u[n] = muli(d * (ia * kmn1)) - muli(o * (ib * kmn1));
+      v[n] = muli(d * (ib * kmn1)) + muli(o * (ia * kmn1));
+    }
+  }
+  __syncthreads();
+  if (warp == 0) ddz_warp(v, Dv, Ny);
+  if (warp == 1) ddz_warp(u, Du, Ny);
+  __syncthreads();
+  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
+    const double2 wn = w[n];
+    ox[n] = Dv[n] - muli(wn * ib);
+    oy[n] = muli(wn * ia) - Du[n];
+  }
+  __syncthreads();
+  // this warp's two lines: fields 2 warp, 2 warp + 1; the first FFT pass
+  // reads the even extensions e[0] = c_0, e[n] = e[M-n] = c_n / 2 (n < Ny),
+  // zero elsewhere, the last one writes the Py values
+  C* wl = lines + (size_t)2 * warp * M;
+  const double2* s0 = (warp == 0) ? u : (warp == 1 ? w : oy);
+  const double2* s1 = (warp == 0) ? v : (warp == 1 ? ox : oz);
+  // w (line 2) and omega_z (line 5) vanish for the mean mode
+  const bool z0 = zero && warp == 1, z1 = zero && warp == 2;
+  auto ld = [&](int l, int n) -> C {
+    const double2* src = l ? s1 : s0;
+    double2 e = make_double2(0.0, 0.0);
+    if (!(l ? z1 : z0)) {
+      if (n == 0) e = src[0];
+      else if (n < Ny) e = src[n] * 0.5;
+      else if (n > M - Ny) e = src[M - n] * 0.5;
+    }
+    return from_d2<C>(e);
+  };
+  const int Py = g.Py;
+  C* d0 = pencil_ptr<C>(out, 2 * warp, p);
+  C* d1 = pencil_ptr<C>(out, 2 * warp + 1, p);
+  auto st = [&](int l, int k, C val) {
+    if (k < Py) (l ? d1 : d0)[k] = val;
+  };
+  wfft_io<C, M, 2, false>(wl, tws, ld, st);
+}
+
 // ---------------------------------------------------------------------------
 // Fused forward wall-normal pass: padded p2s of the three Lamb components,
 // rhsNonlinear, then (unless boot) the right-hand sides of the banded
@@ -613,6 +698,211 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   }
 }
 
+// Same pass with warp FFTs: warp 0 transforms lambda_x and lambda_y and
+// differentiates them, warp 1 transforms lambda_z, while warps 2 and 3
+// build the derivative chains of v and omega_y; no block barrier inside the
+// transforms.
+template <typename C, int M>
+__global__ void __launch_bounds__(128) k_y1w(PencilArr lam, const double2* __restrict__ V,
+                                            const double2* __restrict__ O, double2* Nvp,
+                                            double2* Nop, double2* gv, double2* go, RhsDims rd,
+                                            RhsTabs tb, DnsGeom g, PhysParams ph,
+                                            FftTab<C> tabP, int boot) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Ny = g.Ny;
+  const int Py = g.Py;
+  const int N = Ny - 1;
+  const int LB = Ny + 8;
+  Carve cv(smem_raw);
+  C* tws = cv.take<C>(M);
+  double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients, then fv, fo
+  double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
+  double2* Vc = cv.take<double2>(Ny);
+  double2* Oc = cv.take<double2>(Ny);
+  double2* nvc = cv.take<double2>(Ny);
+  double2* noc = cv.take<double2>(Ny);
+  double2* DV = cv.take<double2>(Ny);
+  double2* D2V = cv.take<double2>(Ny);
+  double2* D3V = cv.take<double2>(Ny);
+  double2* D4V = cv.take<double2>(Ny);
+  double2* DO = cv.take<double2>(Ny);
+  double2* D2O = cv.take<double2>(Ny);
+  double2* red = cv.take<double2>(8);
+  const size_t bytesL = (size_t)3 * M * sizeof(C), bytesI = (size_t)4 * LB * 16;
+  unsigned char* region = cv.take<unsigned char>(bytesL > bytesI ? bytesL : bytesI);
+  C* lines = (C*)region;
+
+  const long long p = blockIdx.x;
+  const int kx = (int)(p % g.Kx);
+  const int kz = (int)(p / g.Kx);
+  const bool zero = (kx == 0 && kz == 0);
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = kmn_of(ia, ib);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // 1. twiddles, state, history
+  for (int n = threadIdx.x; n < M; n += blockDim.x) tws[n] = tabP.tw[n];
+  if (!boot)
+    for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
+      Vc[n] = V[p * Ny + n];
+      Oc[n] = O[p * Ny + n];
+      nvc[n] = Nvp[p * Ny + n];
+      noc[n] = Nop[p * Ny + n];
+    }
+  __syncthreads();
+  // 2. transforms (warp 0: lambda_x, lambda_y; warp 1: lambda_z), read from
+  //    the pencils as even extensions, coefficients written to lc; then the
+  //    derivatives (warp 0: D lambda_x, D lambda_y; warps 2, 3: chains of
+  //    v and omega_y)
+  const double sc = 1.0 / (Py - 1);
+  if (warp < 2) {
+    const int f0 = warp == 0 ? 0 : 2;
+    const C* src0 = pencil_ptr<C>(lam, f0, p);
+    const C* src1 = pencil_ptr<C>(lam, f0 + 1, p);
+    auto ld = [&](int l, int n) -> C {
+      const C* src = l ? src1 : src0;
+      return (n < Py) ? src[n] : src[M - n];
+    };
+    auto st = [&](int l, int k, C val) {
+      if (k < Ny) {
+        double2 c = to_d2(val) * sc;
+        if (k == 0) c = c * 0.5;
+        lc[(size_t)(f0 + l) * Ny + k] = c;
+      }
+    };
+    if (warp == 0) {
+      wfft_io<C, M, 2, false>(lines, tws, ld, st);
+      ddz_warp(lc, D1, Ny);
+      __syncwarp();
+      ddz_warp(lc + Ny, D1 + Ny, Ny);
+    } else {
+      wfft_io<C, M, 1, false>(lines + (size_t)2 * M, tws, ld, st);
+    }
+  } else if (!boot && warp == 2) {
+    ddz_warp(Vc, DV, Ny);
+    __syncwarp();
+    ddz_warp(DV, D2V, Ny);
+    __syncwarp();
+    ddz_warp(D2V, D3V, Ny);
+    __syncwarp();
+    ddz_warp(D3V, D4V, Ny);
+  } else if (!boot && warp == 3) {
+    ddz_warp(Oc, DO, Ny);
+    __syncwarp();
+    ddz_warp(DO, D2O, Ny);
+  }
+  __syncthreads();
+  // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
+  const double dt = ph.dt, Re = ph.Re, gam = ia * dt * 0.5;
+  const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
+  double2* fv = lc;
+  double2* fo = lc + Ny;
+  for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
+    double2 hv, ho;
+    if (zero) {
+      hv = lc[k];
+      ho = lc[Ny + k];
+    } else {
+      hv = lc[2 * Ny + k] * kmn + muli(D1[k] * ia) + muli(D1[Ny + k] * ib);
+      ho = muli(lc[Ny + k] * ia) - muli(lc[k] * ib);
+    }
+    Nvp[p * Ny + k] = hv;
+    Nop[p * Ny + k] = ho;
+    if (boot) continue;
+    double2 a, b;
+    if (zero) {
+      a = Vc[k] + D2V[k] * (dt * 0.5 / Re) - (hv * 1.5 - nvc[k] * 0.5) * dt;
+      b = Oc[k] + D2O[k] * (dt * 0.5 / Re) - (ho * 1.5 - noc[k] * 0.5) * dt;
+    } else {
+      const double2 re = D4V[k] * (dt * 0.5 / Re) + D2V[k] * (1 - kmn * dt / Re)
+                         - Vc[k] * (kmn * (1 - kmn * dt * 0.5 / Re));
+      const double2 im = umul_gl(D2V, k, N, ph) * (-gam) + umul_gl(Vc, k, N, ph) * (kmn * gam)
+                         + Vc[k] * (gam * 2.0 * ph.U2);
+      a = re + muli(im) + (hv * 1.5 - nvc[k] * 0.5) * dt;
+      const double2 ro = D2O[k] * (0.5 / Re * dt) + Oc[k] * (1 - kmn * dt * 0.5 / Re);
+      b = ro + muli(umul_gl(Oc, k, N, ph) * (-gam)) + (ho * 1.5 - noc[k] * 0.5) * dt
+          + muli(upmul_gl(Vc, k, N, ph) * kap);
+    }
+    fv[k] = a;
+    fo[k] = b;
+  }
+  if (boot) return;
+  __syncthreads();
+  // 4. values at the points the equations leave out; integration buffers
+  double2* av = (double2*)region;
+  double2* bv = av + LB;
+  double2* ao = bv + LB;
+  double2* bo = ao + LB;
+  if (warp < 2) {
+    const double2* f = warp ? fo : fv;
+    double2 s0 = make_double2(0.0, 0.0), sN = s0, s1 = s0, sN1 = s0;
+    for (int k = lane; k < Ny; k += 32) {
+      const double2 v = f[k];
+      const double cs = __ldg(tb.cosk + k);
+      const double sg = (k & 1) ? -1.0 : 1.0;
+      s0 = s0 + v;
+      sN = sN + v * sg;
+      s1 = s1 + v * cs;
+      sN1 = sN1 + v * (sg * cs);
+    }
+    s0 = warp_sum(s0);
+    sN = warp_sum(sN);
+    s1 = warp_sum(s1);
+    sN1 = warp_sum(sN1);
+    if (lane == 0) {
+      red[4 * warp + 0] = s0;
+      red[4 * warp + 1] = s1;
+      red[4 * warp + 2] = sN1;
+      red[4 * warp + 3] = sN;
+    }
+  } else {
+    for (int t = threadIdx.x - 64; t < 2 * LB; t += blockDim.x - 64) {
+      const int f = t / LB;
+      const int k = t - f * LB;
+      (f ? ao : av)[k] = (k <= N) ? (f ? fo : fv)[k] : make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  // 5. Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  const int Kv = zero ? 2 : 4;
+  for (int it = 0; it < Kv; ++it) {
+    const int nf = (it < 2) ? 2 : 1;
+    for (int t = threadIdx.x; t < nf * LB; t += blockDim.x) {
+      const int f = t / LB;
+      const int k = t - f * LB;
+      const double2* x = f ? ao : av;
+      double2* y = f ? bo : bv;
+      double2 r = make_double2(0.0, 0.0);
+      if (k >= 1) {
+        const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
+        const double2 xp = (k + 1 < LB) ? x[k + 1] : make_double2(0.0, 0.0);
+        r = (xm - xp) * (1.0 / (2.0 * k));
+      }
+      y[k] = r;
+    }
+    __syncthreads();
+    double2* tmp = av; av = bv; bv = tmp;
+    if (it < 2) { tmp = ao; ao = bo; bo = tmp; }
+  }
+  // 6. rows K .. K+n-1 minus the integrated cardinal corrections
+  for (int r = threadIdx.x; r < rd.nv; r += blockDim.x) {
+    double2 v = (Kv + r < LB) ? av[Kv + r] : make_double2(0.0, 0.0);
+    if (zero) {
+      v = v - red[0] * __ldg(tb.bkco + r) - red[3] * __ldg(tb.bkco + rd.no + r);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) v = v - red[m] * __ldg(tb.bkcv + (size_t)m * rd.nv + r);
+    }
+    gv[p * rd.gp + r] = v;
+  }
+  for (int r = threadIdx.x; r < rd.no; r += blockDim.x) {
+    double2 v = (2 + r < LB) ? ao[2 + r] : make_double2(0.0, 0.0);
+    v = v - red[4] * __ldg(tb.bkco + r) - red[7] * __ldg(tb.bkco + rd.no + r);
+    go[p * rd.gp + r] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
@@ -673,6 +963,15 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
                       PhysParams ph, FftTab<C> tab, cudaStream_t st) {
   return with_len_m(tab.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
+    // warp-FFT form for FP32 (the FP64 form keeps the block FFT, whose
+    // register footprint is smaller)
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+      const size_t sm = (size_t)L * sizeof(C) + 9 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) +
+                        (size_t)6 * L * sizeof(C);
+      cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab);
+      return cudaGetLastError();
+    }
     const size_t sm = y3_smem(g.Ny, FLine<C, L>::stride(tab.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y3<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_y3<C, L><<<(unsigned)g.H, 256, sm, st>>>(V, O, out, g, ph, tab);
@@ -688,6 +987,16 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
                       PhysParams ph, FftTab<C> tabP, int boot, cudaStream_t st) {
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok &&
+                  WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+      auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
+      const size_t bl = (size_t)3 * L * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
+      const size_t sm = a((size_t)L * sizeof(C)) + a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) +
+                        10 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
+      cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_y1w<C, L><<<(unsigned)g.H, 128, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
+      return cudaGetLastError();
+    }
     const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y1<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_y1<C, L><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);

@@ -17,6 +17,9 @@
 // Streamwise pass: two real rows share one complex FFT (a + i b).
 #include "fftline.cuh"
 #include "kernels.cuh"
+#include <type_traits>
+
+#include "wfft.cuh"
 #include "zxpass.cuh"
 
 namespace {
@@ -113,6 +116,100 @@ __global__ void __launch_bounds__(256, 3) k_zf(RowArr in, PencilArr out, DnsGeom
     const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
     if (kx < Kx && y < Py)
       ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * ls + FL::out_pos(n)];
+  }
+}
+
+// Same spanwise passes with warp FFTs: a TX x TY tile of 16 lines
+// (streamwise modes x wall-normal points; zf uses 4 x 4, 32-byte runs on
+// both sides, zb 8 x 2, 64-byte runs on its larger row side), NW warps with
+// 16/NW lines each, no block barrier inside the transforms.
+template <typename C, int L, int NW, int TX, int TY>
+__global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
+  constexpr int NL = TX * TY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = (C*)smem_raw;
+  constexpr int LS = L + 1;  // line stride: the 16 lines of a position fall in distinct banks
+  C* lines = tws + L;
+  constexpr int Pz = L;
+  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  const int hz = Nz / 2;
+  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
+  // zero band [Nz/2, Pz - Nz/2] (Nyquist and padding)
+  const int nzero = Pz - Nz + 1;
+  for (int t = threadIdx.x; t < NL * nzero; t += blockDim.x) {
+    const int li = t / nzero;
+    const int n = hz + (t - li * nzero);
+    lines[(size_t)li * LS + wsw<C>(n)] = cmk<C>(0.0, 0.0);
+  }
+  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
+    const int yl = t % TY;
+    const int kxl = (t / TY) % TX;
+    const int kz = t / NL;
+    if (kz == hz) continue;
+    const int n = (kz < hz) ? kz : kz + (Pz - Nz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    C v = cmk<C>(0.0, 0.0);
+    if (kx < Kx - 1 && y < Py) v = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
+    lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)] = v;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  constexpr int NLW = NL / NW;  // lines per warp
+  wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tws, LS);
+  __syncthreads();
+  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
+    const int kxl = t % TX;
+    const int zp = (t / TX) % Pz;
+    const int yl = t / (TX * Pz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    if (kx < Kx && y < Py)
+      prow<C>(out, f, (long long)y * Pz + zp)[kx] = lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)];
+  }
+}
+
+template <typename C, int L, int NW>
+__global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
+  constexpr int TX = 4, TY = 4, NL = TX * TY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tws = (C*)smem_raw;
+  constexpr int LS = L + 1;  // line stride: the 16 lines of a position fall in distinct banks
+  C* lines = tws + L;
+  constexpr int Pz = L;
+  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
+  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
+    const int kxl = t % TX;
+    const int zp = (t / TX) % Pz;
+    const int yl = t / (TX * Pz);
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    C v = cmk<C>(0.0, 0.0);
+    if (kx < Kx && y < Py) v = prow<C>(in, f, (long long)y * Pz + zp)[kx];
+    lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] = v;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  constexpr int NLW = NL / NW;  // lines per warp
+  wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tws, LS);
+  __syncthreads();
+  const int hz = Nz / 2;
+  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
+    const int yl = t % TY;
+    const int kxl = (t / TY) % TX;
+    const int kz = t / NL;
+    const int kx = kx0 + kxl;
+    const int y = y0 + yl;
+    const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
+    if (kx < Kx && y < Py)
+      ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)];
   }
 }
 
@@ -238,6 +335,94 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
   }
 }
 
+// Same pass with warp FFTs: a CTA of three warps owns four rows of one
+// wall-normal plane.  Warp w inverse-transforms lines 4w..4w+3 (line 3r+q
+// holds row r's packed pair q), reading the half spectra straight from the
+// row arrays in the first FFT pass; after a block barrier the Lamb vector of
+// the four rows is formed pointwise into lines 0-5 (lines r < 4: lambda_x +
+// i lambda_y of row r; lines 4, 5: lambda_z of rows (0, 1), (2, 3)); each
+// warp forward-transforms two of them, and the half spectra are unpacked to
+// the output rows.
+template <typename C, int L>
+__global__ void __launch_bounds__(96) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+                                          const double* __restrict__ Uy, double Ro) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  typedef T_of<C> T;
+  constexpr int Px = L;
+  const int hx = g.Nx / 2;
+  C* tws = (C*)smem_raw;
+  C* z = tws + L;  // 12 lines
+  const long long r0 = (long long)blockIdx.x * 4;
+  const long long nrows = (long long)g.Py * g.Pz;
+  const int warp = threadIdx.x >> 5;
+  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
+  __syncthreads();
+  {
+    // fields of similar magnitude share a transform: (u, v), (ox, oy), (w, oz)
+    const C* fa[4];
+    const C* fb[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int line = 4 * warp + l;
+      const int rl = line / 3, q = line - 3 * (line / 3);
+      long long row = r0 + rl;
+      if (row >= nrows) row = nrows - 1;  // duplicate work, not stored
+      fa[l] = prow<C>(in, q == 0 ? 0 : (q == 1 ? 3 : 2), row);
+      fb[l] = prow<C>(in, q == 0 ? 1 : (q == 1 ? 4 : 5), row);
+    }
+    auto ld = [&](int l, int n) -> C { return pack_c2r<C>(fa[l], fb[l], n, Px, hx); };
+    C* zw = z + (size_t)4 * warp * L;
+    auto st = [&](int l, int k, C v) { zw[(size_t)l * L + wsw<C>(k)] = v; };
+    wfft_io<C, L, 4, true>(zw, tws, ld, st);
+  }
+  __syncthreads();
+  const T ro = (T)Ro;
+  const int y = (int)(r0 / g.Pz);  // the four rows lie in one wall-normal plane
+  const T Ub = (T)Uy[y < g.Py ? y : 0];
+  for (int j = threadIdx.x; j < Px; j += blockDim.x) {
+    const int op = wsw<C>(j);
+    C A[4];
+    T lz[4];
+#pragma unroll
+    for (int rl = 0; rl < 4; ++rl) {
+      const C z0 = z[(size_t)(3 * rl + 0) * L + op];
+      const C z1 = z[(size_t)(3 * rl + 1) * L + op];
+      const C z2 = z[(size_t)(3 * rl + 2) * L + op];
+      const T u = z0.x, v = z0.y, ox = z1.x, oy = z1.y, w = z2.x, oz = z2.y;
+      A[rl].x = oz * v - oy * w - ro * w;
+      A[rl].y = ox * w - oz * u;
+      lz[rl] = oy * u - ox * v + ro * (u + Ub);
+    }
+#pragma unroll
+    for (int rl = 0; rl < 4; ++rl) z[(size_t)rl * L + op] = A[rl];
+    C B0, B1;
+    B0.x = lz[0]; B0.y = lz[1];
+    B1.x = lz[2]; B1.y = lz[3];
+    z[(size_t)4 * L + op] = B0;
+    z[(size_t)5 * L + op] = B1;
+  }
+  __syncthreads();
+  wfft<C, L, 2, false>(z + (size_t)2 * warp * L, tws);
+  __syncthreads();
+  const int Kx = g.Kx;
+  const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
+  for (int t = threadIdx.x; t < 4 * 3 * Kx; t += blockDim.x) {
+    const int k = t % Kx;
+    const int fl = (t / Kx) % 3;
+    const int rl = t / (3 * Kx);
+    const long long row = r0 + rl;
+    if (row >= nrows) continue;
+    const C* Z = (fl < 2) ? z + (size_t)rl * L : z + (size_t)(4 + rl / 2) * L;
+    const bool im = (fl < 2) ? (fl == 1) : (rl & 1);
+    const C zk = Z[wsw<C>(k)];
+    const C zm = Z[wsw<C>((Px - k) % Px)];
+    C v;
+    if (!im) { v.x = zk.x + zm.x; v.y = zk.y - zm.y; }
+    else { v.x = zk.y + zm.y; v.y = zm.x - zk.x; }
+    prow<C>(out, fl, row)[k] = v * sc;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // standalone streamwise C2R / R2C (drop-in transform_3d_one pieces)
 // complex rows in [row][kx] (pitch rs) <-> real rows [row][x] (pitch rps)
@@ -339,6 +524,14 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+      const size_t sm = ((size_t)L + 16 * (L + 1)) * sizeof(C);
+      // 8 x 2 tile: the row side (the larger, Pz > Nz) gets 64-byte runs
+      cudaFuncSetAttribute(k_zbw<C, L, 8, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      dim3 grid((g.Kx + 7) / 8, (g.Py + 1) / 2, nf);
+      k_zbw<C, L, 8, 8, 2><<<grid, 256, sm, st>>>(in, out, g, tab);
+      return cudaGetLastError();
+    }
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zb<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
@@ -351,6 +544,13 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+      const size_t sm = ((size_t)L + 16 * (L + 1)) * sizeof(C);
+      cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
+      k_zfw<C, L, 8><<<grid, 256, sm, st>>>(in, out, g, tab);
+      return cudaGetLastError();
+    }
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zf<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
@@ -363,6 +563,16 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
                            double Ro, cudaStream_t st) {
   return with_len_xz(g.Px, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 4, FftMaxRadix<C>::v>::ok &&
+                  WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+      const long long nrows = (long long)g.Py * g.Pz;
+      if (g.Pz % 4 == 0) {  // four rows per CTA within one wall-normal plane
+        const size_t sm = (size_t)13 * L * sizeof(C);
+        cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro);
+        return cudaGetLastError();
+      }
+    }
     const size_t sm = (size_t)(L > 0 ? 6 : 9) * FLine<C, L>::stride(g.Px) * sizeof(C);
     cudaFuncSetAttribute(k_x_fused<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     const long long nrows = (long long)g.Py * g.Pz;  // Pz is even: row pairs share a plane

@@ -250,6 +250,10 @@ STEP_CASES = [
     dict(mx=24, my=24, mz=32, Re=500.0, Ro=0.0, dt=0.01),
     dict(mx=36, my=48, mz=64, Re=2000.0, Ro=0.2, dt=0.002, U=(0.0, 1.0, 0.0)),
     dict(mx=48, my=36, mz=64, Re=8400.0, Ro=0.0, dt=0.002, U=(1.0, 0.0, -1.0)),
+    # wall-normal lengths of the 256x129x256 workload (padded DCT on 512 points)
+    dict(mx=48, my=48, mz=512, Re=3000.0, Ro=0.02, dt=0.001),
+    # streamwise / spanwise lengths of that workload (384-point lines)
+    dict(mx=384, my=384, mz=32, Re=3000.0, Ro=0.02, dt=0.001),
 ]
 
 
@@ -284,7 +288,7 @@ def _fresh(pb, V, Om):
     return q
 
 
-@pytest.mark.parametrize("case", STEP_CASES[:2])
+@pytest.mark.parametrize("case", STEP_CASES[:2] + STEP_CASES[4:])
 def test_step_mixed_close_to_fp64(pkg, case):
     case = dict(case)
     U = case.pop("U", (0.5, 0.5, 0.0))
