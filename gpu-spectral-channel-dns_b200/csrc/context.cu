@@ -146,7 +146,10 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
   mark();
   const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
-  const RhsTabs tb{c->rtab, c->rtab + 4 * (size_t)c->wd.nv, c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no};
+  const size_t nv = c->wd.nv, no = c->wd.no;
+  const double* t0 = c->rtab;
+  const RhsTabs tb{t0, t0 + 4 * nv, t0 + 4 * nv + 2 * no, t0 + 4 * nv + 2 * no + g.Ny,
+                   t0 + 4 * nv + 2 * no + g.Ny + 5 * nv};
   if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
                         boot, c->st)))
     return e;
@@ -305,7 +308,7 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
       (e = c->alloc(&c->ro, gn)) || (e = c->alloc(&c->status, 1)) ||
       (e = c->alloc((unsigned char**)&c->F6, f6 * csz)) ||
       (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
-      (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny)))
+      (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny + 8 * (size_t)c->wd.nv)))
     return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
   cudaMemcpy(c->T0, T0.data(), NN * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->T2, T2.data(), NN * 8, cudaMemcpyHostToDevice);
@@ -317,13 +320,17 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   {
     // y1 tables (integrated cardinal corrections, cos(k pi/N))
     const int N = Ny - 1, nv = c->wd.nv, no = c->wd.no;
-    std::vector<double> tab(4 * (size_t)nv + 2 * (size_t)no + Ny);
+    std::vector<double> tab(4 * (size_t)nv + 2 * (size_t)no + Ny + 8 * (size_t)nv);
     const int mv[4] = {0, 1, N - 1, N};
     for (int m = 0; m < 4; ++m) wall::cardinal_rows(N, mv[m], 4, nv, &tab[(size_t)m * nv]);
     wall::cardinal_rows(N, 0, 2, no, &tab[4 * (size_t)nv]);
     wall::cardinal_rows(N, N, 2, no, &tab[4 * (size_t)nv + no]);
     const long double PI = 3.141592653589793238462643383279502884L;
     for (int k = 0; k <= N; ++k) tab[4 * (size_t)nv + 2 * (size_t)no + k] = (double)cosl(PI * k / N);
+    // rows of B^4 (from row 4) and B^2 (from row 2) as 5- and 3-point stencils
+    double* b4 = &tab[4 * (size_t)nv + 2 * (size_t)no + Ny];
+    double* b2 = b4 + 5 * (size_t)nv;
+    wall::integration_stencils(N, nv, b4, b2);
     cudaMemcpy(c->rtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice);
   }
   cudaMemset(c->status, 0, sizeof(int));

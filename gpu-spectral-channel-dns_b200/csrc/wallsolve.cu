@@ -78,6 +78,9 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   double2* ring = (double2*)(smem_raw + WALL_HDR);
   double* Qs = (double*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG);
   double2* S = (double2*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG + wd.qbytes);
+  // recombination weights 2k/(k+1), (k-3)/(k-1) of the clamped basis, k <= N
+  double* rc2 = (double*)(S + (size_t)32 * wd.SP);
+  double* rc4 = rc2 + g.Ny;
 
   const int lane = threadIdx.x;
   const int q = lane >> 1, b = lane & 1;
@@ -138,6 +141,10 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   }
   __syncwarp();
   for (int k = lane; k < 7 * wd.no; k += 32) Qs[k] = Qg[k];
+  for (int k = lane; k < g.Ny; k += 32) {
+    rc2[k] = 2.0 * k / (k + 1);
+    rc4[k] = (k >= 4) ? (double)(k - 3) / (double)(k - 1) : 0.0;
+  }
   if (lane == 0) {
     mbar_expect_tx(gbar, (uint32_t)(__popc(amask) * wd.nv * 16));
     for (int c = 0; c < min(WALL_NST, total); ++c) issue(c);
@@ -169,9 +176,15 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       for (int rr = 0; rr < rows; ++rr) {
         const int i = r0 + rr;
         const double2* Lr = ch + rr * CF::E0 * 16;
-        double2 acc = Sr[i];
+        // the older entries in independent partial sums; the newest (y_{i-1})
+        // last, so only it is on the row-to-row critical path
+        double2 a0 = Sr[i], a1 = make_double2(0.0, 0.0);
 #pragma unroll
-        for (int e = 0; e < KLV; ++e) acc = acc - cmul(Lr[e * 16], yw[e]);
+        for (int e = 0; e < KLV - 1; ++e) {
+          if (e & 1) a1 = a1 + cmul(Lr[e * 16], yw[e]);
+          else a0 = a0 - cmul(Lr[e * 16], yw[e]);
+        }
+        const double2 acc = (a0 - a1) - cmul(Lr[(KLV - 1) * 16], yw[KLV - 1]);
         Sr[i] = acc;
 #pragma unroll
         for (int e = 0; e < KLV - 1; ++e) yw[e] = yw[e + 1];
@@ -209,11 +222,17 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       for (int rr = 0; rr < rows; ++rr) {
         const int i = wd.nv - 1 - (r0 + rr);
         const double2* Ur = ch + rr * CF::E1 * 16;
-        double2 acc = Sr[i];
+        double2 a0 = Sr[i];
         if (i >= N + 2) Sr[i] = make_double2(0.0, 0.0);  // no tilting term above row N+1
-        acc = acc - cmul(Ur[(KUV + 1) * 16], xd0) - cmul(Ur[(KUV + 2) * 16], xd1);
+        // independent partial sums; x_{i+1} enters last
+        double2 a1 = cmul(Ur[(KUV + 1) * 16], xd0) + cmul(Ur[(KUV + 2) * 16], xd1);
+        double2 a2 = make_double2(0.0, 0.0);
 #pragma unroll
-        for (int e = KUV; e >= 1; --e) acc = acc - cmul(Ur[e * 16], xw[e - 1]);
+        for (int e = KUV; e >= 2; --e) {
+          if (e & 1) a1 = a1 + cmul(Ur[e * 16], xw[e - 1]);
+          else a2 = a2 + cmul(Ur[e * 16], xw[e - 1]);
+        }
+        const double2 acc = (a0 - (a1 + a2)) - cmul(Ur[16], xw[0]);
         const double2 x = cmul(Ur[0], acc);
         if (i == wd.nv - 1) xd1 = x;
         if (i == wd.nv - 2) xd0 = x;
@@ -223,8 +242,7 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
         if (i < nbv) {
           if (!zero) {
             const int k = i + 4;
-            emit(k, sel(i + 4 < nbv, xw[4]) - sel(i + 2 < nbv, xw[2]) * (2.0 * k / (k + 1)) +
-                        x * ((double)(i + 1) / (double)(i + 3)));
+            emit(k, sel(i + 4 < nbv, xw[4]) - sel(i + 2 < nbv, xw[2]) * rc2[k] + x * rc4[k]);
           } else {
             emit(i + 2, x - sel(i + 2 < nbv, xw[2]));
           }
@@ -271,9 +289,13 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
         if (rr < rows) {
           const int i = r0 + rr;
           const double2* Lr = ch + rr * CF::E2 * 16;
-          double2 acc = Sr[i] + gcur[rr];
+          double2 a0 = Sr[i] + gcur[rr], a1 = make_double2(0.0, 0.0);
 #pragma unroll
-          for (int e = 0; e < KLO; ++e) acc = acc - cmul(Lr[e * 16], ow[e]);
+          for (int e = 0; e < KLO - 1; ++e) {
+            if (e & 1) a1 = a1 + cmul(Lr[e * 16], ow[e]);
+            else a0 = a0 - cmul(Lr[e * 16], ow[e]);
+          }
+          const double2 acc = (a0 - a1) - cmul(Lr[(KLO - 1) * 16], ow[KLO - 1]);
           Sr[i] = acc;
 #pragma unroll
           for (int e = 0; e < KLO - 1; ++e) ow[e] = ow[e + 1];
@@ -296,9 +318,13 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       for (int rr = 0; rr < rows; ++rr) {
         const int i = wd.no - 1 - (r0 + rr);
         const double2* Ur = ch + rr * CF::E3 * 16;
-        double2 acc = Sr[i];
+        double2 a1 = make_double2(0.0, 0.0), a2 = a1;
 #pragma unroll
-        for (int e = KUO; e >= 1; --e) acc = acc - cmul(Ur[e * 16], zw[e - 1]);
+        for (int e = KUO; e >= 2; --e) {
+          if (e & 1) a1 = a1 + cmul(Ur[e * 16], zw[e - 1]);
+          else a2 = a2 + cmul(Ur[e * 16], zw[e - 1]);
+        }
+        const double2 acc = (Sr[i] - (a1 + a2)) - cmul(Ur[16], zw[0]);
         const double2 x = cmul(Ur[0], acc);
 #pragma unroll
         for (int e = KUO - 1; e >= 1; --e) zw[e] = zw[e - 1];
@@ -315,7 +341,8 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
 }
 
 size_t wall_smem_bytes(const WallDims& wd) {
-  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)32 * wd.SP * 16;
+  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)32 * wd.SP * 16 +
+         (size_t)2 * (wd.nv + 2) * 8;
 }
 
 // band instances: base-flow degree 0, 1, 2

@@ -95,6 +95,11 @@ void integrate_rows(int K, int N, const cx* rho, int n, cx* g);
 // polynomial of the Gauss-Lobatto point y_m (1 at y_m, 0 at the others)
 void cardinal_rows(int N, int m, int K, int n, double* out);
 
+// Rows 4..4+n-1 of B^4 and 2..2+n-1 of B^2 as stencils on an (N+1)-coefficient
+// vector f: (B^4 f)_{r+4} = sum_d b4[5r + d/2 + 2] f_{r+4+d}, d = -4,-2,0,2,4;
+// (B^2 f)_{r+2} = sum_d b2[3r + d/2 + 1] f_{r+2+d}, d = -2,0,2.
+void integration_stencils(int N, int n, double* b4, double* b2);
+
 // Chebyshev coefficients (N+1) from basis unknowns: v or Dirichlet recombination
 void recombine(int eq, int N, const cx* x, cx* a);
 

@@ -327,6 +327,22 @@ void cardinal_rows(int N, int m, int K, int n, double* out) {
   for (int r = 0; r < n; ++r) out[r] = g[r].re;
 }
 
+void integration_stencils(int N, int n, double* b4, double* b2) {
+  std::fill(b4, b4 + (size_t)5 * n, 0.0);
+  std::fill(b2, b2 + (size_t)3 * n, 0.0);
+  const size_t m = (size_t)N + n + 12;
+  for (int k = 0; k <= N; ++k) {
+    Vec e(m, 0.0);
+    e[k] = 1.0;
+    const Vec e2 = int_B_pow(e, 2), e4 = int_B_pow(e2, 2);
+    for (int r = 0; r < n; ++r) {
+      const int d4 = k - (r + 4), d2 = k - (r + 2);
+      if (e4[r + 4] != 0.0 && d4 >= -4 && d4 <= 4 && (d4 & 1) == 0) b4[(size_t)5 * r + d4 / 2 + 2] = e4[r + 4];
+      if (e2[r + 2] != 0.0 && d2 >= -2 && d2 <= 2 && (d2 & 1) == 0) b2[(size_t)3 * r + d2 / 2 + 1] = e2[r + 2];
+    }
+  }
+}
+
 void recombine(int eq, int N, const cx* x, cx* a) {
   const int nb = (eq == EQ_V) ? N - 3 : N - 1;
   auto b = [&](int j) { return (j >= 0 && j < nb) ? x[j] : cx{0, 0}; };

@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 // build the derivative chains of v and omega_y; no block barrier inside the
 // transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(128) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(128, 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
@@ -829,11 +829,8 @@ __global__ void __launch_bounds__(128) k_y1w(PencilArr lam, const double2* __res
   }
   if (boot) return;
   __syncthreads();
-  // 4. values at the points the equations leave out; integration buffers
-  double2* av = (double2*)region;
-  double2* bv = av + LB;
-  double2* ao = bv + LB;
-  double2* bo = ao + LB;
+  // 4. values at the points the equations leave out (warps 0, 1) and the
+  //    K-fold integrals of fv, fo by their banded stencils (all threads)
   if (warp < 2) {
     const double2* f = warp ? fo : fv;
     double2 s0 = make_double2(0.0, 0.0), sN = s0, s1 = s0, sN1 = s0;
@@ -851,55 +848,50 @@ __global__ void __launch_bounds__(128) k_y1w(PencilArr lam, const double2* __res
     s1 = warp_sum(s1);
     sN1 = warp_sum(sN1);
     if (lane == 0) {
-      red[4 * warp + 0] = s0;
-      red[4 * warp + 1] = s1;
-      red[4 * warp + 2] = sN1;
-      red[4 * warp + 3] = sN;
+      red[4 * warp + 0] = s0;   // y = 1
+      red[4 * warp + 1] = s1;   // y_1
+      red[4 * warp + 2] = sN1;  // y_{N-1}
+      red[4 * warp + 3] = sN;   // y = -1
     }
-  } else {
-    for (int t = threadIdx.x - 64; t < 2 * LB; t += blockDim.x - 64) {
-      const int f = t / LB;
-      const int k = t - f * LB;
-      (f ? ao : av)[k] = (k <= N) ? (f ? fo : fv)[k] : make_double2(0.0, 0.0);
+  }
+  auto fget = [&](const double2* f, int k) { return (k >= 0 && k <= N) ? f[k] : make_double2(0.0, 0.0); };
+  constexpr int RPT = 2;  // rows per thread (n <= 2 * blockDim = 256)
+  double2 iv[RPT], io[RPT];
+#pragma unroll
+  for (int t = 0; t < RPT; ++t) {
+    const int r = threadIdx.x + t * blockDim.x;
+    iv[t] = make_double2(0.0, 0.0);
+    io[t] = make_double2(0.0, 0.0);
+    if (r < rd.nv) {
+      if (zero) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) iv[t] = iv[t] + fget(fv, r + 2 + 2 * d - 2) * __ldg(tb.b2 + 3 * r + d);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 5; ++d) iv[t] = iv[t] + fget(fv, r + 4 + 2 * d - 4) * __ldg(tb.b4 + 5 * r + d);
+      }
+    }
+    if (r < rd.no) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) io[t] = io[t] + fget(fo, r + 2 + 2 * d - 2) * __ldg(tb.b2 + 3 * r + d);
     }
   }
   __syncthreads();
-  // 5. Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
-  const int Kv = zero ? 2 : 4;
-  for (int it = 0; it < Kv; ++it) {
-    const int nf = (it < 2) ? 2 : 1;
-    for (int t = threadIdx.x; t < nf * LB; t += blockDim.x) {
-      const int f = t / LB;
-      const int k = t - f * LB;
-      const double2* x = f ? ao : av;
-      double2* y = f ? bo : bv;
-      double2 r = make_double2(0.0, 0.0);
-      if (k >= 1) {
-        const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
-        const double2 xp = (k + 1 < LB) ? x[k + 1] : make_double2(0.0, 0.0);
-        r = (xm - xp) * (1.0 / (2.0 * k));
-      }
-      y[k] = r;
-    }
-    __syncthreads();
-    double2* tmp = av; av = bv; bv = tmp;
-    if (it < 2) { tmp = ao; ao = bo; bo = tmp; }
-  }
-  // 6. rows K .. K+n-1 minus the integrated cardinal corrections
-  for (int r = threadIdx.x; r < rd.nv; r += blockDim.x) {
-    double2 v = (Kv + r < LB) ? av[Kv + r] : make_double2(0.0, 0.0);
-    if (zero) {
-      v = v - red[0] * __ldg(tb.bkco + r) - red[3] * __ldg(tb.bkco + rd.no + r);
-    } else {
+  // 5. minus the integrated cardinal corrections, out
 #pragma unroll
-      for (int m = 0; m < 4; ++m) v = v - red[m] * __ldg(tb.bkcv + (size_t)m * rd.nv + r);
+  for (int t = 0; t < RPT; ++t) {
+    const int r = threadIdx.x + t * blockDim.x;
+    if (r < rd.nv) {
+      double2 v = iv[t];
+      if (zero) {
+        v = v - red[0] * __ldg(tb.bkco + r) - red[3] * __ldg(tb.bkco + rd.no + r);
+      } else {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) v = v - red[m] * __ldg(tb.bkcv + (size_t)m * rd.nv + r);
+      }
+      gv[p * rd.gp + r] = v;
     }
-    gv[p * rd.gp + r] = v;
-  }
-  for (int r = threadIdx.x; r < rd.no; r += blockDim.x) {
-    double2 v = (2 + r < LB) ? ao[2 + r] : make_double2(0.0, 0.0);
-    v = v - red[4] * __ldg(tb.bkco + r) - red[7] * __ldg(tb.bkco + rd.no + r);
-    go[p * rd.gp + r] = v;
+    if (r < rd.no) go[p * rd.gp + r] = io[t] - red[4] * __ldg(tb.bkco + r) - red[7] * __ldg(tb.bkco + rd.no + r);
   }
 }
 

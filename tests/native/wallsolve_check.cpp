@@ -101,4 +101,39 @@ int ws_integrate_values(int K, int N, int n, const double* vals, double* g) {
   return 0;
 }
 
+// max |stencil - integrate_rows| over random vectors, K = 4 and 2
+double ws_stencil_err(int N, int n) {
+  std::vector<double> b4((size_t)5 * n), b2((size_t)3 * n);
+  wall::integration_stencils(N, n, b4.data(), b2.data());
+  std::vector<cx> f(N + 1), g4(n), g2(n);
+  unsigned s = 12345;
+  for (auto& x : f) {
+    s = s * 1103515245u + 12345u;
+    x.re = (double)(s >> 8) / (1 << 24) - 0.5;
+    s = s * 1103515245u + 12345u;
+    x.im = (double)(s >> 8) / (1 << 24) - 0.5;
+  }
+  wall::integrate_rows(4, N, f.data(), n, g4.data());
+  wall::integrate_rows(2, N, f.data(), n, g2.data());
+  auto fg = [&](int k) { return (k >= 0 && k <= N) ? f[k] : cx{0, 0}; };
+  double err = 0, mx = 0;
+  for (int r = 0; r < n; ++r) {
+    cx a{0, 0}, b{0, 0};
+    for (int d = 0; d < 5; ++d) {
+      const cx v = fg(r + 4 + 2 * d - 4);
+      a.re += v.re * b4[5 * r + d];
+      a.im += v.im * b4[5 * r + d];
+    }
+    for (int d = 0; d < 3; ++d) {
+      const cx v = fg(r + 2 + 2 * d - 2);
+      b.re += v.re * b2[3 * r + d];
+      b.im += v.im * b2[3 * r + d];
+    }
+    err = std::fmax(err, std::fmax(std::hypot(a.re - g4[r].re, a.im - g4[r].im),
+                                   std::hypot(b.re - g2[r].re, b.im - g2[r].im)));
+    mx = std::fmax(mx, std::fmax(std::hypot(g4[r].re, g4[r].im), std::hypot(g2[r].re, g2[r].im)));
+  }
+  return err / mx;
+}
+
 }  // extern "C"

@@ -148,3 +148,10 @@ def test_tilting_table(ws, N, U3):
     out = np.zeros(n, dtype=np.complex128)
     assert ws.ws_tilt(C.c_int(N), C.c_int(n), C.c_double(U3[1]), C.c_double(U3[2]), dp(w), dp(out)) == 0
     assert np.max(np.abs(out - ref)) <= 1e-13 * max(np.max(np.abs(ref)), 1e-300) + 1e-15
+
+
+@pytest.mark.parametrize("N,n", [(8, 10), (32, 34), (128, 130), (192, 195)])
+def test_integration_stencils(ws, N, n):
+    """The banded stencils the y1 kernel applies equal the K-fold integration."""
+    ws.ws_stencil_err.restype = C.c_double
+    assert ws.ws_stencil_err(C.c_int(N), C.c_int(n)) < 1e-15
