@@ -79,20 +79,29 @@ def wall_dims(g, U):
 
 
 def kernel_bytes(g, c, U=(0.5, 0.5, 0.0)):
+    """Algorithmic bytes per launch, by the pencil-pass model: each pass reads
+    its input fields once and writes its output fields once (padded
+    transforms at c bytes per complex value); the FP64 state and the AB2
+    history (16 B complex) are read and written once per step.  The banded
+    factors the wall solve streams are implementation cost, reported apart
+    (factor_bytes)."""
     Kx, Nz, Ny, Py, Pz = g["Kx"], g["Nz"], g["Ny"], g["Py"], g["Pz"]
     H = Kx * Nz
     s = 16
-    n, fac = wall_dims(g, U)
     return {
-        "y3_uvw_s2p": s * 2 * H * Ny + c * 6 * H * Py,
-        "zb_span_inverse": c * 6 * H * Py + c * 6 * Kx * Pz * Py,
-        "x_c2r_lamb_r2c": c * 6 * Kx * Pz * Py + c * 3 * Kx * Pz * Py,
-        "zf_span_forward": c * 3 * Kx * Pz * Py + c * 3 * H * Py,
-        # lambda in; v, omega, history in; history and the two integrated rhs out
-        "y1_p2s_rhs": c * 3 * H * Py + s * 4 * H * Ny + s * 2 * H * Ny + s * 2 * H * n,
-        # banded factors and the two integrated rhs in, v and omega out
-        "y2_solve": fac + s * 2 * H * n + s * 2 * H * Ny,
+        "y3_uvw_s2p": s * 2 * H * Ny + c * 6 * H * Py,                  # v, omega in; 6 fields out
+        "zb_span_inverse": c * 6 * H * Py + c * 6 * Kx * Pz * Py,       # pad Nz -> Pz
+        "x_c2r_lamb_r2c": c * 6 * Kx * Pz * Py + c * 3 * Kx * Pz * Py,  # read 6, write 3
+        "zf_span_forward": c * 3 * Kx * Pz * Py + c * 3 * H * Py,       # truncate Pz -> Nz
+        # lambda in; v, omega, history in; history out
+        "y1_p2s_rhs": c * 3 * H * Py + s * 6 * H * Ny,
+        # v, omega out
+        "y2_solve": s * 2 * H * Ny,
     }
+
+
+def factor_bytes(g, U=(0.5, 0.5, 0.0)):
+    return wall_dims(g, U)[1]
 
 
 def measured_peaks():
@@ -120,7 +129,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -313,19 +322,33 @@ def run_one(args):
     return {"only": args.only, "config": args.config, "kernel_ms": {k: round(v, 4) for k, v in kms.items()}}
 
 
-def roofline(kms, geo, c, peak):
+def measured_traffic(kernel, config, prec):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of one ncu capture, from the committed summary profiles/dram_traffic.json
+    (None when that kernel, workload and precision were not captured)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            d = json.load(f)
+        e = d["captures"][f"{config}/{prec}/{kernel}"]
+        return int(e["read"] + e["write"])
+    except Exception:
+        return None
+
+
+def roofline(kms, geo, c, peak, config="256x129x256", prec="mixed"):
     kb = kernel_bytes(geo, c)
     top = max(kms, key=kms.get)
     achieved = kb[top] / (kms[top] * 1e-3) / 1e9
     return top, {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                 "unit": "GB/s", "frac": round(achieved / peak, 4),
+                 "traffic": measured_traffic(top, config, prec),
                  "bytes_per_launch": kb[top], "ms_per_launch": round(kms[top], 4)}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -357,8 +380,8 @@ def main():
         return
     r = run_ours(args, rank, world)
     peak, peak_kind = measured_peaks()
-    top64, roof64 = roofline(r["kms64"], r["geo"], 16, peak)
-    topmx, roofmx = roofline(r["kmsmx"], r["geo"], 8, peak)
+    top64, roof64 = roofline(r["kms64"], r["geo"], 16, peak, args.config, "fp64")
+    topmx, roofmx = roofline(r["kmsmx"], r["geo"], 8, peak, args.config, "mixed")
     step_bytes64 = sum(kernel_bytes(r["geo"], 16).values())
     step_bytes_mx = sum(kernel_bytes(r["geo"], 8).values())
     out = None
@@ -394,6 +417,8 @@ def main():
                               "after_steps": args.steps + args.warmup},
             "roofline": dict(roofmx, peak_kind=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"),
             "step_frac_of_peak": round(step_bytes_mx / (r["msmx"] * 1e-3) / 1e9 / peak, 4),
+            "step_bytes_algorithmic": step_bytes_mx,
+            "factor_bytes_per_step": factor_bytes(r["geo"]),
             "kernel_ms": {"fp64": {k: round(v, 4) for k, v in r["kms64"].items()},
                           "mixed": {k: round(v, 4) for k, v in r["kmsmx"].items()}},
             "e2e": {"value": round(n * 1000.0 / r["e2e_ms"], 2), "unit": "steps/s",
