@@ -37,7 +37,7 @@ struct Carve {
 // Chebyshev coefficient derivative executed by one full warp:
 // b_i = sum_{j>i, j-i odd} 2 j a_j, b_0 halved (source/RPCFKernels.cu:476-520),
 // evaluated as parity-split suffix sums.  a, b in shared memory, no alias.
-__device__ void ddz_warp(const double2* a, double2* b, int N) {
+__device__ __noinline__ void ddz_warp(const double2* a, double2* b, int N) {
   const int lane = threadIdx.x & 31;
   const int c = (N + 31) / 32;
   const int j0 = lane * c;
@@ -479,7 +479,12 @@ __device__ __forceinline__ double2 y2mul(const double2* X, int j, int N) {
 }
 // coefficient k of the Gauss-Lobatto interpolant of U(y) X(y)
 __device__ __forceinline__ double2 umul_gl(const double2* X, int k, int N, const PhysParams& ph) {
-  auto u = [&](int j) { return cget(X, j, N) * ph.U0 + ymul(X, j, N) * ph.U1 + y2mul(X, j, N) * ph.U2; };
+  const bool quad = ph.U2 != 0.0;
+  auto u = [&](int j) {
+    double2 r = cget(X, j, N) * ph.U0 + ymul(X, j, N) * ph.U1;
+    if (quad) r = r + y2mul(X, j, N) * ph.U2;
+    return r;
+  };
   double2 r = u(k);
   if (k == N - 1 || k == N - 2) r = r + u(2 * N - k);
   return r;
@@ -698,12 +703,11 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   }
 }
 
-// Same pass with warp FFTs: warp 0 transforms lambda_x and lambda_y and
-// differentiates them, warp 1 transforms lambda_z, while warps 2 and 3
-// build the derivative chains of v and omega_y; no block barrier inside the
-// transforms.
+// Same pass with warp FFTs: warps 0-2 transform one Lamb line each (0 and 1
+// also differentiate theirs), while warps 3 and 4 build the derivative
+// chains of v and omega_y; no block barrier inside the transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(128, 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
@@ -751,35 +755,25 @@ __global__ void __launch_bounds__(128, 4) k_y1w(PencilArr lam, const double2* __
       noc[n] = Nop[p * Ny + n];
     }
   __syncthreads();
-  // 2. transforms (warp 0: lambda_x, lambda_y; warp 1: lambda_z), read from
-  //    the pencils as even extensions, coefficients written to lc; then the
-  //    derivatives (warp 0: D lambda_x, D lambda_y; warps 2, 3: chains of
-  //    v and omega_y)
+  // 2. transforms, one Lamb line per warp (0: lambda_x, 1: lambda_y,
+  //    2: lambda_z), read from the pencils as even extensions, coefficients
+  //    written to lc, and the warp's own derivative (D lambda_x, D lambda_y);
+  //    warps 3 and 4 build the derivative chains of v and omega_y meanwhile
   const double sc = 1.0 / (Py - 1);
-  if (warp < 2) {
-    const int f0 = warp == 0 ? 0 : 2;
-    const C* src0 = pencil_ptr<C>(lam, f0, p);
-    const C* src1 = pencil_ptr<C>(lam, f0 + 1, p);
-    auto ld = [&](int l, int n) -> C {
-      const C* src = l ? src1 : src0;
-      return (n < Py) ? src[n] : src[M - n];
-    };
-    auto st = [&](int l, int k, C val) {
+  if (warp < 3) {
+    const C* src = pencil_ptr<C>(lam, warp, p);
+    double2* lf = lc + (size_t)warp * Ny;
+    auto ld = [&](int, int n) -> C { return (n < Py) ? src[n] : src[M - n]; };
+    auto st = [&](int, int k, C val) {
       if (k < Ny) {
         double2 c = to_d2(val) * sc;
         if (k == 0) c = c * 0.5;
-        lc[(size_t)(f0 + l) * Ny + k] = c;
+        lf[k] = c;
       }
     };
-    if (warp == 0) {
-      wfft_io<C, M, 2, false>(lines, tws, ld, st);
-      ddz_warp(lc, D1, Ny);
-      __syncwarp();
-      ddz_warp(lc + Ny, D1 + Ny, Ny);
-    } else {
-      wfft_io<C, M, 1, false>(lines + (size_t)2 * M, tws, ld, st);
-    }
-  } else if (!boot && warp == 2) {
+    wfft_io<C, M, 1, false>(lines + (size_t)warp * M, tws, ld, st);
+    if (warp < 2) ddz_warp(lf, D1 + (size_t)warp * Ny, Ny);
+  } else if (!boot && warp == 3) {
     ddz_warp(Vc, DV, Ny);
     __syncwarp();
     ddz_warp(DV, D2V, Ny);
@@ -787,7 +781,7 @@ __global__ void __launch_bounds__(128, 4) k_y1w(PencilArr lam, const double2* __
     ddz_warp(D2V, D3V, Ny);
     __syncwarp();
     ddz_warp(D3V, D4V, Ny);
-  } else if (!boot && warp == 3) {
+  } else if (!boot && warp == 4) {
     ddz_warp(Oc, DO, Ny);
     __syncwarp();
     ddz_warp(DO, D2O, Ny);
@@ -979,14 +973,13 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
                       PhysParams ph, FftTab<C> tabP, int boot, cudaStream_t st) {
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok &&
-                  WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
       const size_t bl = (size_t)3 * L * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
       const size_t sm = a((size_t)L * sizeof(C)) + a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) +
                         10 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
       cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_y1w<C, L><<<(unsigned)g.H, 128, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
+      k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
       return cudaGetLastError();
     }
     const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L), sizeof(C));

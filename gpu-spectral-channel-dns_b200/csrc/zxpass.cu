@@ -144,31 +144,53 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
     const int n = hz + (t - li * nzero);
     lines[(size_t)li * LS + wsw<C>(n)] = cmk<C>(0.0, 0.0);
   }
-  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
-    const int yl = t % TY;
-    const int kxl = (t / TY) % TX;
-    const int kz = t / NL;
-    if (kz == hz) continue;
-    const int n = (kz < hz) ? kz : kz + (Pz - Nz);
-    const int kx = kx0 + kxl;
-    const int y = y0 + yl;
-    C v = cmk<C>(0.0, 0.0);
-    if (kx < Kx - 1 && y < Py) v = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
-    lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)] = v;
+  // loads in batches of ZB independent requests per thread before their stores
+  constexpr int ZB = 8;
+  for (int t0 = threadIdx.x; t0 < Nz * NL; t0 += ZB * (int)blockDim.x) {
+    C v[ZB];
+    int pos[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int yl = t % TY;
+      const int kxl = (t / TY) % TX;
+      const int kz = t / NL;
+      const int n = (kz < hz) ? kz : kz + (Pz - Nz);
+      const int kx = kx0 + kxl;
+      const int y = y0 + yl;
+      v[u] = cmk<C>(0.0, 0.0);
+      pos[u] = (t < Nz * NL && kz != hz) ? (kxl * TY + yl) * LS + wsw<C>(n) : -1;
+      if (pos[u] >= 0 && kx < Kx - 1 && y < Py) v[u] = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u)
+      if (pos[u] >= 0) lines[pos[u]] = v[u];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
   wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tws, LS);
   __syncthreads();
-  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
-    const int kxl = t % TX;
-    const int zp = (t / TX) % Pz;
-    const int yl = t / (TX * Pz);
-    const int kx = kx0 + kxl;
-    const int y = y0 + yl;
-    if (kx < Kx && y < Py)
-      prow<C>(out, f, (long long)y * Pz + zp)[kx] = lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)];
+  for (int t0 = threadIdx.x; t0 < TY * Pz * TX; t0 += ZB * (int)blockDim.x) {
+    C v[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int kxl = t % TX;
+      const int zp = (t / TX) % Pz;
+      const int yl = t / (TX * Pz);
+      v[u] = (t < TY * Pz * TX) ? lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] : cmk<C>(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int kxl = t % TX;
+      const int zp = (t / TX) % Pz;
+      const int yl = t / (TX * Pz);
+      const int kx = kx0 + kxl;
+      const int y = y0 + yl;
+      if (t < TY * Pz * TX && kx < Kx && y < Py) prow<C>(out, f, (long long)y * Pz + zp)[kx] = v[u];
+    }
   }
 }
 
@@ -185,15 +207,29 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
   for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
-  for (int t = threadIdx.x; t < TY * Pz * TX; t += blockDim.x) {
-    const int kxl = t % TX;
-    const int zp = (t / TX) % Pz;
-    const int yl = t / (TX * Pz);
-    const int kx = kx0 + kxl;
-    const int y = y0 + yl;
-    C v = cmk<C>(0.0, 0.0);
-    if (kx < Kx && y < Py) v = prow<C>(in, f, (long long)y * Pz + zp)[kx];
-    lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] = v;
+  // loads in batches of ZB independent requests per thread before their stores
+  constexpr int ZB = 8;
+  for (int t0 = threadIdx.x; t0 < TY * Pz * TX; t0 += ZB * (int)blockDim.x) {
+    C v[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int kxl = t % TX;
+      const int zp = (t / TX) % Pz;
+      const int yl = t / (TX * Pz);
+      const int kx = kx0 + kxl;
+      const int y = y0 + yl;
+      v[u] = cmk<C>(0.0, 0.0);
+      if (t < TY * Pz * TX && kx < Kx && y < Py) v[u] = prow<C>(in, f, (long long)y * Pz + zp)[kx];
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int kxl = t % TX;
+      const int zp = (t / TX) % Pz;
+      const int yl = t / (TX * Pz);
+      if (t < TY * Pz * TX) lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] = v[u];
+    }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5;
@@ -201,15 +237,27 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tws, LS);
   __syncthreads();
   const int hz = Nz / 2;
-  for (int t = threadIdx.x; t < Nz * NL; t += blockDim.x) {
-    const int yl = t % TY;
-    const int kxl = (t / TY) % TX;
-    const int kz = t / NL;
-    const int kx = kx0 + kxl;
-    const int y = y0 + yl;
-    const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
-    if (kx < Kx && y < Py)
-      ppen<C>(out, f, (long long)kz * Kx + kx)[y] = lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)];
+  for (int t0 = threadIdx.x; t0 < Nz * NL; t0 += ZB * (int)blockDim.x) {
+    C v[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int yl = t % TY;
+      const int kxl = (t / TY) % TX;
+      const int kz = t / NL;
+      const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
+      v[u] = (t < Nz * NL) ? lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)] : cmk<C>(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int yl = t % TY;
+      const int kxl = (t / TY) % TX;
+      const int kz = t / NL;
+      const int kx = kx0 + kxl;
+      const int y = y0 + yl;
+      if (t < Nz * NL && kx < Kx && y < Py) ppen<C>(out, f, (long long)kz * Kx + kx)[y] = v[u];
+    }
   }
 }
 
