@@ -203,10 +203,14 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
 #pragma unroll
     for (int j = 0; j < 7; ++j) P[j] = make_double2(0.0, 0.0);
     const int nbv = zero ? N - 1 : N - 3;
+    // base-flow degree (KLV = deg U + 4): U' = U1 (degree 1) makes the
+    // tilting operator B^2 U1, three diagonals; U' = 0 (degree 0) none
+    constexpr int DEG = KLV - 4;
     auto emit = [&](int k, double2 a) {
       if (active) V[pen * Ny + k] = a;
 #pragma unroll
       for (int j = 0; j < 7; ++j) {
+        if (DEG == 0 || (DEG == 1 && (j & 1) == 0)) continue;
         const int r = k + 1 - j;
         if (r >= 0 && r < wd.no) P[j] = P[j] + a * Qs[7 * r + j];
       }

@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 #include <type_traits>
 
+#include "mbar.cuh"
 #include "wfft.cuh"
 #include "zxpass.cuh"
 
@@ -392,34 +393,51 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
 // warp forward-transforms two of them, and the half spectra are unpacked to
 // the output rows.
 template <typename C, int L>
-__global__ void __launch_bounds__(96) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
-                                          const double* __restrict__ Uy, double Ro) {
+__global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+                                          const double* __restrict__ Uy, double Ro, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
   constexpr int Px = L;
   const int hx = g.Nx / 2;
   C* tws = (C*)smem_raw;
-  C* z = tws + L;  // 12 lines
+  C* z = tws + L;                                       // 12 lines
+  uint64_t* bars = (uint64_t*)(z + (size_t)12 * L);      // one per warp
   const long long r0 = (long long)blockIdx.x * 4;
   const long long nrows = (long long)g.Py * g.Pz;
-  const int warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* zw = z + (size_t)4 * warp * L;
+  // stage this warp's 8 half-spectrum rows (bins 0..hx-1, 16 B aligned) at
+  // the start of its own lines: the first FFT pass reads them all before it
+  // writes its output over them
+  constexpr int SR = 128;  // staged bins per row (>= hx)
+  uint64_t* bar = bars + warp;
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(bar, 8 * SR * sizeof(C));
+  }
+  __syncwarp();
+  if (lane < 8) {
+    const int line = 4 * warp + (lane >> 1);
+    const int rl = line / 3, q = line - 3 * (line / 3);
+    long long row = r0 + rl;
+    if (row >= nrows) row = nrows - 1;  // duplicate work, not stored
+    // fields of similar magnitude share a transform: (u, v), (ox, oy), (w, oz)
+    const int fa = q == 0 ? 0 : (q == 1 ? 3 : 2), fb = q == 0 ? 1 : (q == 1 ? 4 : 5);
+    bulk_g2s(zw + (size_t)lane * SR, prow<C>(in, (lane & 1) ? fb : fa, row), SR * sizeof(C), bar);
+  }
   for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
+  if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, 1LL << 31, status))) {
+    if (lane == 0) {
+      atomicOr(status, 1);
+      mbar_wait_bounded(bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+    }
+    return;
+  }
   __syncthreads();
   {
-    // fields of similar magnitude share a transform: (u, v), (ox, oy), (w, oz)
-    const C* fa[4];
-    const C* fb[4];
-#pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const int line = 4 * warp + l;
-      const int rl = line / 3, q = line - 3 * (line / 3);
-      long long row = r0 + rl;
-      if (row >= nrows) row = nrows - 1;  // duplicate work, not stored
-      fa[l] = prow<C>(in, q == 0 ? 0 : (q == 1 ? 3 : 2), row);
-      fb[l] = prow<C>(in, q == 0 ? 1 : (q == 1 ? 4 : 5), row);
-    }
-    auto ld = [&](int l, int n) -> C { return pack_c2r<C>(fa[l], fb[l], n, Px, hx); };
-    C* zw = z + (size_t)4 * warp * L;
+    const C* stg = zw;
+    auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
     auto st = [&](int l, int k, C v) { zw[(size_t)l * L + wsw<C>(k)] = v; };
     wfft_io<C, L, 4, true>(zw, tws, ld, st);
   }
@@ -454,20 +472,33 @@ __global__ void __launch_bounds__(96) k_xw(RowArr in, RowArr out, DnsGeom g, Fft
   __syncthreads();
   const int Kx = g.Kx;
   const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
-  for (int t = threadIdx.x; t < 4 * 3 * Kx; t += blockDim.x) {
-    const int k = t % Kx;
-    const int fl = (t / Kx) % 3;
-    const int rl = t / (3 * Kx);
-    const long long row = r0 + rl;
-    if (row >= nrows) continue;
-    const C* Z = (fl < 2) ? z + (size_t)rl * L : z + (size_t)(4 + rl / 2) * L;
-    const bool im = (fl < 2) ? (fl == 1) : (rl & 1);
-    const C zk = Z[wsw<C>(k)];
-    const C zm = Z[wsw<C>((Px - k) % Px)];
-    C v;
-    if (!im) { v.x = zk.x + zm.x; v.y = zk.y - zm.y; }
-    else { v.x = zk.y + zm.y; v.y = zm.x - zk.x; }
-    prow<C>(out, fl, row)[k] = v * sc;
+  constexpr int XB = 8;  // outputs per thread per batch: shared loads first
+  for (int t0 = threadIdx.x; t0 < 4 * 3 * Kx; t0 += XB * (int)blockDim.x) {
+    C zk[XB], zm[XB];
+#pragma unroll
+    for (int u = 0; u < XB; ++u) {
+      const int t = min(t0 + u * (int)blockDim.x, 4 * 3 * Kx - 1);
+      const int k = t % Kx;
+      const int fl = (t / Kx) % 3;
+      const int rl = t / (3 * Kx);
+      const C* Z = (fl < 2) ? z + (size_t)rl * L : z + (size_t)(4 + rl / 2) * L;
+      zk[u] = Z[wsw<C>(k)];
+      zm[u] = Z[wsw<C>((Px - k) % Px)];
+    }
+#pragma unroll
+    for (int u = 0; u < XB; ++u) {
+      const int t = t0 + u * blockDim.x;
+      const int k = t % Kx;
+      const int fl = (t / Kx) % 3;
+      const int rl = t / (3 * Kx);
+      const long long row = r0 + rl;
+      if (t >= 4 * 3 * Kx || row >= nrows) continue;
+      const bool im = (fl < 2) ? (fl == 1) : (rl & 1);
+      C v;
+      if (!im) { v.x = zk[u].x + zm[u].x; v.y = zk[u].y - zm[u].y; }
+      else { v.x = zk[u].y + zm[u].y; v.y = zm[u].x - zk[u].x; }
+      prow<C>(out, fl, row)[k] = v * sc;
+    }
   }
 }
 
@@ -608,16 +639,19 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
 }
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
-                           double Ro, cudaStream_t st) {
+                           double Ro, int* status, cudaStream_t st) {
   return with_len_xz(g.Px, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 4, FftMaxRadix<C>::v>::ok &&
                   WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
       const long long nrows = (long long)g.Py * g.Pz;
-      if (g.Pz % 4 == 0) {  // four rows per CTA within one wall-normal plane
-        const size_t sm = (size_t)13 * L * sizeof(C);
+      // four rows per CTA within one wall-normal plane; a warp's 8 staged
+      // rows of 128 bins fit in its 4 lines
+      if (g.Pz % 4 == 0 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * L && in.rs >= 128 && in.rs % 2 == 0 &&
+          in.fs % 2 == 0) {
+        const size_t sm = (size_t)13 * L * sizeof(C) + 64;
         cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro);
+        k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
         return cudaGetLastError();
       }
     }
@@ -661,7 +695,7 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
   template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
   template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
-                                         double, cudaStream_t);                                   \
+                                         double, int*, cudaStream_t);                             \
   template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \
                                        FftTab<C>, cudaStream_t);                                  \
   template cudaError_t launch_x_r2c<C>(const T_of<C>*, long long, RowArr, long long, DnsGeom,     \

@@ -8,7 +8,7 @@ template <typename C>
 cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st);
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
-                           double Ro, cudaStream_t st);
+                           double Ro, int* status, cudaStream_t st);
 template <typename C>
 cudaError_t launch_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
                          FftTab<C> tab, cudaStream_t st);
