@@ -215,6 +215,21 @@ def cpu_baseline():
             "step_seconds": step_s}
 
 
+def dist_max(x):
+    """Maximum over the ranks of a time-like float, on the process group's
+    device (CUDA for NCCL, host for gloo)."""
+    import torch
+    dev = "cuda" if torch.distributed.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_ranks, ms_per_step_max):
+    """Whole-job steps/s of n independent replicas timed as the slowest rank."""
+    return n_ranks * 1000.0 / ms_per_step_max
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -246,9 +261,7 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = dist_max(ms)
         return ms / K
 
     def rel(a, b):
@@ -311,9 +324,7 @@ def run_ours(args, rank, world):
             raise RuntimeError(lib.dns_last_error().decode())
     e2e_ms = (time.perf_counter() - t0) * 1e3 / K
     if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = dist_max(e2e_ms)
     geo = dict(Kx=cmx.Kx, Nz=cmx.Nz, Ny=cmx.Ny, Py=cmx.Py, Pz=cmx.Pz)
     mem = cmx.memory_bytes()
     cmx.close()
@@ -408,7 +419,7 @@ def main():
     if rank == 0:
         cpu = None if (args.no_cpu_baseline or world > 1 or args.config != "256x129x256") else cpu_baseline()
         n = world
-        value = n * 1000.0 / r["msmx"]
+        value = replica_value(n, r["msmx"])
         out = {
             "metric": METRIC,
             "value": round(value, 2),
@@ -428,7 +439,7 @@ def main():
                                     f"Ro {CFG['Ro']:g}, dt {CFG['dt']:g}"),
                        "parallelism": f"replicas x{n}" if n > 1 else "single GPU",
                        "l2": "per-step working set ~10-16 GB >> 126 MB L2 (no flush needed)"},
-            "fp64": {"steps_per_s": round(n * 1000.0 / r["ms64"], 2), "ms_per_step": round(r["ms64"], 4),
+            "fp64": {"steps_per_s": round(replica_value(n, r["ms64"]), 2), "ms_per_step": round(r["ms64"], 4),
                      "roofline": roof64, "step_bytes_algorithmic": step_bytes64,
                      "step_frac_of_peak": round(step_bytes64 / (r["ms64"] * 1e-3) / 1e9 / peak, 4)},
             "mixed_vs_fp64": {"speedup": round(r["ms64"] / r["msmx"], 3),
@@ -443,7 +454,7 @@ def main():
             "factor_bytes_per_step": factor_bytes(r["geo"]),
             "kernel_ms": {"fp64": {k: round(v, 4) for k, v in r["kms64"].items()},
                           "mixed": {k: round(v, 4) for k, v in r["kmsmx"].items()}},
-            "e2e": {"value": round(n * 1000.0 / r["e2e_ms"], 2), "unit": "steps/s",
+            "e2e": {"value": round(replica_value(n, r["e2e_ms"]), 2), "unit": "steps/s",
                     "h2d_bytes_per_step": r["state_bytes"], "d2h_bytes_per_step": r["state_bytes"]},
             "gpu_launches": 6 * args.steps,
             "cpu_baseline": cpu,

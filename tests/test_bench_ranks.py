@@ -1,0 +1,64 @@
+"""Host logic of the multi-GPU bench path on CPU (gloo, two ranks).
+
+``bench.py --gpus N`` runs N independent replicas (the step does not shard
+at the workload size); each rank times its own replica on the device and the
+job reports the slowest rank's time and the sum of the replicas' steps/s.
+Here two gloo ranks check the max-over-ranks reduction and the replica
+accounting; the reference arm exits without work on ranks other than 0.
+"""
+import importlib.util
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    b = _bench()
+    ms = b.dist_max(2.0 + 3.0 * rank)  # rank 1 is the slower replica
+    q.put((rank, ms, b.replica_value(world, ms)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo():
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs)
+    got = sorted(q.get(timeout=5) for _ in range(2))
+    for rank, ms, value in got:
+        assert ms == 5.0                      # both ranks see the slowest time
+        assert value == pytest.approx(400.0)  # 2 replicas x 1000 / 5 ms
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--gpus", "2"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == ""
