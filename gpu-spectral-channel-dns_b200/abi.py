@@ -28,6 +28,7 @@ EXPORTS = [
     "dns_transform_3d_one", "dns_transform", "dns_cuda_transpose", "dns_cheby_s2p",
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
+    "dns_write_recovery", "dns_read_recovery", "dns_write_fields",
 ]
 
 
@@ -89,6 +90,9 @@ def load_library(path: str | None = None):
         "dns_set_state": [vp, vp, vp, sz, i],
         "dns_get_state": [vp, vp, vp, sz, i],
         "dns_get_history": [vp, vp, vp, sz, i],
+        "dns_write_recovery": [vp, C.c_char_p],
+        "dns_read_recovery": [vp, C.c_char_p],
+        "dns_write_fields": [vp, C.c_char_p, C.c_char_p],
         "dns_set_history": [vp, vp, vp, sz, i],
         "dns_bootstrap": [vp],
         "dns_step": [vp, i],
@@ -220,6 +224,19 @@ class Context:
         Nv = self._pencils(Nv)
         No = self._pencils(No)
         self._call("dns_set_history", Nv.ctypes.data, No.ctypes.data, self.Ny * 16, HOST)
+
+    def write_recovery(self, path):
+        """The reference's recovery file (write_recover_data)."""
+        self._call("dns_write_recovery", os.fsencode(path))
+
+    def read_recovery(self, path):
+        """Restore state and AB2 history from a recovery file."""
+        self._call("dns_read_recovery", os.fsencode(path))
+
+    def write_fields(self, velocity_path=None, vorticity_path=None):
+        """The reference's output_velocity files (physical u, v, w and vorticity)."""
+        self._call("dns_write_fields", None if velocity_path is None else os.fsencode(velocity_path),
+                   None if vorticity_path is None else os.fsencode(vorticity_path))
 
     def set_state_device(self, v_ptr, o_ptr, pitch):
         self._call("dns_set_state", C.c_void_p(v_ptr), C.c_void_p(o_ptr), pitch, DEVICE)

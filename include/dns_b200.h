@@ -115,6 +115,26 @@ dns_status dns_get_state(dns_ctx* ctx, void* v, void* omega, size_t pitch, int w
 dns_status dns_get_history(dns_ctx* ctx, void* nv, void* nomega, size_t pitch, int where);
 dns_status dns_set_history(dns_ctx* ctx, const void* nv, const void* nomega, size_t pitch, int where);
 
+/* Recovery file in the reference's format (source/output.cpp:105-178):
+ * int mx, my, mz; size_t pSize, tSize (the reference's allocator sizes,
+ * source/operation.cpp:152-180, pitches from cudaMalloc3D on this device);
+ * Ny complex each of lambx0, lambz0, lambx0_p, lambz0_p, tv0, tomega_y_0;
+ * tSize bytes each of rhs_v, rhs_v_p, rhs_omega_y, nonlinear_v,
+ * nonlinear_omega_y in the pitched [Nz][Kx] pencil layout.  The "_p" fields
+ * are written with the current values (a restart never reads them: the next
+ * step replaces them before use).  Reading restores state and AB2 history
+ * (the writer's pencil pitch is taken from tSize), after which dns_step
+ * continues the run. */
+dns_status dns_write_recovery(dns_ctx* ctx, const char* path);
+dns_status dns_read_recovery(dns_ctx* ctx, const char* path);
+
+/* output_velocity / write_velocity (source/output.cpp:19-103): the physical
+ * velocity (u, v span, w wall-normal) and vorticity (omega_x, omega_y span,
+ * omega_z wall-normal) of the current state on the padded grid, each
+ * component as Py planes x my rows x mx doubles, unpitched, three components
+ * per file.  Either path may be NULL.  Allocates its work buffers. */
+dns_status dns_write_fields(dns_ctx* ctx, const char* velocity_path, const char* vorticity_path);
+
 /* The "extra previous step" of source/main_loop.cpp:39-52: store the
  * nonlinear term of the current state as the AB2 history, so the first step
  * is forward Euler in the nonlinear term as in the reference. */
