@@ -28,7 +28,7 @@ EXPORTS = [
     "dns_transform_3d_one", "dns_transform", "dns_cuda_transpose", "dns_cheby_s2p",
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
-    "dns_write_recovery", "dns_read_recovery", "dns_write_fields",
+    "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
 ]
 
 
@@ -93,6 +93,7 @@ def load_library(path: str | None = None):
         "dns_write_recovery": [vp, C.c_char_p],
         "dns_read_recovery": [vp, C.c_char_p],
         "dns_write_fields": [vp, C.c_char_p, C.c_char_p],
+        "dns_init_flow": [vp],
         "dns_set_history": [vp, vp, vp, sz, i],
         "dns_bootstrap": [vp],
         "dns_step": [vp, i],
@@ -237,6 +238,10 @@ class Context:
         """The reference's output_velocity files (physical u, v, w and vorticity)."""
         self._call("dns_write_fields", None if velocity_path is None else os.fsencode(velocity_path),
                    None if vorticity_path is None else os.fsencode(vorticity_path))
+
+    def init_flow(self):
+        """The reference's analytic initial state (initFlow); bootstrap next."""
+        self._call("dns_init_flow")
 
     def set_state_device(self, v_ptr, o_ptr, pitch):
         self._call("dns_set_state", C.c_void_p(v_ptr), C.c_void_p(o_ptr), pitch, DEVICE)

@@ -135,6 +135,14 @@ dns_status dns_read_recovery(dns_ctx* ctx, const char* path);
  * per file.  Either path may be NULL.  Allocates its work buffers. */
 dns_status dns_write_fields(dns_ctx* ctx, const char* velocity_path, const char* vorticity_path);
 
+/* initFlow (source/RPCFKernels.cu:358-431): set the state to the reference's
+ * analytic three-mode perturbation (amplitude 0.005), evaluated on mx x my
+ * points and the Ny Gauss-Lobatto planes and taken to spectral space by the
+ * forward transform without padding.  Like dns_set_state it leaves the AB2
+ * history alone: call dns_bootstrap (the reference's "extra previous step")
+ * before the first dns_step of a fresh run.  Allocates its work buffers. */
+dns_status dns_init_flow(dns_ctx* ctx);
+
 /* The "extra previous step" of source/main_loop.cpp:39-52: store the
  * nonlinear term of the current state as the AB2 history, so the first step
  * is forward Euler in the nonlinear term as in the reference. */

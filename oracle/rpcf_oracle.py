@@ -388,6 +388,55 @@ def rhs_nonlinear(tlx, tly, tlz, sz: Sizes, aphi, beta):
 
 
 # --------------------------------------------------------------------------
+# analytic initial condition (initFlow, source/RPCFKernels.cu:358-431)
+# --------------------------------------------------------------------------
+EPSILON_INIT = 0.005  # source/RPCFKernels.cu:132
+
+
+def init_fields(sz: Sizes, aphi, beta):
+    """init_flow_kernel (source/RPCFKernels.cu:311-356) for the two fields
+    that enter the state: w (:182-194) and omega_z (:212-223).
+
+    Points: x = i/px*lx, y = j/py*ly (lx = 2 pi aphi, ly = 2 pi beta,
+    source/data.cpp:5-6), z = cos(pi k/(nz-1)) for the nz planes k, both
+    fields zero on the wall planes k = 0, nz-1.  Returns two XYZ arrays of
+    shape (pz, my, mx); planes nz..pz-1 are zero (not read by the no-padding
+    transform).
+    """
+    lx = 2 * PI * aphi
+    ly = 2 * PI * beta
+    nz = sz.nz
+    xx = (np.arange(sz.mx) * 1.0) / sz.mx * lx
+    yy = (np.arange(sz.my) * 1.0) / sz.my * ly
+    zz = np.cos(PI * np.arange(nz) / (nz - 1))
+    z, y, x = np.meshgrid(zz, yy, xx, indexing="ij")
+    e = EPSILON_INIT
+    sa1, sa2 = np.sin(2 * PI * x / lx), np.sin(4.0 * PI * x / lx)
+    ca1, ca2 = np.cos(2 * PI * x / lx), np.cos(4.0 * PI * x / lx)
+    sb1, sb2 = np.sin(2 * PI * y / ly), np.sin(4 * PI * y / ly)
+    cb1, cb2 = np.cos(2.0 * PI * y / ly), np.cos(4.0 * PI * y / ly)
+    w = e * (-2.0 / 3.0) * (1.0 + np.cos(1.5 * PI * z)) * (sa1 * sb1 + sa2 * sb1 + sa1 * sb2)
+    oz = e * 2.0 * PI * np.sin(1.5 * PI * z) * (
+        lx / ly * (ca1 * cb1 + 0.5 * ca2 * cb1 + 2.0 * ca1 * cb2)
+        + ly / lx * (0.5 * ca1 * cb1 + ca2 * cb1 + 0.25 * ca1 * cb2))
+    W = np.zeros((sz.pz, sz.my, sz.mx))
+    OZ = np.zeros_like(W)
+    W[1:nz - 1] = w[1:nz - 1]
+    OZ[1:nz - 1] = oz[1:nz - 1]
+    return W, OZ
+
+
+def init_state(sz: Sizes, aphi, beta):
+    """initFlow's state: the no-padding forward transforms of w and omega_z
+    (source/RPCFKernels.cu:397-406), copied to rhs_v / rhs_omega_y.
+    Returns (V, O), each (ny, hnx, nz) complex."""
+    W, OZ = init_fields(sz, aphi, beta)
+    V = transform_forward(W, sz, pad=False)[..., :sz.nz]
+    O = transform_forward(OZ, sz, pad=False)[..., :sz.nz]
+    return V, O
+
+
+# --------------------------------------------------------------------------
 # full problem / time step
 # --------------------------------------------------------------------------
 @dataclass
