@@ -137,7 +137,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
   mark();
-  if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->st))) return e;
+  if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->status, c->st))) return e;
   mark();
   if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st))) return e;
   mark();
@@ -151,7 +151,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   const RhsTabs tb{t0, t0 + 4 * nv, t0 + 4 * nv + 2 * no, t0 + 4 * nv + 2 * no + g.Ny,
                    t0 + 4 * nv + 2 * no + g.Ny + 5 * nv};
   if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
-                        boot, c->st)))
+                        boot, c->status, c->st)))
     return e;
   mark();
   if (!boot)

@@ -39,4 +39,7 @@ struct PhysParams {
   double U0, U1, U2;    // base flow U(y) = U0 + U1 y + U2 y^2
 };
 
+// 16-byte alignment of a device pointer (bulk-copy sources)
+inline bool aligned16(const void* p) { return ((unsigned long long)p & 15ull) == 0; }
+
 #define DNS_CHECK_LAUNCH() do { cudaError_t e__ = cudaGetLastError(); if (e__ != cudaSuccess) return e__; } while (0)

@@ -7,22 +7,33 @@
 // writes y[(j/Ns) Ns R + (j mod Ns) + r Ns].  The NL L / R butterflies of a
 // pass are spread evenly over the 32 lanes (every radix of a plan divides
 // NL L / 32), a lane loads all its inputs before the warp synchronises and
-// writes, so the transform runs in place.  Input and output are in natural
-// order at swizzled positions wsw(i): the low bits of the index are XORed
-// with the next ones, which makes the strided accesses of the early passes
-// bank-conflict free without padding within a line; the line stride is a
-// parameter (padded where several lines are addressed at one position).
+// writes, so the transform runs in place.
+//
+// Layout: element i of a line sits at wsw(i) = i + i / 2^S, one padding
+// slot after every 2^S elements (2^S x the element size = 128 bytes), which
+// spreads the strided accesses of the early passes over the banks.  The map
+// is linear within runs that do not cross a 2^S boundary, so where a pass's
+// R accesses of a butterfly are i = b + c_r with compile-time c_r and no
+// carry from the low S bits of b into c_r (checked at compile time for all
+// butterflies of the pass), wsw(b + c_r) = wsw(b) + wsw(c_r): one address
+// per butterfly and immediate offsets.  Lines are wlen(L) elements apart
+// unless the caller passes another stride.
 #pragma once
 #include "fft2.cuh"
 
-// swizzle within aligned blocks: 16 elements (FP32 complex, 128 B) or 8
-// elements (FP64 complex)
+// butterfly index range hint for the device compiler (lets it resolve, per
+// compile-time r, which branch of a first-pass load function applies)
+#ifdef __CUDA_ARCH__
+#define WFFT_ASSUME(c) __builtin_assume(c)
+#else
+#define WFFT_ASSUME(c) ((void)0)
+#endif
+
 template <typename C> struct WSwz { enum { S = 4 }; };
 template <> struct WSwz<double2> { enum { S = 3 }; };
-template <typename C> DNS_HD int wsw(int i) {
-  constexpr int S = WSwz<C>::S;
-  return i ^ ((i >> S) & ((1 << S) - 1));
-}
+template <typename C> DNS_HD constexpr int wsw(int i) { return i + (i >> WSwz<C>::S); }
+// line length covering positions wsw(0..L-1)
+template <typename C> DNS_HD constexpr int wlen(int L) { return L + (L >> WSwz<C>::S); }
 
 // plans: radices (up to 48 FP32, 8 FP64 for register pressure), each
 // dividing NL L / 32
@@ -61,30 +72,54 @@ WPLAN(384, 3, 8, 6, 4, 4, 4)
 // One pass, split into the load (inputs of the lane's butterfly q, twiddled,
 // transformed) and the store of its outputs, so that host code can run the
 // same index arithmetic lane by lane.
+// true when no butterfly j < NB of a pass stores across a 2^S boundary
+// from its first output: (base(j) mod 2^S) + (r Ns mod 2^S) < 2^S for all r
+constexpr bool wlin_store(int M, int NB, int Ns, int R) {
+  for (int j = 0; j < NB; ++j) {
+    const int b = ((j / Ns) * Ns * R + j % Ns) & M;
+    for (int r = 0; r < R; ++r)
+      if (b + ((r * Ns) & M) > M) return false;
+  }
+  return true;
+}
+
 template <typename C, int L, int NL, bool INV, int R, int Ns>
 struct WPass {
   static constexpr int NB = L / R;        // butterflies per line
   static constexpr int B = NL * NB / 32;  // butterflies per lane
   static_assert((NL * NB) % 32 == 0, "radix does not divide the lane share");
+  static constexpr int S = WSwz<C>::S, M = (1 << S) - 1;
+  // loads i = j + r NB: no carry for any j when NB is a multiple of 2^S
+  static constexpr bool LIN_LD = (NB & M) == 0;
+  // stores i = base(j) + r Ns, base(j) = (j / Ns) Ns R + j mod Ns
+  static constexpr bool LIN_ST = wlin_store(M, NB, Ns, R);
   DNS_HD static void load(const C* buf, int ls, const C* tw, int lane, int q, C* v) {
     const int w = lane + 32 * q;
     const int line = w / NB;
     const int j = w - line * NB;
+    WFFT_ASSUME(j >= 0 && j < NB);
     const C* x = buf + line * ls;
+    if constexpr (LIN_LD) {
+      const C* xb = x + wsw<C>(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = x[wsw<C>(j + r * NB)];
+      for (int r = 0; r < R; ++r) v[r] = xb[wsw<C>(r * NB)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = x[wsw<C>(j + r * NB)];
+    }
     if (Ns > 1) {
       const int k = j % Ns;
       if (k > 0) {
         constexpr int step = L / (Ns * R);
-        const C w1 = tw[k * step];
+        const int ks = k * step;
+        const C w1 = tw[ks];
         C wr = w1;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           if (FftMaxRadix<C>::v == 8) {
             if (r > 1) wr = cmul(wr, w1);
           } else {
-            wr = tw[r * k * step];
+            wr = tw[r * ks];
           }
           v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
         }
@@ -97,6 +132,7 @@ struct WPass {
     const int w = lane + 32 * q;
     const int line = w / NB;
     const int j = w - line * NB;
+    WFFT_ASSUME(j >= 0 && j < NB);
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = ld(line, j + r * NB);
     Codelet<R, INV, C>::run(v);
@@ -106,6 +142,7 @@ struct WPass {
     const int w = lane + 32 * q;
     const int line = w / NB;
     const int j = w - line * NB;
+    WFFT_ASSUME(j >= 0 && j < NB);
     const int base = (j / Ns) * Ns * R + (j % Ns);
 #pragma unroll
     for (int r = 0; r < R; ++r) st(line, base + r * Ns, v[r]);
@@ -114,10 +151,17 @@ struct WPass {
     const int w = lane + 32 * q;
     const int line = w / NB;
     const int j = w - line * NB;
+    WFFT_ASSUME(j >= 0 && j < NB);
     C* y = buf + line * ls;
     const int base = (j / Ns) * Ns * R + (j % Ns);
+    if constexpr (LIN_ST) {
+      C* yb = y + wsw<C>(base);
 #pragma unroll
-    for (int r = 0; r < R; ++r) y[wsw<C>(base + r * Ns)] = v[r];
+      for (int r = 0; r < R; ++r) yb[wsw<C>(r * Ns)] = v[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) y[wsw<C>(base + r * Ns)] = v[r];
+    }
   }
 };
 
@@ -157,7 +201,7 @@ struct WDo<C, L, NL, INV, Radices<Rs...>> {
 
 // Variant with the input and output fused into the first and last passes:
 // the first pass reads ld(line, n), the last hands st(line, k, value) every
-// output; buf (NL lines of L) holds the intermediate passes only.
+// output; buf (NL lines, wlen(L) apart) holds the intermediate passes only.
 template <typename C, int L, int NL, bool INV, int Ns, bool FIRST, int R, int... Rest>
 struct WRunIO {
   template <class LD, class ST>
@@ -168,13 +212,13 @@ struct WRunIO {
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
       if constexpr (FIRST) P::template load_fn<LD>(ld, lane, q, v[q]);
-      else P::load(buf, L, tw, lane, q, v[q]);
+      else P::load(buf, wlen<C>(L), tw, lane, q, v[q]);
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
       if constexpr (LAST) P::template store_fn<ST>(st, lane, q, v[q]);
-      else P::store(buf, L, lane, q, v[q]);
+      else P::store(buf, wlen<C>(L), lane, q, v[q]);
     }
     __syncwarp();
     if constexpr (!LAST) WRunIO<C, L, NL, INV, Ns * R, false, Rest...>::go(buf, tw, lane, ld, st);
@@ -193,12 +237,12 @@ __device__ __forceinline__ void wfft_io(C* buf, const C* __restrict__ tw, LD ld,
   WDoIO<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, tw, threadIdx.x & 31, ld, st);
 }
 
-// Transform the NL lines at buf (line stride ls >= L, positions wsw(i)) by
+// Transform the NL lines at buf (line stride ls >= wlen(L), positions wsw(i)) by
 // the calling warp.  The lines must have been written by this warp (or be
 // visible to it after a barrier); a __syncwarp is taken first.
 // tw: W_L^j, j < L.
 template <typename C, int L, int NL, bool INV>
-__device__ __forceinline__ void wfft(C* buf, const C* __restrict__ tw, int ls = L) {
+__device__ __forceinline__ void wfft(C* buf, const C* __restrict__ tw, int ls = wlen<C>(L)) {
   __syncwarp();
   WDo<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, ls, tw, threadIdx.x & 31);
 }

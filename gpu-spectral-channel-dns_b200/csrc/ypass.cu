@@ -19,6 +19,7 @@
 // same way: coefficient-space derivatives, then the no-pad DCT.
 #include "fftline.cuh"
 #include "kernels.cuh"
+#include "mbar.cuh"
 #include "wfft.cuh"
 #include "ypass.cuh"
 
@@ -360,7 +361,8 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
 // staged in shared memory.
 template <typename C, int M>
 __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const double2* __restrict__ O,
-                                           PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab) {
+                                           PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab,
+                                           int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   Carve cv(smem_raw);
@@ -374,7 +376,8 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   double2* Dv = cv.take<double2>(Ny);
   double2* ox = cv.take<double2>(Ny);
   double2* oy = cv.take<double2>(Ny);
-  C* lines = cv.take<C>((size_t)6 * M);
+  constexpr int MW = wlen<C>(M);
+  C* lines = cv.take<C>((size_t)6 * MW);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -383,12 +386,24 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
   const double kmn = kmn_of(ia, ib);
   const double kmn1 = zero ? 0.0 : 1.0 / kmn;
-  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    w[n] = V[p * Ny + n];
-    oz[n] = O[p * Ny + n];
+  // twiddles and the pencil's state by bulk copies on one barrier
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(&bar, (uint32_t)(M * sizeof(C) + 2 * Ny * 16));
+    bulk_g2s(tws, tab.tw, (uint32_t)(M * sizeof(C)), &bar);
+    bulk_g2s(w, V + p * Ny, (uint32_t)(Ny * 16), &bar);
+    bulk_g2s(oz, O + p * Ny, (uint32_t)(Ny * 16), &bar);
   }
-  for (int n = threadIdx.x; n < M; n += blockDim.x) tws[n] = tab.tw[n];
   __syncthreads();
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, 1LL << 31, status))) {
+    if (threadIdx.x == 0) {
+      atomicOr(status, 1);
+      mbar_wait_bounded(&bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+    }
+    return;
+  }
   const int warp = threadIdx.x >> 5;
   if (!zero && warp == 0) ddz_warp(w, Dw, Ny);
   __syncthreads();
@@ -415,7 +430,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   // this warp's two lines: fields 2 warp, 2 warp + 1; the first FFT pass
   // reads the even extensions e[0] = c_0, e[n] = e[M-n] = c_n / 2 (n < Ny),
   // zero elsewhere, the last one writes the Py values
-  C* wl = lines + (size_t)2 * warp * M;
+  C* wl = lines + (size_t)2 * warp * MW;
   const double2* s0 = (warp == 0) ? u : (warp == 1 ? w : oy);
   const double2* s1 = (warp == 0) ? v : (warp == 1 ? ox : oz);
   // w (line 2) and omega_z (line 5) vanish for the mean mode
@@ -711,7 +726,7 @@ __global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
-                                            FftTab<C> tabP, int boot) {
+                                            FftTab<C> tabP, int boot, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Ny = g.Ny;
   const int Py = g.Py;
@@ -732,7 +747,7 @@ __global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __
   double2* DO = cv.take<double2>(Ny);
   double2* D2O = cv.take<double2>(Ny);
   double2* red = cv.take<double2>(8);
-  const size_t bytesL = (size_t)3 * M * sizeof(C), bytesI = (size_t)4 * LB * 16;
+  const size_t bytesL = (size_t)3 * wlen<C>(M) * sizeof(C), bytesI = (size_t)4 * LB * 16;
   unsigned char* region = cv.take<unsigned char>(bytesL > bytesI ? bytesL : bytesI);
   C* lines = (C*)region;
 
@@ -745,23 +760,40 @@ __global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __
   const double kmn = kmn_of(ia, ib);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // 1. twiddles, state, history
-  for (int n = threadIdx.x; n < M; n += blockDim.x) tws[n] = tabP.tw[n];
-  if (!boot)
-    for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-      Vc[n] = V[p * Ny + n];
-      Oc[n] = O[p * Ny + n];
-      nvc[n] = Nvp[p * Ny + n];
-      noc[n] = Nop[p * Ny + n];
+  // 1. bulk copies on one barrier: twiddles, the three Lamb pencils (Py
+  //    values, natural order, at the start of each warp's line: the first
+  //    FFT pass reads them all before it writes the line), state, history
+  const uint32_t lamb = (uint32_t)(((Py + 1) & ~1) * sizeof(C));
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(&bar, (uint32_t)(M * sizeof(C)) + 3 * lamb + (boot ? 0u : (uint32_t)(4 * Ny * 16)));
+    bulk_g2s(tws, tabP.tw, (uint32_t)(M * sizeof(C)), &bar);
+    for (int f = 0; f < 3; ++f) bulk_g2s(lines + (size_t)f * wlen<C>(M), pencil_ptr<C>(lam, f, p), lamb, &bar);
+    if (!boot) {
+      bulk_g2s(Vc, V + p * Ny, (uint32_t)(Ny * 16), &bar);
+      bulk_g2s(Oc, O + p * Ny, (uint32_t)(Ny * 16), &bar);
+      bulk_g2s(nvc, Nvp + p * Ny, (uint32_t)(Ny * 16), &bar);
+      bulk_g2s(noc, Nop + p * Ny, (uint32_t)(Ny * 16), &bar);
     }
+  }
   __syncthreads();
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, 1LL << 31, status))) {
+    if (threadIdx.x == 0) {
+      atomicOr(status, 1);
+      mbar_wait_bounded(&bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+    }
+    return;
+  }
   // 2. transforms, one Lamb line per warp (0: lambda_x, 1: lambda_y,
   //    2: lambda_z), read from the pencils as even extensions, coefficients
   //    written to lc, and the warp's own derivative (D lambda_x, D lambda_y);
   //    warps 3 and 4 build the derivative chains of v and omega_y meanwhile
   const double sc = 1.0 / (Py - 1);
   if (warp < 3) {
-    const C* src = pencil_ptr<C>(lam, warp, p);
+    C* wline = lines + (size_t)warp * wlen<C>(M);
+    const C* src = wline;  // staged pencil
     double2* lf = lc + (size_t)warp * Ny;
     auto ld = [&](int, int n) -> C { return (n < Py) ? src[n] : src[M - n]; };
     auto st = [&](int, int k, C val) {
@@ -771,7 +803,7 @@ __global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __
         lf[k] = c;
       }
     };
-    wfft_io<C, M, 1, false>(lines + (size_t)warp * M, tws, ld, st);
+    wfft_io<C, M, 1, false>(wline, tws, ld, st);
     if (warp < 2) ddz_warp(lf, D1 + (size_t)warp * Ny, Ny);
   } else if (!boot && warp == 3) {
     ddz_warp(Vc, DV, Ny);
@@ -946,17 +978,21 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
 
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
-                      PhysParams ph, FftTab<C> tab, cudaStream_t st) {
+                      PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st) {
+  // the warp form stages its inputs by bulk copies: 16-byte aligned sources
+  const bool bulk_ok = aligned16(V) && aligned16(O) && aligned16(tab.tw);
   return with_len_m(tab.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     // warp-FFT form for FP32 (the FP64 form keeps the block FFT, whose
     // register footprint is smaller)
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     if (bulk_ok) {
       const size_t sm = (size_t)L * sizeof(C) + 9 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) +
-                        (size_t)6 * L * sizeof(C);
+                        (size_t)6 * wlen<C>(L) * sizeof(C);
       cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab);
+      k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab, status);
       return cudaGetLastError();
+     }
     }
     const size_t sm = y3_smem(g.Ny, FLine<C, L>::stride(tab.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y3<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -964,23 +1000,31 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y3<double2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<double2>, cudaStream_t);
-template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<float2>, cudaStream_t);
+template cudaError_t launch_y3<double2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<double2>, int*, cudaStream_t);
+template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<float2>, int*, cudaStream_t);
 
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
                       double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
-                      PhysParams ph, FftTab<C> tabP, int boot, cudaStream_t st) {
+                      PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st) {
+  // the warp form stages its inputs by bulk copies: 16-byte aligned pencils
+  // with room for Py rounded up to even
+  const bool bulk_ok = aligned16(lam.base) && (lam.ps * sizeof(C)) % 16 == 0 &&
+                       (lam.fs * sizeof(C)) % 16 == 0 && lam.ps >= ((g.Py + 1) & ~1) && aligned16(V) &&
+                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && aligned16(tabP.tw);
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
+     if (bulk_ok) {
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
-      const size_t bl = (size_t)3 * L * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
+      const size_t bl = (size_t)3 * wlen<C>(L) * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
       const size_t sm = a((size_t)L * sizeof(C)) + a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) +
                         10 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
       cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
+      k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot,
+                                                    status);
       return cudaGetLastError();
+     }
     }
     const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y1<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -988,5 +1032,5 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<double2>, int, cudaStream_t);
-template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<float2>, int, cudaStream_t);
+template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<double2>, int, int*, cudaStream_t);
+template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<float2>, int, int*, cudaStream_t);

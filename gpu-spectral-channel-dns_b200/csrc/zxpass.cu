@@ -121,115 +121,131 @@ __global__ void __launch_bounds__(256, 3) k_zf(RowArr in, PencilArr out, DnsGeom
 }
 
 // Same spanwise passes with warp FFTs: a TX x TY tile of 16 lines
-// (streamwise modes x wall-normal points; zf uses 4 x 4, 32-byte runs on
-// both sides, zb 8 x 2, 64-byte runs on its larger row side), NW warps with
+// (streamwise modes x wall-normal points; both passes use 4 x 4: 32-byte
+// runs, whole sectors, on both sides), NW warps with
 // 16/NW lines each, no block barrier inside the transforms.
+//
+// Index arithmetic: on the pencil side a thread keeps one line (its kx and
+// y) and walks the spanwise wavenumbers kz = t/16 + 16 m; on the row side it
+// keeps one kx and walks the flat (y, zp) index of the tile's rows, whose
+// global offset is i * rs from the tile's first row.  Both walks are strided
+// by a constant, so an element costs one multiply-add of its address.
+namespace {
+template <typename C, int L, int TX, int TY, int NT>
+struct SpanTile {
+  static constexpr int NL = TX * TY;
+  static constexpr int LS = wlen<C>(L) + 1;  // odd line stride: the 16 lines of a position fall in distinct banks
+  static constexpr int KS = NT / NL;         // kz stride of the pencil-side walk
+  static constexpr int IS = NT / TX;         // (y, zp) stride of the row-side walk
+  static_assert(NT % NL == 0 && NT % TX == 0, "tile does not divide the block");
+};
+}  // namespace
+
 template <typename C, int L, int NW, int TX, int TY>
 __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGeom g, FftTab<C> tab) {
-  constexpr int NL = TX * TY;
+  typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
+  constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = (C*)smem_raw;
-  constexpr int LS = L + 1;  // line stride: the 16 lines of a position fall in distinct banks
   C* lines = tws + L;
-  constexpr int Pz = L;
   const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
   const int hz = Nz / 2;
   for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
-  // zero band [Nz/2, Pz - Nz/2] (Nyquist and padding)
-  const int nzero = Pz - Nz + 1;
-  for (int t = threadIdx.x; t < NL * nzero; t += blockDim.x) {
-    const int li = t / nzero;
-    const int n = hz + (t - li * nzero);
-    lines[(size_t)li * LS + wsw<C>(n)] = cmk<C>(0.0, 0.0);
-  }
-  // loads in batches of ZB independent requests per thread before their stores
-  constexpr int ZB = 8;
-  for (int t0 = threadIdx.x; t0 < Nz * NL; t0 += ZB * (int)blockDim.x) {
-    C v[ZB];
-    int pos[ZB];
+  // pencil side: line li = (kxl, yl) of this thread
+  {
+    const int li = threadIdx.x % NL;
+    const int kx = kx0 + li / TY, y = y0 + li % TY;
+    C* dst = lines + li * LS;
+    // zero band [Nz/2, Pz - Nz/2] (Nyquist and padding)
+    for (int n = hz + threadIdx.x / NL; n <= Pz - hz; n += ST::KS) dst[wsw<C>(n)] = cmk<C>(0.0, 0.0);
+    // the streamwise Nyquist column (kx = Kx - 1) and rows beyond Py stay zero
+    const bool ok = kx < Kx - 1 && y < Py;
+    const C* src = ppen<C>(in, f, ok ? kx : 0) + (ok ? y : 0);
+    const long long kzs = (long long)Kx * in.ps;
+    // loads in batches of ZB independent requests per thread before their stores
+    constexpr int ZB = 8;
+    for (int kz0 = threadIdx.x / NL; kz0 < Nz; kz0 += ZB * ST::KS) {
+      C v[ZB];
 #pragma unroll
-    for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int yl = t % TY;
-      const int kxl = (t / TY) % TX;
-      const int kz = t / NL;
-      const int n = (kz < hz) ? kz : kz + (Pz - Nz);
-      const int kx = kx0 + kxl;
-      const int y = y0 + yl;
-      v[u] = cmk<C>(0.0, 0.0);
-      pos[u] = (t < Nz * NL && kz != hz) ? (kxl * TY + yl) * LS + wsw<C>(n) : -1;
-      if (pos[u] >= 0 && kx < Kx - 1 && y < Py) v[u] = ppen<C>(in, f, (long long)kz * Kx + kx)[y];
+      for (int u = 0; u < ZB; ++u) {
+        const int kz = kz0 + u * ST::KS;
+        v[u] = (ok && kz < Nz && kz != hz) ? src[kz * kzs] : cmk<C>(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < ZB; ++u) {
+        const int kz = kz0 + u * ST::KS;
+        if (kz < Nz && kz != hz) dst[wsw<C>(kz < hz ? kz : kz + (Pz - Nz))] = v[u];
+      }
     }
-#pragma unroll
-    for (int u = 0; u < ZB; ++u)
-      if (pos[u] >= 0) lines[pos[u]] = v[u];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
   wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tws, LS);
   __syncthreads();
-  for (int t0 = threadIdx.x; t0 < TY * Pz * TX; t0 += ZB * (int)blockDim.x) {
+  // row side: this thread's kx, flat index i = yl * Pz + zp
+  const int kxl = threadIdx.x % TX;
+  const int kx = kx0 + kxl;
+  if (kx >= Kx || y0 >= Py) return;
+  const int ni = min(TY, Py - y0) * Pz;
+  C* rowb = prow<C>(out, f, (long long)y0 * Pz) + kx;
+  const C* lb = lines + kxl * TY * LS;
+  constexpr int ZB = 8;
+  for (int i0 = threadIdx.x / TX; i0 < ni; i0 += ZB * ST::IS) {
     C v[ZB];
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int kxl = t % TX;
-      const int zp = (t / TX) % Pz;
-      const int yl = t / (TX * Pz);
-      v[u] = (t < TY * Pz * TX) ? lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] : cmk<C>(0.0, 0.0);
+      const int i = i0 + u * ST::IS;
+      const int yl = i / Pz, zp = i - yl * Pz;
+      v[u] = (i < ni) ? lb[yl * LS + wsw<C>(zp)] : cmk<C>(0.0, 0.0);
     }
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int kxl = t % TX;
-      const int zp = (t / TX) % Pz;
-      const int yl = t / (TX * Pz);
-      const int kx = kx0 + kxl;
-      const int y = y0 + yl;
-      if (t < TY * Pz * TX && kx < Kx && y < Py) prow<C>(out, f, (long long)y * Pz + zp)[kx] = v[u];
+      const int i = i0 + u * ST::IS;
+      if (i < ni) rowb[(long long)i * out.rs] = v[u];
     }
   }
 }
 
 template <typename C, int L, int NW>
 __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
-  constexpr int TX = 4, TY = 4, NL = TX * TY;
+  constexpr int TX = 4, TY = 4;
+  typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
+  constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = (C*)smem_raw;
-  constexpr int LS = L + 1;  // line stride: the 16 lines of a position fall in distinct banks
   C* lines = tws + L;
-  constexpr int Pz = L;
   const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
   for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
-  // loads in batches of ZB independent requests per thread before their stores
   constexpr int ZB = 8;
-  for (int t0 = threadIdx.x; t0 < TY * Pz * TX; t0 += ZB * (int)blockDim.x) {
-    C v[ZB];
+  // row side: this thread's kx, flat index i = yl * Pz + zp; rows beyond
+  // Py and columns beyond Kx read as zero
+  {
+    const int kxl = threadIdx.x % TX;
+    const int kx = kx0 + kxl;
+    const int ni = TY * Pz;
+    const int nv = (kx < Kx && y0 < Py) ? min(TY, Py - y0) * Pz : 0;
+    const C* rowb = prow<C>(in, f, (long long)y0 * Pz) + kx;
+    C* lb = lines + kxl * TY * LS;
+    for (int i0 = threadIdx.x / TX; i0 < ni; i0 += ZB * ST::IS) {
+      C v[ZB];
 #pragma unroll
-    for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int kxl = t % TX;
-      const int zp = (t / TX) % Pz;
-      const int yl = t / (TX * Pz);
-      const int kx = kx0 + kxl;
-      const int y = y0 + yl;
-      v[u] = cmk<C>(0.0, 0.0);
-      if (t < TY * Pz * TX && kx < Kx && y < Py) v[u] = prow<C>(in, f, (long long)y * Pz + zp)[kx];
-    }
+      for (int u = 0; u < ZB; ++u) {
+        const int i = i0 + u * ST::IS;
+        v[u] = (i < nv) ? rowb[(long long)i * in.rs] : cmk<C>(0.0, 0.0);
+      }
 #pragma unroll
-    for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int kxl = t % TX;
-      const int zp = (t / TX) % Pz;
-      const int yl = t / (TX * Pz);
-      if (t < TY * Pz * TX) lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(zp)] = v[u];
+      for (int u = 0; u < ZB; ++u) {
+        const int i = i0 + u * ST::IS;
+        const int yl = i / Pz, zp = i - yl * Pz;
+        if (i < ni) lb[yl * LS + wsw<C>(zp)] = v[u];
+      }
     }
   }
   __syncthreads();
@@ -237,27 +253,25 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   constexpr int NLW = NL / NW;  // lines per warp
   wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tws, LS);
   __syncthreads();
+  // pencil side: line li = (kxl, yl) of this thread, wavenumbers kz
   const int hz = Nz / 2;
-  for (int t0 = threadIdx.x; t0 < Nz * NL; t0 += ZB * (int)blockDim.x) {
+  const int li = threadIdx.x % NL;
+  const int kx = kx0 + li / TY, y = y0 + li % TY;
+  if (kx >= Kx || y >= Py) return;
+  const C* lsrc = lines + li * LS;
+  C* dst = ppen<C>(out, f, kx) + y;
+  const long long kzs = (long long)Kx * out.ps;
+  for (int kz0 = threadIdx.x / NL; kz0 < Nz; kz0 += ZB * ST::KS) {
     C v[ZB];
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int yl = t % TY;
-      const int kxl = (t / TY) % TX;
-      const int kz = t / NL;
-      const int n = (kz <= hz) ? kz : kz + (Pz - Nz);
-      v[u] = (t < Nz * NL) ? lines[(size_t)(kxl * TY + yl) * LS + wsw<C>(n)] : cmk<C>(0.0, 0.0);
+      const int kz = kz0 + u * ST::KS;
+      v[u] = (kz < Nz) ? lsrc[wsw<C>(kz <= hz ? kz : kz + (Pz - Nz))] : cmk<C>(0.0, 0.0);
     }
 #pragma unroll
     for (int u = 0; u < ZB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int yl = t % TY;
-      const int kxl = (t / TY) % TX;
-      const int kz = t / NL;
-      const int kx = kx0 + kxl;
-      const int y = y0 + yl;
-      if (t < Nz * NL && kx < Kx && y < Py) ppen<C>(out, f, (long long)kz * Kx + kx)[y] = v[u];
+      const int kz = kz0 + u * ST::KS;
+      if (kz < Nz) dst[kz * kzs] = v[u];
     }
   }
 }
@@ -393,19 +407,20 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
 // warp forward-transforms two of them, and the half spectra are unpacked to
 // the output rows.
 template <typename C, int L>
-__global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+__global__ void __launch_bounds__(96, 4) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
                                           const double* __restrict__ Uy, double Ro, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
   constexpr int Px = L;
   const int hx = g.Nx / 2;
   C* tws = (C*)smem_raw;
+  constexpr int LW = wlen<C>(L);                        // line stride
   C* z = tws + L;                                       // 12 lines
-  uint64_t* bars = (uint64_t*)(z + (size_t)12 * L);      // one per warp
+  uint64_t* bars = (uint64_t*)(z + (size_t)12 * LW);     // one per warp
   const long long r0 = (long long)blockIdx.x * 4;
   const long long nrows = (long long)g.Py * g.Pz;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* zw = z + (size_t)4 * warp * L;
+  C* zw = z + (size_t)4 * warp * LW;
   // stage this warp's 8 half-spectrum rows (bins 0..hx-1, 16 B aligned) at
   // the start of its own lines: the first FFT pass reads them all before it
   // writes its output over them
@@ -438,7 +453,7 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
   {
     const C* stg = zw;
     auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
-    auto st = [&](int l, int k, C v) { zw[(size_t)l * L + wsw<C>(k)] = v; };
+    auto st = [&](int l, int k, C v) { zw[(size_t)l * LW + wsw<C>(k)] = v; };
     wfft_io<C, L, 4, true>(zw, tws, ld, st);
   }
   __syncthreads();
@@ -451,53 +466,54 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     T lz[4];
 #pragma unroll
     for (int rl = 0; rl < 4; ++rl) {
-      const C z0 = z[(size_t)(3 * rl + 0) * L + op];
-      const C z1 = z[(size_t)(3 * rl + 1) * L + op];
-      const C z2 = z[(size_t)(3 * rl + 2) * L + op];
+      const C z0 = z[(size_t)(3 * rl + 0) * LW + op];
+      const C z1 = z[(size_t)(3 * rl + 1) * LW + op];
+      const C z2 = z[(size_t)(3 * rl + 2) * LW + op];
       const T u = z0.x, v = z0.y, ox = z1.x, oy = z1.y, w = z2.x, oz = z2.y;
       A[rl].x = oz * v - oy * w - ro * w;
       A[rl].y = ox * w - oz * u;
       lz[rl] = oy * u - ox * v + ro * (u + Ub);
     }
 #pragma unroll
-    for (int rl = 0; rl < 4; ++rl) z[(size_t)rl * L + op] = A[rl];
+    for (int rl = 0; rl < 4; ++rl) z[(size_t)rl * LW + op] = A[rl];
     C B0, B1;
     B0.x = lz[0]; B0.y = lz[1];
     B1.x = lz[2]; B1.y = lz[3];
-    z[(size_t)4 * L + op] = B0;
-    z[(size_t)5 * L + op] = B1;
+    z[(size_t)4 * LW + op] = B0;
+    z[(size_t)5 * LW + op] = B1;
   }
   __syncthreads();
-  wfft<C, L, 2, false>(z + (size_t)2 * warp * L, tws);
+  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, tws);
   __syncthreads();
+  // unpack: output row o = 3 rl + fl (field fl of row rl) by warp o mod 3,
+  // lanes over the bins k; shared loads of a batch before its stores
   const int Kx = g.Kx;
   const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
-  constexpr int XB = 8;  // outputs per thread per batch: shared loads first
-  for (int t0 = threadIdx.x; t0 < 4 * 3 * Kx; t0 += XB * (int)blockDim.x) {
-    C zk[XB], zm[XB];
+  constexpr int XB = 5;
+  for (int o = warp; o < 12; o += 3) {
+    const int rl = o / 3, fl = o - 3 * rl;
+    const long long row = r0 + rl;
+    if (row >= nrows) continue;
+    const C* Z = (fl < 2) ? z + (size_t)rl * LW : z + (size_t)(4 + rl / 2) * LW;
+    const bool im = (fl < 2) ? (fl == 1) : (rl & 1);
+    C* dst = prow<C>(out, fl, row);
+    for (int k0 = lane; k0 < Kx; k0 += 32 * XB) {
+      C zk[XB], zm[XB];
 #pragma unroll
-    for (int u = 0; u < XB; ++u) {
-      const int t = min(t0 + u * (int)blockDim.x, 4 * 3 * Kx - 1);
-      const int k = t % Kx;
-      const int fl = (t / Kx) % 3;
-      const int rl = t / (3 * Kx);
-      const C* Z = (fl < 2) ? z + (size_t)rl * L : z + (size_t)(4 + rl / 2) * L;
-      zk[u] = Z[wsw<C>(k)];
-      zm[u] = Z[wsw<C>((Px - k) % Px)];
-    }
+      for (int u = 0; u < XB; ++u) {
+        const int k = min(k0 + 32 * u, Kx - 1);
+        zk[u] = Z[wsw<C>(k)];
+        zm[u] = Z[wsw<C>(k ? Px - k : 0)];
+      }
 #pragma unroll
-    for (int u = 0; u < XB; ++u) {
-      const int t = t0 + u * blockDim.x;
-      const int k = t % Kx;
-      const int fl = (t / Kx) % 3;
-      const int rl = t / (3 * Kx);
-      const long long row = r0 + rl;
-      if (t >= 4 * 3 * Kx || row >= nrows) continue;
-      const bool im = (fl < 2) ? (fl == 1) : (rl & 1);
-      C v;
-      if (!im) { v.x = zk[u].x + zm[u].x; v.y = zk[u].y - zm[u].y; }
-      else { v.x = zk[u].y + zm[u].y; v.y = zm[u].x - zk[u].x; }
-      prow<C>(out, fl, row)[k] = v * sc;
+      for (int u = 0; u < XB; ++u) {
+        const int k = k0 + 32 * u;
+        if (k >= Kx) continue;
+        C v;
+        if (!im) { v.x = zk[u].x + zm[u].x; v.y = zk[u].y - zm[u].y; }
+        else { v.x = zk[u].y + zm[u].y; v.y = zm[u].x - zk[u].x; }
+        dst[k] = v * sc;
+      }
     }
   }
 }
@@ -604,11 +620,15 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-      const size_t sm = ((size_t)L + 16 * (L + 1)) * sizeof(C);
-      // 8 x 2 tile: the row side (the larger, Pz > Nz) gets 64-byte runs
-      cudaFuncSetAttribute(k_zbw<C, L, 8, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      dim3 grid((g.Kx + 7) / 8, (g.Py + 1) / 2, nf);
-      k_zbw<C, L, 8, 8, 2><<<grid, 256, sm, st>>>(in, out, g, tab);
+      const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
+      // 4 x 4 tile: whole 32-byte sectors on both sides.  Three CTAs per SM
+      // and the rest of the SM's memory as L1: the pencil-side gathers of
+      // neighbouring threads share sectors (measured: a quarter faster than
+      // four CTAs with a small L1)
+      cudaFuncSetAttribute(k_zbw<C, L, 8, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(k_zbw<C, L, 8, 4, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
+      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
+      k_zbw<C, L, 8, 4, 4><<<grid, 256, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
     }
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
@@ -624,8 +644,9 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-      const size_t sm = ((size_t)L + 16 * (L + 1)) * sizeof(C);
+      const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
       dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
       k_zfw<C, L, 8><<<grid, 256, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
@@ -647,9 +668,9 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
       const long long nrows = (long long)g.Py * g.Pz;
       // four rows per CTA within one wall-normal plane; a warp's 8 staged
       // rows of 128 bins fit in its 4 lines
-      if (g.Pz % 4 == 0 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * L && in.rs >= 128 && in.rs % 2 == 0 &&
+      if (g.Pz % 4 == 0 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
           in.fs % 2 == 0) {
-        const size_t sm = (size_t)13 * L * sizeof(C) + 64;
+        const size_t sm = ((size_t)L + 12 * (size_t)wlen<C>(L)) * sizeof(C) + 64;
         cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
         return cudaGetLastError();

@@ -14,9 +14,9 @@ struct HRun {
     typedef WPass<C, L, NL, INV, R, Ns> P;
     std::vector<C> v(32 * P::B * R);
     for (int lane = 0; lane < 32; ++lane)
-      for (int q = 0; q < P::B; ++q) P::load(buf, L, tw, lane, q, &v[(lane * P::B + q) * R]);
+      for (int q = 0; q < P::B; ++q) P::load(buf, wlen<C>(L), tw, lane, q, &v[(lane * P::B + q) * R]);
     for (int lane = 0; lane < 32; ++lane)
-      for (int q = 0; q < P::B; ++q) P::store(buf, L, lane, q, &v[(lane * P::B + q) * R]);
+      for (int q = 0; q < P::B; ++q) P::store(buf, wlen<C>(L), lane, q, &v[(lane * P::B + q) * R]);
     if constexpr (sizeof...(Rest) > 0) HRun<C, L, NL, INV, Ns * R, Rest...>::go(buf, tw);
   }
 };
@@ -37,12 +37,12 @@ struct HRunIO {
     for (int lane = 0; lane < 32; ++lane)
       for (int q = 0; q < P::B; ++q) {
         if constexpr (FIRST) P::load_fn(ld, lane, q, &v[(lane * P::B + q) * R]);
-        else P::load(buf, L, tw, lane, q, &v[(lane * P::B + q) * R]);
+        else P::load(buf, wlen<C>(L), tw, lane, q, &v[(lane * P::B + q) * R]);
       }
     for (int lane = 0; lane < 32; ++lane)
       for (int q = 0; q < P::B; ++q) {
         if constexpr (LAST) P::store_fn(st, lane, q, &v[(lane * P::B + q) * R]);
-        else P::store(buf, L, lane, q, &v[(lane * P::B + q) * R]);
+        else P::store(buf, wlen<C>(L), lane, q, &v[(lane * P::B + q) * R]);
       }
     if constexpr (!LAST) HRunIO<C, L, NL, INV, Ns * R, false, Rest...>::go(buf, tw, ld, st);
   }
@@ -57,7 +57,8 @@ struct HDoIO<C, L, NL, INV, Radices<Rs...>> {
 template <typename C, int L, int NL, bool INV, bool IO = false>
 double check() {
   const long double PI = 3.141592653589793238462643383279502884L;
-  std::vector<C> tw(L), buf(NL * L);
+  constexpr int LW = wlen<C>(L);
+  std::vector<C> tw(L), buf(NL * LW, cmk<C>(1e30, 1e30));
   for (int j = 0; j < L; ++j) tw[j] = cmk<C>((double)cosl(-2 * PI * j / L), (double)sinl(-2 * PI * j / L));
   std::mt19937 rng(L * 7 + NL);
   std::normal_distribution<double> nd;
@@ -70,7 +71,7 @@ double check() {
   for (int l = 0; l < NL; ++l)
     for (int n = 0; n < L; ++n) {
       in[l * L + n] = cmk<C>((double)xr[l * L + n], (double)xi[l * L + n]);
-      buf[l * L + wsw<C>(n)] = in[l * L + n];
+      buf[l * LW + wsw<C>(n)] = in[l * L + n];
     }
   typedef typename WPlan<L, NL, FftMaxRadix<C>::v>::R RS;
   if (IO) {
@@ -78,7 +79,7 @@ double check() {
     auto st = [&](int l, int k, C v) { outv[l * L + k] = v; };
     HDoIO<C, L, NL, INV, RS>::go(buf.data(), tw.data(), ld, st);
     for (int l = 0; l < NL; ++l)
-      for (int k = 0; k < L; ++k) buf[l * L + wsw<C>(k)] = outv[l * L + k];
+      for (int k = 0; k < L; ++k) buf[l * LW + wsw<C>(k)] = outv[l * L + k];
   } else {
     HDo<C, L, NL, INV, RS>::go(buf.data(), tw.data());
   }
@@ -92,7 +93,7 @@ double check() {
         sr += xr[l * L + n] * c - xi[l * L + n] * s;
         si += xr[l * L + n] * s + xi[l * L + n] * c;
       }
-      const C got = buf[l * L + wsw<C>(k)];
+      const C got = buf[l * LW + wsw<C>(k)];
       err = fmax(err, (double)hypotl(got.x - sr, got.y - si));
       nrm = fmax(nrm, (double)hypotl(sr, si));
     }
