@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
                                            PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab,
                                            int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Ny = g.Ny;
+  constexpr int Ny = M / 4 + 1;  // the launcher checks g.Ny, g.Py against M
   Carve cv(smem_raw);
   C* tws = cv.take<C>(M);
   double2* w = cv.take<double2>(Ny);
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
     }
     return from_d2<C>(e);
   };
-  const int Py = g.Py;
+  constexpr int Py = M / 2 + 1;
   C* d0 = pencil_ptr<C>(out, 2 * warp, p);
   C* d1 = pencil_ptr<C>(out, 2 * warp + 1, p);
   auto st = [&](int l, int k, C val) {
@@ -722,15 +722,15 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 // also differentiate theirs), while warps 3 and 4 build the derivative
 // chains of v and omega_y; no block barrier inside the transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(160, 3) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
                                             FftTab<C> tabP, int boot, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Ny = g.Ny;
-  const int Py = g.Py;
-  const int N = Ny - 1;
+  constexpr int Ny = M / 4 + 1;  // the launcher checks g.Ny, g.Py against M
+  constexpr int Py = M / 2 + 1;
+  constexpr int N = Ny - 1;
   const int LB = Ny + 8;
   Carve cv(smem_raw);
   C* tws = cv.take<C>(M);
@@ -979,8 +979,10 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
                       PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st) {
-  // the warp form stages its inputs by bulk copies: 16-byte aligned sources
-  const bool bulk_ok = aligned16(V) && aligned16(O) && aligned16(tab.tw);
+  // the warp form stages its inputs by bulk copies (16-byte aligned
+  // sources) and takes Ny = M/4 + 1, Py = M/2 + 1 as compile-time constants
+  const bool bulk_ok = aligned16(V) && aligned16(O) && aligned16(tab.tw) &&
+                       g.Ny == tab.plan.L / 4 + 1 && g.Py == tab.plan.L / 2 + 1;
   return with_len_m(tab.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     // warp-FFT form for FP32 (the FP64 form keeps the block FFT, whose
@@ -1007,11 +1009,13 @@ template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
                       double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
                       PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st) {
-  // the warp form stages its inputs by bulk copies: 16-byte aligned pencils
-  // with room for Py rounded up to even
+  // the warp form stages its inputs by bulk copies (16-byte aligned pencils
+  // with room for Py rounded up to even) and takes Ny = M/4 + 1,
+  // Py = M/2 + 1 as compile-time constants
   const bool bulk_ok = aligned16(lam.base) && (lam.ps * sizeof(C)) % 16 == 0 &&
                        (lam.fs * sizeof(C)) % 16 == 0 && lam.ps >= ((g.Py + 1) & ~1) && aligned16(V) &&
-                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && aligned16(tabP.tw);
+                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && aligned16(tabP.tw) &&
+                       g.Ny == tabP.plan.L / 4 + 1 && g.Py == tabP.plan.L / 2 + 1;
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {

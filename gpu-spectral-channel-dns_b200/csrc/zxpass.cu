@@ -148,11 +148,12 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = (C*)smem_raw;
   C* lines = tws + L;
-  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
+  const int Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
-  const int hz = Nz / 2;
+  constexpr int hz = Nz / 2;
   for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
   // pencil side: line li = (kxl, yl) of this thread
   {
@@ -218,7 +219,8 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tws = (C*)smem_raw;
   C* lines = tws + L;
-  const int Nz = g.Nz, Kx = g.Kx, Py = g.Py;
+  constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
+  const int Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tws, LS);
   __syncthreads();
   // pencil side: line li = (kxl, yl) of this thread, wavenumbers kz
-  const int hz = Nz / 2;
+  constexpr int hz = Nz / 2;
   const int li = threadIdx.x % NL;
   const int kx = kx0 + li / TY, y = y0 + li % TY;
   if (kx >= Kx || y >= Py) return;
@@ -412,7 +414,7 @@ __global__ void __launch_bounds__(96, 4) k_xw(RowArr in, RowArr out, DnsGeom g, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
   constexpr int Px = L;
-  const int hx = g.Nx / 2;
+  constexpr int hx = L / 3;  // Nx / 2 = mx / 3 (the launcher checks it): branches of the packing resolve at compile time
   C* tws = (C*)smem_raw;
   constexpr int LW = wlen<C>(L);                        // line stride
   C* z = tws + L;                                       // 12 lines
@@ -620,6 +622,7 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     if (g.Nz == L / 3 * 2) {
       const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
       // 4 x 4 tile: whole 32-byte sectors on both sides.  Three CTAs per SM
       // and the rest of the SM's memory as L1: the pencil-side gathers of
@@ -630,6 +633,7 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
       dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
       k_zbw<C, L, 8, 4, 4><<<grid, 256, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
+     }
     }
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zb<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -644,12 +648,14 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     if (g.Nz == L / 3 * 2) {
       const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
       dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
       k_zfw<C, L, 8><<<grid, 256, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
+     }
     }
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zf<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -668,7 +674,7 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
       const long long nrows = (long long)g.Py * g.Pz;
       // four rows per CTA within one wall-normal plane; a warp's 8 staged
       // rows of 128 bins fit in its 4 lines
-      if (g.Pz % 4 == 0 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
+      if (g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
           in.fs % 2 == 0) {
         const size_t sm = ((size_t)L + 12 * (size_t)wlen<C>(L)) * sizeof(C) + 64;
         cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
