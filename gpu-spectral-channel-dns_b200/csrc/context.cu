@@ -113,6 +113,8 @@ dns_status build_wall_solver(dns_ctx* c) {
   wd.nslots = (long long)g.Kx * g.Kh;
   wd.ngroups = (wd.nslots + 15) / 16;
   if (wall_smem_bytes(wd) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
+  if (wall_scratch_complex(wd) * 16 > c->F6_bytes)
+    return fail(DNS_ERR_ARG, "wall solve scratch does not fit the transform buffer");
   CK(c->alloc(&c->wfac, fac.size()));
   CK(c->alloc(&c->wQ, Q.size()));
   CK(cudaMemcpy(c->wfac, fac.data(), fac.size() * 16, cudaMemcpyHostToDevice));
@@ -155,8 +157,8 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
     return e;
   mark();
   if (!boot)
-    if ((e = launch_wall_solve(c->wfac, c->V, c->O, c->rv, c->ro, c->wQ, c->wd, g, c->ph,
-                               c->status, c->st)))
+    if ((e = launch_wall_solve(c->wfac, c->V, c->O, c->rv, c->ro, c->wQ, (double2*)c->F6, c->wd, g,
+                               c->ph, c->status, c->st)))
       return e;
   mark();
   return cudaSuccess;
@@ -298,7 +300,6 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   c->wd.delta = wall::base_degree(p->U1, p->U2);
   c->wd.nv = c->wd.no = Ny + c->wd.delta;
   c->wd.gp = c->wd.nv;
-  c->wd.SP = (std::max(c->wd.nv, c->wd.no) | 1);
   c->wd.qbytes = (int)((7 * (size_t)c->wd.no * 8 + 15) & ~(size_t)15);
   const size_t gn = (size_t)g.H * c->wd.gp;
   if ((e = c->alloc(&c->T0, NN)) || (e = c->alloc(&c->T2, NN)) || (e = c->alloc(&c->T4, NN)) ||
@@ -306,7 +307,7 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
       (e = c->alloc(&c->Uy, g.Py)) || (e = c->alloc(&c->V, hn)) || (e = c->alloc(&c->O, hn)) ||
       (e = c->alloc(&c->Nvp, hn)) || (e = c->alloc(&c->Nop, hn)) || (e = c->alloc(&c->rv, gn)) ||
       (e = c->alloc(&c->ro, gn)) || (e = c->alloc(&c->status, 1)) ||
-      (e = c->alloc((unsigned char**)&c->F6, f6 * csz)) ||
+      (e = c->alloc((unsigned char**)&c->F6, c->F6_bytes = f6 * csz)) ||
       (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
       (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny + 8 * (size_t)c->wd.nv)))
     return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));

@@ -37,8 +37,9 @@ struct dns_ctx {
   double* wQ = nullptr;
   WallDims wd{};
   double* rtab = nullptr;  // y1 tables: B^4 C_m (4 x nv), B^2 C_m (2 x no), cos(k pi/N)
-  void* F6 = nullptr;
+  void* F6 = nullptr;  // also the wall solve's scratch (free while it runs)
   void* G6 = nullptr;
+  size_t F6_bytes = 0;
   double2* scratch = nullptr;
   int* status = nullptr;
   bool have_state = false, booted = false, wall_ready = false;

@@ -10,8 +10,11 @@
 // the order the solve reads them (v forward rows, v backward rows, omega
 // forward rows, omega backward rows; each row holds its entries for the 16
 // slots side by side), and are streamed through a shared-memory ring with
-// cp.async.bulk and mbarriers.  Each lane keeps its right-hand side, the
-// intermediate solution and the tilting term in one shared-memory row.
+// cp.async.bulk and mbarriers.  Each lane keeps its intermediate solution
+// and tilting term in one column of a global scratch of the group (rows
+// interleaved over the lanes, L2-resident, read two ring chunks ahead into
+// registers), so that a CTA needs only the ring and two small tables in
+// shared memory and several CTAs share an SM.
 //
 // Inputs from the y1 kernel: g_v, g_o (rows K.. of the integrated
 // collocation right-hand sides, the v^n part of the tilting term included).
@@ -37,8 +40,9 @@ __device__ __forceinline__ double2 sel(bool p, double2 a) { return p ? a : make_
 template <int KLV, int KUV, int KLO, int KUO>
 struct WallCfg {
   static constexpr int E0 = KLV, E1 = 1 + KUV + 2, E2 = KLO, E3 = 1 + KUO;
-  static constexpr int R0 = rows_per_chunk(E0, 64), R1 = rows_per_chunk(E1, 64);
-  static constexpr int R2 = rows_per_chunk(E2, 16), R3 = rows_per_chunk(E3, 64);
+  // rows per ring chunk; the solve keeps two chunks of vector rows in registers
+  static constexpr int R0 = rows_per_chunk(E0, 12), R1 = rows_per_chunk(E1, 12);
+  static constexpr int R2 = rows_per_chunk(E2, 8), R3 = rows_per_chunk(E3, 12);
 };
 
 // chunk c of a group's stream: byte count and offset (complex values)
@@ -69,17 +73,15 @@ template <int KLV, int KUV, int KLO, int KUO>
 __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ fac, double2* V,
                                                    double2* O, const double2* __restrict__ gv,
                                                    const double2* __restrict__ go,
-                                                   const double* __restrict__ Qg, WallDims wd,
-                                                   DnsGeom g, PhysParams ph, int* status) {
+                                                   const double* __restrict__ Qg, double2* Sw,
+                                                   WallDims wd, DnsGeom g, PhysParams ph, int* status) {
   typedef WallCfg<KLV, KUV, KLO, KUO> CF;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = (uint64_t*)smem_raw;
-  uint64_t* gbar = full + WALL_NST;
   double2* ring = (double2*)(smem_raw + WALL_HDR);
   double* Qs = (double*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG);
-  double2* S = (double2*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG + wd.qbytes);
   // recombination weights 2k/(k+1), (k-3)/(k-1) of the clamped basis, k <= N
-  double* rc2 = (double*)(S + (size_t)32 * wd.SP);
+  double* rc2 = Qs + wd.qbytes / 8;
   double* rc4 = rc2 + g.Ny;
 
   const int lane = threadIdx.x;
@@ -97,7 +99,11 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
   const double kap = zero ? 0.0 : -0.5 * ib * ph.dt;  // tilting weight of this pencil
   const int N = g.Ny - 1, Ny = g.Ny;
-  double2* Sr = S + (size_t)lane * wd.SP;
+  // this lane's vector (right-hand side, intermediate solution, tilting
+  // term) in the group's scratch, rows interleaved over the 32 lanes: a
+  // row of the warp is one contiguous 512-byte access
+  double2* S = Sw + (long long)blockIdx.x * 32 * wd.nv + lane;
+  const double2 z2 = make_double2(0.0, 0.0);
   const double2* gfac = fac + (long long)blockIdx.x * wd.group_complex;
   const int nch0 = (wd.nv + CF::R0 - 1) / CF::R0, nch1 = (wd.nv + CF::R1 - 1) / CF::R1;
   const int nch2 = (wd.no + CF::R2 - 1) / CF::R2, nch3 = (wd.no + CF::R3 - 1) / CF::R3;
@@ -131,12 +137,14 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       issue(c + WALL_NST);
     }
   };
+  // scratch rows (plain loads: the kernel writes them) and right-hand sides
+  auto lds = [&](int i) { return (i >= 0 && i < wd.nv) ? S[32 * i] : z2; };
+  const double2* gvp = gv + pen * wd.gp;
+  const double2* gop = go + pen * wd.gp;
 
-  // ---- start: barriers, ring prefetch, right-hand sides of v -------------
-  const unsigned amask = __ballot_sync(0xffffffffu, active);
+  // ---- start: barriers, ring prefetch, tables ----------------------------
   if (lane == 0) {
     for (int s = 0; s < WALL_NST; ++s) mbar_init(&full[s], 1);
-    mbar_init(gbar, 1);
     fence_mbar_init();
   }
   __syncwarp();
@@ -145,63 +153,67 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
     rc2[k] = 2.0 * k / (k + 1);
     rc4[k] = (k >= 4) ? (double)(k - 3) / (double)(k - 1) : 0.0;
   }
-  if (lane == 0) {
-    mbar_expect_tx(gbar, (uint32_t)(__popc(amask) * wd.nv * 16));
+  if (lane == 0)
     for (int c = 0; c < min(WALL_NST, total); ++c) issue(c);
-  }
-  __syncwarp();
-  if (active) bulk_g2s(Sr, gv + pen * wd.gp, (uint32_t)(wd.nv * 16), gbar);
-  else
-    for (int i = 0; i < wd.nv; ++i) Sr[i] = make_double2(0.0, 0.0);
-  {
-    const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(gbar, 0, WALL_WAIT_LIMIT, status));
-    if (!ok) {
-      if (lane == 0) mbar_wait_bounded(gbar, 0, WALL_WAIT_LIMIT, nullptr);
-      abort_at(0);
-      return;
-    }
-  }
   __syncwarp();
 
   int c = 0;
   // ---- v: forward substitution (unit lower band) -------------------------
+  // the right-hand side rows of each chunk are loaded one chunk ahead
   {
+    constexpr int R = CF::R0;
     double2 yw[KLV];
 #pragma unroll
-    for (int e = 0; e < KLV; ++e) yw[e] = make_double2(0.0, 0.0);
-    for (int r0 = 0; r0 < wd.nv; r0 += CF::R0, ++c) {
+    for (int e = 0; e < KLV; ++e) yw[e] = z2;
+    double2 nxt[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) nxt[rr] = (active && rr < wd.nv) ? __ldg(gvp + rr) : z2;
+    for (int r0 = 0; r0 < wd.nv; r0 += R, ++c) {
+      double2 cur[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        cur[rr] = nxt[rr];
+        const int i = r0 + R + rr;
+        nxt[rr] = (active && i < wd.nv) ? __ldg(gvp + i) : z2;
+      }
       if (!wait_chunk(c)) { abort_at(c); return; }
       const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
-      const int rows = min(CF::R0, wd.nv - r0);
-      for (int rr = 0; rr < rows; ++rr) {
-        const int i = r0 + rr;
-        const double2* Lr = ch + rr * CF::E0 * 16;
-        // the older entries in independent partial sums; the newest (y_{i-1})
-        // last, so only it is on the row-to-row critical path
-        double2 a0 = Sr[i], a1 = make_double2(0.0, 0.0);
+      const int rows = min(R, wd.nv - r0);
 #pragma unroll
-        for (int e = 0; e < KLV - 1; ++e) {
-          if (e & 1) a1 = a1 + cmul(Lr[e * 16], yw[e]);
-          else a0 = a0 - cmul(Lr[e * 16], yw[e]);
+      for (int rr = 0; rr < R; ++rr) {
+        if (rr < rows) {
+          const int i = r0 + rr;
+          const double2* Lr = ch + rr * CF::E0 * 16;
+          // the older entries in independent partial sums; the newest
+          // (y_{i-1}) last, so only it is on the row-to-row critical path
+          double2 a0 = cur[rr], a1 = z2;
+#pragma unroll
+          for (int e = 0; e < KLV - 1; ++e) {
+            if (e & 1) a1 = a1 + cmul(Lr[e * 16], yw[e]);
+            else a0 = a0 - cmul(Lr[e * 16], yw[e]);
+          }
+          const double2 acc = (a0 - a1) - cmul(Lr[(KLV - 1) * 16], yw[KLV - 1]);
+          S[32 * i] = acc;
+#pragma unroll
+          for (int e = 0; e < KLV - 1; ++e) yw[e] = yw[e + 1];
+          yw[KLV - 1] = acc;
         }
-        const double2 acc = (a0 - a1) - cmul(Lr[(KLV - 1) * 16], yw[KLV - 1]);
-        Sr[i] = acc;
-#pragma unroll
-        for (int e = 0; e < KLV - 1; ++e) yw[e] = yw[e + 1];
-        yw[KLV - 1] = acc;
       }
       release(c);
     }
   }
   // ---- v: back substitution, recombination, tilting term -----------------
+  // rows descend; a chunk's rows are loaded one chunk ahead.  The tilting
+  // term of row k+1 is written over rows already consumed (k + 1 > i).
   {
+    constexpr int R = CF::R1;
     double2 xw[KUV];
 #pragma unroll
-    for (int e = 0; e < KUV; ++e) xw[e] = make_double2(0.0, 0.0);
-    double2 xd0 = make_double2(0.0, 0.0), xd1 = make_double2(0.0, 0.0);
+    for (int e = 0; e < KUV; ++e) xw[e] = z2;
+    double2 xd0 = z2, xd1 = z2;
     double2 P[7];  // P[j]: partial tilting sum of row k+1-j, k = next coefficient emitted
 #pragma unroll
-    for (int j = 0; j < 7; ++j) P[j] = make_double2(0.0, 0.0);
+    for (int j = 0; j < 7; ++j) P[j] = z2;
     const int nbv = zero ? N - 1 : N - 3;
     // base-flow degree (KLV = deg U + 4): U' = U1 (degree 1) makes the
     // tilting operator B^2 U1, three diagonals; U' = 0 (degree 0) none
@@ -214,41 +226,53 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
         const int r = k + 1 - j;
         if (r >= 0 && r < wd.no) P[j] = P[j] + a * Qs[7 * r + j];
       }
-      if (k + 1 < wd.no) Sr[k + 1] = muli(P[0] * kap);
+      if (k + 1 < wd.no) S[32 * (k + 1)] = muli(P[0] * kap);
 #pragma unroll
       for (int j = 0; j < 6; ++j) P[j] = P[j + 1];
-      P[6] = make_double2(0.0, 0.0);
+      P[6] = z2;
     };
-    for (int r0 = 0; r0 < wd.nv; r0 += CF::R1, ++c) {
+    double2 nxt[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) nxt[rr] = lds(wd.nv - 1 - rr);
+    for (int r0 = 0; r0 < wd.nv; r0 += R, ++c) {
+      double2 cur[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        cur[rr] = nxt[rr];
+        nxt[rr] = lds(wd.nv - 1 - (r0 + R + rr));
+      }
       if (!wait_chunk(c)) { abort_at(c); return; }
       const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
-      const int rows = min(CF::R1, wd.nv - r0);
-      for (int rr = 0; rr < rows; ++rr) {
-        const int i = wd.nv - 1 - (r0 + rr);
-        const double2* Ur = ch + rr * CF::E1 * 16;
-        double2 a0 = Sr[i];
-        if (i >= N + 2) Sr[i] = make_double2(0.0, 0.0);  // no tilting term above row N+1
-        // independent partial sums; x_{i+1} enters last
-        double2 a1 = cmul(Ur[(KUV + 1) * 16], xd0) + cmul(Ur[(KUV + 2) * 16], xd1);
-        double2 a2 = make_double2(0.0, 0.0);
+      const int rows = min(R, wd.nv - r0);
 #pragma unroll
-        for (int e = KUV; e >= 2; --e) {
-          if (e & 1) a1 = a1 + cmul(Ur[e * 16], xw[e - 1]);
-          else a2 = a2 + cmul(Ur[e * 16], xw[e - 1]);
-        }
-        const double2 acc = (a0 - (a1 + a2)) - cmul(Ur[16], xw[0]);
-        const double2 x = cmul(Ur[0], acc);
-        if (i == wd.nv - 1) xd1 = x;
-        if (i == wd.nv - 2) xd0 = x;
+      for (int rr = 0; rr < R; ++rr) {
+        if (rr < rows) {
+          const int i = wd.nv - 1 - (r0 + rr);
+          const double2* Ur = ch + rr * CF::E1 * 16;
+          const double2 a0 = cur[rr];
+          if (i >= N + 2) S[32 * i] = z2;  // no tilting term above row N+1
+          // independent partial sums; x_{i+1} enters last
+          double2 a1 = cmul(Ur[(KUV + 1) * 16], xd0) + cmul(Ur[(KUV + 2) * 16], xd1);
+          double2 a2 = z2;
 #pragma unroll
-        for (int e = KUV - 1; e >= 1; --e) xw[e] = xw[e - 1];
-        xw[0] = x;
-        if (i < nbv) {
-          if (!zero) {
-            const int k = i + 4;
-            emit(k, sel(i + 4 < nbv, xw[4]) - sel(i + 2 < nbv, xw[2]) * rc2[k] + x * rc4[k]);
-          } else {
-            emit(i + 2, x - sel(i + 2 < nbv, xw[2]));
+          for (int e = KUV; e >= 2; --e) {
+            if (e & 1) a1 = a1 + cmul(Ur[e * 16], xw[e - 1]);
+            else a2 = a2 + cmul(Ur[e * 16], xw[e - 1]);
+          }
+          const double2 acc = (a0 - (a1 + a2)) - cmul(Ur[16], xw[0]);
+          const double2 x = cmul(Ur[0], acc);
+          if (i == wd.nv - 1) xd1 = x;
+          if (i == wd.nv - 2) xd0 = x;
+#pragma unroll
+          for (int e = KUV - 1; e >= 1; --e) xw[e] = xw[e - 1];
+          xw[0] = x;
+          if (i < nbv) {
+            if (!zero) {
+              const int k = i + 4;
+              emit(k, sel(i + 4 < nbv, xw[4]) - sel(i + 2 < nbv, xw[2]) * rc2[k] + x * rc4[k]);
+            } else {
+              emit(i + 2, x - sel(i + 2 < nbv, xw[2]));
+            }
           }
         }
       }
@@ -263,44 +287,46 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       emit(1, make_double2(-xw[1].x, -xw[1].y));
       emit(0, make_double2(-xw[0].x, -xw[0].y));
     }
-    Sr[0] = muli(P[0] * kap);
+    S[0] = muli(P[0] * kap);
   }
   // ---- omega: forward substitution (adds g_o to the tilting term) --------
   {
-    constexpr int R2 = CF::R2;
+    constexpr int R = CF::R2;
     double2 ow[KLO];
 #pragma unroll
-    for (int e = 0; e < KLO; ++e) ow[e] = make_double2(0.0, 0.0);
-    const double2* gop = go + pen * wd.gp;
-    double2 gnext[R2];
+    for (int e = 0; e < KLO; ++e) ow[e] = z2;
+    double2 gnext[R], snext[R];
 #pragma unroll
-    for (int rr = 0; rr < R2; ++rr)
-      gnext[rr] = (active && rr < wd.no) ? __ldg(gop + rr) : make_double2(0.0, 0.0);
-    for (int r0 = 0; r0 < wd.no; r0 += R2, ++c) {
-      double2 gcur[R2];
+    for (int rr = 0; rr < R; ++rr) {
+      gnext[rr] = (active && rr < wd.no) ? __ldg(gop + rr) : z2;
+      snext[rr] = (rr < wd.no) ? lds(rr) : z2;
+    }
+    for (int r0 = 0; r0 < wd.no; r0 += R, ++c) {
+      double2 gcur[R], scur[R];
 #pragma unroll
-      for (int rr = 0; rr < R2; ++rr) gcur[rr] = gnext[rr];
-#pragma unroll
-      for (int rr = 0; rr < R2; ++rr) {
-        const int i = r0 + R2 + rr;
-        gnext[rr] = (active && i < wd.no) ? __ldg(gop + i) : make_double2(0.0, 0.0);
+      for (int rr = 0; rr < R; ++rr) {
+        gcur[rr] = gnext[rr];
+        scur[rr] = snext[rr];
+        const int i = r0 + R + rr;
+        gnext[rr] = (active && i < wd.no) ? __ldg(gop + i) : z2;
+        snext[rr] = (i < wd.no) ? lds(i) : z2;
       }
       if (!wait_chunk(c)) { abort_at(c); return; }
       const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
-      const int rows = min(R2, wd.no - r0);
+      const int rows = min(R, wd.no - r0);
 #pragma unroll
-      for (int rr = 0; rr < R2; ++rr) {
+      for (int rr = 0; rr < R; ++rr) {
         if (rr < rows) {
           const int i = r0 + rr;
           const double2* Lr = ch + rr * CF::E2 * 16;
-          double2 a0 = Sr[i] + gcur[rr], a1 = make_double2(0.0, 0.0);
+          double2 a0 = scur[rr] + gcur[rr], a1 = z2;
 #pragma unroll
           for (int e = 0; e < KLO - 1; ++e) {
             if (e & 1) a1 = a1 + cmul(Lr[e * 16], ow[e]);
             else a0 = a0 - cmul(Lr[e * 16], ow[e]);
           }
           const double2 acc = (a0 - a1) - cmul(Lr[(KLO - 1) * 16], ow[KLO - 1]);
-          Sr[i] = acc;
+          S[32 * i] = acc;
 #pragma unroll
           for (int e = 0; e < KLO - 1; ++e) ow[e] = ow[e + 1];
           ow[KLO - 1] = acc;
@@ -311,29 +337,42 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   }
   // ---- omega: back substitution and recombination ------------------------
   {
+    constexpr int R = CF::R3;
     double2 zw[KUO];
 #pragma unroll
-    for (int e = 0; e < KUO; ++e) zw[e] = make_double2(0.0, 0.0);
+    for (int e = 0; e < KUO; ++e) zw[e] = z2;
     const int nbo = N - 1;
-    for (int r0 = 0; r0 < wd.no; r0 += CF::R3, ++c) {
+    double2 nxt[R];
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) nxt[rr] = (rr < wd.no) ? lds(wd.no - 1 - rr) : z2;
+    for (int r0 = 0; r0 < wd.no; r0 += R, ++c) {
+      double2 cur[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        cur[rr] = nxt[rr];
+        nxt[rr] = lds(wd.no - 1 - (r0 + R + rr));
+      }
       if (!wait_chunk(c)) { abort_at(c); return; }
       const double2* ch = ring + (size_t)(c % WALL_NST) * (WALL_STG / 16) + q;
-      const int rows = min(CF::R3, wd.no - r0);
-      for (int rr = 0; rr < rows; ++rr) {
-        const int i = wd.no - 1 - (r0 + rr);
-        const double2* Ur = ch + rr * CF::E3 * 16;
-        double2 a1 = make_double2(0.0, 0.0), a2 = a1;
+      const int rows = min(R, wd.no - r0);
 #pragma unroll
-        for (int e = KUO; e >= 2; --e) {
-          if (e & 1) a1 = a1 + cmul(Ur[e * 16], zw[e - 1]);
-          else a2 = a2 + cmul(Ur[e * 16], zw[e - 1]);
+      for (int rr = 0; rr < R; ++rr) {
+        if (rr < rows) {
+          const int i = wd.no - 1 - (r0 + rr);
+          const double2* Ur = ch + rr * CF::E3 * 16;
+          double2 a1 = z2, a2 = z2;
+#pragma unroll
+          for (int e = KUO; e >= 2; --e) {
+            if (e & 1) a1 = a1 + cmul(Ur[e * 16], zw[e - 1]);
+            else a2 = a2 + cmul(Ur[e * 16], zw[e - 1]);
+          }
+          const double2 acc = (cur[rr] - (a1 + a2)) - cmul(Ur[16], zw[0]);
+          const double2 x = cmul(Ur[0], acc);
+#pragma unroll
+          for (int e = KUO - 1; e >= 1; --e) zw[e] = zw[e - 1];
+          zw[0] = x;
+          if (i < nbo && active) O[pen * Ny + i + 2] = x - sel(i + 2 < nbo, zw[2]);
         }
-        const double2 acc = (Sr[i] - (a1 + a2)) - cmul(Ur[16], zw[0]);
-        const double2 x = cmul(Ur[0], acc);
-#pragma unroll
-        for (int e = KUO - 1; e >= 1; --e) zw[e] = zw[e - 1];
-        zw[0] = x;
-        if (i < nbo && active) O[pen * Ny + i + 2] = x - sel(i + 2 < nbo, zw[2]);
       }
       release(c);
     }
@@ -345,9 +384,9 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
 }
 
 size_t wall_smem_bytes(const WallDims& wd) {
-  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)32 * wd.SP * 16 +
-         (size_t)2 * (wd.nv + 2) * 8;
+  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)2 * (wd.nv + 2) * 8;
 }
+size_t wall_scratch_complex(const WallDims& wd) { return (size_t)wd.ngroups * 32 * wd.nv; }
 
 // band instances: base-flow degree 0, 1, 2
 bool wall_band_of(int delta, int* klv, int* kuv, int* klo, int* kuo) {
@@ -359,23 +398,24 @@ bool wall_band_of(int delta, int* klv, int* kuv, int* klo, int* kuo) {
 
 template <int A, int B, int C, int D>
 static cudaError_t launch_inst(const double2* fac, double2* V, double2* O, const double2* gv,
-                               const double2* go, const double* Q, const WallDims& wd,
+                               const double2* go, const double* Q, double2* Sw, const WallDims& wd,
                                const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
   const size_t sm = wall_smem_bytes(wd);
   cudaError_t e = cudaFuncSetAttribute(k_wall_solve<A, B, C, D>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
-  k_wall_solve<A, B, C, D><<<(unsigned)wd.ngroups, 32, sm, st>>>(fac, V, O, gv, go, Q, wd, g, ph, status);
+  k_wall_solve<A, B, C, D><<<(unsigned)wd.ngroups, 32, sm, st>>>(fac, V, O, gv, go, Q, Sw, wd, g, ph,
+                                                                  status);
   return cudaGetLastError();
 }
 
 cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const double2* gv,
-                              const double2* go, const double* Q, const WallDims& wd,
+                              const double2* go, const double* Q, double2* Sw, const WallDims& wd,
                               const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
   switch (wd.delta) {
-    case 0: return launch_inst<4, 8, 2, 4>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
-    case 1: return launch_inst<5, 9, 3, 6>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
-    case 2: return launch_inst<6, 10, 4, 8>(fac, V, O, gv, go, Q, wd, g, ph, status, st);
+    case 0: return launch_inst<4, 8, 2, 4>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 1: return launch_inst<5, 9, 3, 6>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 2: return launch_inst<6, 10, 4, 8>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
   }
   return cudaErrorInvalidValue;
 }
