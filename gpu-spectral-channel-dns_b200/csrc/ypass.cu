@@ -369,15 +369,19 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   C* tws = cv.take<C>(M);
   double2* w = cv.take<double2>(Ny);
   double2* oz = cv.take<double2>(Ny);
-  double2* Dw = cv.take<double2>(Ny);
   double2* u = cv.take<double2>(Ny);
   double2* v = cv.take<double2>(Ny);
-  double2* Du = cv.take<double2>(Ny);
-  double2* Dv = cv.take<double2>(Ny);
   double2* ox = cv.take<double2>(Ny);
   double2* oy = cv.take<double2>(Ny);
   constexpr int MW = wlen<C>(M);
   C* lines = cv.take<C>((size_t)6 * MW);
+  // the derivatives live in the line buffers: dead before the transforms
+  // write them (a block barrier between)
+  static_assert((size_t)3 * ((Ny * 16 + 15) / 16 * 16) <= (size_t)6 * MW * sizeof(C), "derivatives do not fit the lines");
+  Carve cd(lines);
+  double2* Dw = cd.take<double2>(Ny);
+  double2* Du = cd.take<double2>(Ny);
+  double2* Dv = cd.take<double2>(Ny);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -989,7 +993,7 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
     // register footprint is smaller)
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
      if (bulk_ok) {
-      const size_t sm = (size_t)L * sizeof(C) + 9 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) +
+      const size_t sm = (size_t)L * sizeof(C) + 6 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) +
                         (size_t)6 * wlen<C>(L) * sizeof(C);
       cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab, status);
