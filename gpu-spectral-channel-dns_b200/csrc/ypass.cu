@@ -726,7 +726,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 // also differentiate theirs), while warps 3 and 4 build the derivative
 // chains of v and omega_y; no block barrier inside the transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __
   constexpr int N = Ny - 1;
   const int LB = Ny + 8;
   Carve cv(smem_raw);
-  C* tws = cv.take<C>(M);
+  const C* tws = tabP.tw;  // twiddles through L1 (the table is 4 KB)
   double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients, then fv, fo
   double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
   double2* Vc = cv.take<double2>(Ny);
@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __
   double2* noc = cv.take<double2>(Ny);
   double2* DV = cv.take<double2>(Ny);
   double2* D2V = cv.take<double2>(Ny);
-  double2* D3V = cv.take<double2>(Ny);
+  double2* D3V = DV;  // DV is dead once D2V is formed
   double2* D4V = cv.take<double2>(Ny);
   double2* DO = cv.take<double2>(Ny);
   double2* D2O = cv.take<double2>(Ny);
@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __
   const double kmn = kmn_of(ia, ib);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // 1. bulk copies on one barrier: twiddles, the three Lamb pencils (Py
+  // 1. bulk copies on one barrier: the three Lamb pencils (Py
   //    values, natural order, at the start of each warp's line: the first
   //    FFT pass reads them all before it writes the line), state, history
   const uint32_t lamb = (uint32_t)(((Py + 1) & ~1) * sizeof(C));
@@ -772,8 +772,7 @@ __global__ void __launch_bounds__(160, 4) k_y1w(PencilArr lam, const double2* __
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
-    mbar_expect_tx(&bar, (uint32_t)(M * sizeof(C)) + 3 * lamb + (boot ? 0u : (uint32_t)(4 * Ny * 16)));
-    bulk_g2s(tws, tabP.tw, (uint32_t)(M * sizeof(C)), &bar);
+    mbar_expect_tx(&bar, 3 * lamb + (boot ? 0u : (uint32_t)(4 * Ny * 16)));
     for (int f = 0; f < 3; ++f) bulk_g2s(lines + (size_t)f * wlen<C>(M), pencil_ptr<C>(lam, f, p), lamb, &bar);
     if (!boot) {
       bulk_g2s(Vc, V + p * Ny, (uint32_t)(Ny * 16), &bar);
@@ -1026,8 +1025,8 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
      if (bulk_ok) {
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
       const size_t bl = (size_t)3 * wlen<C>(L) * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
-      const size_t sm = a((size_t)L * sizeof(C)) + a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) +
-                        10 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
+      const size_t sm = a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) + 9 * a((size_t)g.Ny * 16) +
+                        a(8 * 16) + a(bl > bi ? bl : bi);
       cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot,
                                                     status);

@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
 // warp forward-transforms two of them, and the half spectra are unpacked to
 // the output rows.
 template <typename C, int L>
-__global__ void __launch_bounds__(96, 4) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+__global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
                                           const double* __restrict__ Uy, double Ro, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
