@@ -25,6 +25,7 @@
 
 #include "../../include/dns_b200.h"
 #include "context_impl.cuh"
+#include "wfft.cuh"
 #include "kernels.cuh"
 #include "setup.cuh"
 #include "wallsolve.h"
@@ -61,13 +62,29 @@ template <typename C> cudaError_t make_fft(int L, DevFft<C>& f) {
   if (e) return e;
   e = cudaMemcpy(f.tw, tw.data(), sizeof(C) * L, cudaMemcpyHostToDevice);
   if (e) return e;
-  return cudaMemcpy(f.drev, dr.data(), sizeof(short) * L, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(f.drev, dr.data(), sizeof(short) * L, cudaMemcpyHostToDevice);
+  if (e) return e;
+  // FP32 warp-FFT tables (1, 2, 4 lines per warp) where the length has a plan
+  if (std::is_same<C, float2>::value) {
+    for (int i = 0; i < 3; ++i) {
+      std::vector<C> t;
+      const int n = i == 0 ? wtw_table_any<C, 1>(L, t) : (i == 1 ? wtw_table_any<C, 2>(L, t) : wtw_table_any<C, 4>(L, t));
+      if (n <= 0) continue;
+      if ((e = cudaMalloc(&f.wt[i], sizeof(C) * n))) return e;
+      if ((e = cudaMemcpy(f.wt[i], t.data(), sizeof(C) * n, cudaMemcpyHostToDevice))) return e;
+    }
+  }
+  return cudaSuccess;
 }
 template <typename C> void free_fft(DevFft<C>& f) {
   cudaFree(f.tw);
   cudaFree(f.drev);
   f.tw = nullptr;
   f.drev = nullptr;
+  for (int i = 0; i < 3; ++i) {
+    cudaFree(f.wt[i]);
+    f.wt[i] = nullptr;
+  }
 }
 
 bool fft_len_ok(int L) {

@@ -9,11 +9,13 @@ template <typename C> struct DevFft {
   FftPlan plan;
   C* tw = nullptr;
   short* drev = nullptr;
+  C* wt[3] = {nullptr, nullptr, nullptr};
   FftTab<C> tab() const {
     FftTab<C> t;
     t.plan = plan;
     t.tw = tw;
     t.drev = drev;
+    for (int i = 0; i < 3; ++i) t.wt[i] = wt[i];
     return t;
   }
 };

@@ -19,6 +19,7 @@ template <typename C> struct FftTab {
   FftPlan plan;
   const C* tw;          // W_L^j, j < L
   const short* drev;    // digit-reversed position of natural index n
+  const C* wt[3];       // FP32 warp-FFT twiddle tables of the plans with 1, 2, 4 lines per warp
 };
 
 struct PencilArr {      // generic pencil-major array

@@ -19,6 +19,9 @@
 // per butterfly and immediate offsets.  Lines are wlen(L) elements apart
 // unless the caller passes another stride.
 #pragma once
+#include <cmath>
+#include <vector>
+
 #include "fft2.cuh"
 
 // butterfly index range hint for the device compiler (lets it resolve, per
@@ -83,6 +86,29 @@ constexpr bool wlin_store(int M, int NB, int Ns, int R) {
   return true;
 }
 
+// FP32 twiddles: one table per plan, pass by pass (passes with Ns > 1), the
+// (R - 1) Ns values W_L^{r k L/(Ns R)}, r = 1..R-1, k < Ns, stored [r][k]:
+// the lanes of a pass (consecutive k) read consecutive entries.  FP64 passes
+// use W_L^j, j < L, and a product recurrence instead.
+template <int... Rs> constexpr int wtw_offset(Radices<Rs...>, int Ns) {
+  const int rs[] = {Rs...};
+  int off = 0, ns = 1;
+  for (int i = 0; i < (int)sizeof...(Rs) && ns != Ns; ++i) {
+    if (ns > 1) off += (rs[i] - 1) * ns;
+    ns *= rs[i];
+  }
+  return off;
+}
+template <int... Rs> constexpr int wtw_size(Radices<Rs...>) {
+  const int rs[] = {Rs...};
+  int off = 0, ns = 1;
+  for (int i = 0; i < (int)sizeof...(Rs); ++i) {
+    if (ns > 1) off += (rs[i] - 1) * ns;
+    ns *= rs[i];
+  }
+  return off;
+}
+
 template <typename C, int L, int NL, bool INV, int R, int Ns>
 struct WPass {
   static constexpr int NB = L / R;        // butterflies per line
@@ -93,6 +119,7 @@ struct WPass {
   static constexpr bool LIN_LD = (NB & M) == 0;
   // stores i = base(j) + r Ns, base(j) = (j / Ns) Ns R + j mod Ns
   static constexpr bool LIN_ST = wlin_store(M, NB, Ns, R);
+  static constexpr int TWO = wtw_offset(typename WPlan<L, NL, FftMaxRadix<C>::v>::R(), Ns);
   DNS_HD static void load(const C* buf, int ls, const C* tw, int lane, int q, C* v) {
     const int w = lane + 32 * q;
     const int line = w / NB;
@@ -111,17 +138,21 @@ struct WPass {
       const int k = j % Ns;
       if (k > 0) {
         constexpr int step = L / (Ns * R);
-        const int ks = k * step;
-        const C w1 = tw[ks];
-        C wr = w1;
+        if constexpr (FftMaxRadix<C>::v == 8) {
+          const C w1 = tw[k * step];
+          C wr = w1;
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          if (FftMaxRadix<C>::v == 8) {
+          for (int r = 1; r < R; ++r) {
             if (r > 1) wr = cmul(wr, w1);
-          } else {
-            wr = tw[r * ks];
+            v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
           }
-          v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+        } else {
+          const C* tk = tw + TWO + k;  // entry (r, k) at tk[(r - 1) Ns]
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            const C wr = tk[(r - 1) * Ns];
+            v[r] = INV ? cmulc(v[r], wr) : cmul(v[r], wr);
+          }
         }
       }
     }
@@ -164,6 +195,50 @@ struct WPass {
     }
   }
 };
+
+// host: the FP32 twiddle table of plan (L, NL) (wtw_size entries), values
+// rounded from long double like the W_L^j table; -1 if there is no plan
+template <typename C, int L, int NL, int... Rs>
+void wtw_fill_radices(Radices<Rs...>, C* out) {
+  const long double PI = 3.141592653589793238462643383279502884L;
+  const int rs[] = {Rs...};
+  int off = 0, ns = 1;
+  for (int i = 0; i < (int)sizeof...(Rs); ++i) {
+    const int R = rs[i];
+    if (ns > 1) {
+      const int step = L / (ns * R);
+      for (int r = 1; r < R; ++r)
+        for (int k = 0; k < ns; ++k) {
+          const long double a = -2.0L * PI * (long double)(r * k * step) / (long double)L;
+          out[off + (r - 1) * ns + k] = cmk<C>((double)cosl(a), (double)sinl(a));
+        }
+      off += (R - 1) * ns;
+    }
+    ns *= R;
+  }
+}
+template <typename C, int L, int NL> int wtw_table(std::vector<C>& out) {
+  if constexpr (WPlan<L, NL, FftMaxRadix<C>::v>::ok) {
+    typedef typename WPlan<L, NL, FftMaxRadix<C>::v>::R RS;
+    out.assign(wtw_size(RS()), cmk<C>(0.0, 0.0));
+    wtw_fill_radices<C, L, NL>(RS(), out.data());
+    return (int)out.size();
+  } else {
+    return -1;
+  }
+}
+// runtime length: the lengths that have warp plans
+template <typename C, int NL> int wtw_table_any(int L, std::vector<C>& out) {
+  switch (L) {
+    case 128: return wtw_table<C, 128, NL>(out);
+    case 192: return wtw_table<C, 192, NL>(out);
+    case 256: return wtw_table<C, 256, NL>(out);
+    case 384: return wtw_table<C, 384, NL>(out);
+    case 512: return wtw_table<C, 512, NL>(out);
+    case 768: return wtw_table<C, 768, NL>(out);
+  }
+  return -1;
+}
 
 #ifdef __CUDACC__
 template <typename C, int L, int NL, bool INV, int R, int Ns>
@@ -240,7 +315,7 @@ __device__ __forceinline__ void wfft_io(C* buf, const C* __restrict__ tw, LD ld,
 // Transform the NL lines at buf (line stride ls >= wlen(L), positions wsw(i)) by
 // the calling warp.  The lines must have been written by this warp (or be
 // visible to it after a barrier); a __syncwarp is taken first.
-// tw: W_L^j, j < L.
+// tw: the plan's twiddle table (FP32, wtw_table) or W_L^j, j < L (FP64).
 template <typename C, int L, int NL, bool INV>
 __device__ __forceinline__ void wfft(C* buf, const C* __restrict__ tw, int ls = wlen<C>(L)) {
   __syncwarp();

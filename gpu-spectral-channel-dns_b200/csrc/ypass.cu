@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
 }
 
 // Same pass with the warp FFT: three warps per pencil, two of the six lines
-// per warp, no block barrier inside the transforms; the twiddle table is
-// staged in shared memory.
+// per warp, no block barrier inside the transforms; twiddles from the
+// plan's table through L1.
 template <typename C, int M>
 __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const double2* __restrict__ O,
                                            PencilArr out, DnsGeom g, PhysParams ph, FftTab<C> tab,
@@ -366,7 +366,6 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int Ny = M / 4 + 1;  // the launcher checks g.Ny, g.Py against M
   Carve cv(smem_raw);
-  C* tws = cv.take<C>(M);
   double2* w = cv.take<double2>(Ny);
   double2* oz = cv.take<double2>(Ny);
   double2* u = cv.take<double2>(Ny);
@@ -395,8 +394,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
-    mbar_expect_tx(&bar, (uint32_t)(M * sizeof(C) + 2 * Ny * 16));
-    bulk_g2s(tws, tab.tw, (uint32_t)(M * sizeof(C)), &bar);
+    mbar_expect_tx(&bar, (uint32_t)(2 * Ny * 16));
     bulk_g2s(w, V + p * Ny, (uint32_t)(Ny * 16), &bar);
     bulk_g2s(oz, O + p * Ny, (uint32_t)(Ny * 16), &bar);
   }
@@ -455,7 +453,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   auto st = [&](int l, int k, C val) {
     if (k < Py) (l ? d1 : d0)[k] = val;
   };
-  wfft_io<C, M, 2, false>(wl, tws, ld, st);
+  wfft_io<C, M, 2, false>(wl, tab.wt[1], ld, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -737,7 +735,6 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
   constexpr int N = Ny - 1;
   const int LB = Ny + 8;
   Carve cv(smem_raw);
-  const C* tws = tabP.tw;  // twiddles through L1 (the table is 4 KB)
   double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients, then fv, fo
   double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
   double2* Vc = cv.take<double2>(Ny);
@@ -806,7 +803,7 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
         lf[k] = c;
       }
     };
-    wfft_io<C, M, 1, false>(wline, tws, ld, st);
+    wfft_io<C, M, 1, false>(wline, tabP.wt[0], ld, st);
     if (warp < 2) ddz_warp(lf, D1 + (size_t)warp * Ny, Ny);
   } else if (!boot && warp == 3) {
     ddz_warp(Vc, DV, Ny);
@@ -984,7 +981,7 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
                       PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st) {
   // the warp form stages its inputs by bulk copies (16-byte aligned
   // sources) and takes Ny = M/4 + 1, Py = M/2 + 1 as compile-time constants
-  const bool bulk_ok = aligned16(V) && aligned16(O) && aligned16(tab.tw) &&
+  const bool bulk_ok = aligned16(V) && aligned16(O) && tab.wt[1] &&
                        g.Ny == tab.plan.L / 4 + 1 && g.Py == tab.plan.L / 2 + 1;
   return with_len_m(tab.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
@@ -992,8 +989,7 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
     // register footprint is smaller)
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
      if (bulk_ok) {
-      const size_t sm = (size_t)L * sizeof(C) + 6 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) +
-                        (size_t)6 * wlen<C>(L) * sizeof(C);
+      const size_t sm = 6 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) + (size_t)6 * wlen<C>(L) * sizeof(C);
       cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab, status);
       return cudaGetLastError();
@@ -1017,7 +1013,7 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
   // Py = M/2 + 1 as compile-time constants
   const bool bulk_ok = aligned16(lam.base) && (lam.ps * sizeof(C)) % 16 == 0 &&
                        (lam.fs * sizeof(C)) % 16 == 0 && lam.ps >= ((g.Py + 1) & ~1) && aligned16(V) &&
-                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && aligned16(tabP.tw) &&
+                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && tabP.wt[0] &&
                        g.Ny == tabP.plan.L / 4 + 1 && g.Py == tabP.plan.L / 2 + 1;
   return with_len_m(tabP.plan.L, [&](auto LL) {
     constexpr int L = decltype(LL)::value;

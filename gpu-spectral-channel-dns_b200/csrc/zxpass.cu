@@ -146,15 +146,13 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
   constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tws = (C*)smem_raw;
-  C* lines = tws + L;
+  C* lines = (C*)smem_raw;
   constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
   const int Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
   constexpr int hz = Nz / 2;
-  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
   // pencil side: line li = (kxl, yl) of this thread
   {
     const int li = threadIdx.x % NL;
@@ -185,7 +183,7 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
-  wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tws, LS);
+  wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tab.wt[1], LS);
   __syncthreads();
   // row side: this thread's kx, flat index i = yl * Pz + zp
   const int kxl = threadIdx.x % TX;
@@ -217,14 +215,12 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
   constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tws = (C*)smem_raw;
-  C* lines = tws + L;
+  C* lines = (C*)smem_raw;
   constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
   const int Kx = g.Kx, Py = g.Py;
   const int kx0 = blockIdx.x * TX;
   const int y0 = blockIdx.y * TY;
   const int f = blockIdx.z;
-  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
   constexpr int ZB = 8;
   // row side: this thread's kx, flat index i = yl * Pz + zp; rows beyond
   // Py and columns beyond Kx read as zero
@@ -253,7 +249,7 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
-  wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tws, LS);
+  wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tab.wt[1], LS);
   __syncthreads();
   // pencil side: line li = (kxl, yl) of this thread, wavenumbers kz
   constexpr int hz = Nz / 2;
@@ -415,9 +411,8 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
   typedef T_of<C> T;
   constexpr int Px = L;
   constexpr int hx = L / 3;  // Nx / 2 = mx / 3 (the launcher checks it): branches of the packing resolve at compile time
-  C* tws = (C*)smem_raw;
   constexpr int LW = wlen<C>(L);                        // line stride
-  C* z = tws + L;                                       // 12 lines
+  C* z = (C*)smem_raw;                                  // 12 lines
   uint64_t* bars = (uint64_t*)(z + (size_t)12 * LW);     // one per warp
   const long long r0 = (long long)blockIdx.x * 4;
   const long long nrows = (long long)g.Py * g.Pz;
@@ -443,7 +438,6 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     const int fa = q == 0 ? 0 : (q == 1 ? 3 : 2), fb = q == 0 ? 1 : (q == 1 ? 4 : 5);
     bulk_g2s(zw + (size_t)lane * SR, prow<C>(in, (lane & 1) ? fb : fa, row), SR * sizeof(C), bar);
   }
-  for (int n = threadIdx.x; n < L; n += blockDim.x) tws[n] = tab.tw[n];
   if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, 1LL << 31, status))) {
     if (lane == 0) {
       atomicOr(status, 1);
@@ -456,7 +450,7 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     const C* stg = zw;
     auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
     auto st = [&](int l, int k, C v) { zw[(size_t)l * LW + wsw<C>(k)] = v; };
-    wfft_io<C, L, 4, true>(zw, tws, ld, st);
+    wfft_io<C, L, 4, true>(zw, tab.wt[2], ld, st);
   }
   __syncthreads();
   const T ro = (T)Ro;
@@ -485,7 +479,7 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     z[(size_t)5 * LW + op] = B1;
   }
   __syncthreads();
-  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, tws);
+  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, tab.wt[1]);
   __syncthreads();
   // unpack: output row o = 3 rl + fl (field fl of row rl) by warp o mod 3,
   // lanes over the bins k; shared loads of a batch before its stores
@@ -622,8 +616,8 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-     if (g.Nz == L / 3 * 2) {
-      const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
+     if (g.Nz == L / 3 * 2 && tab.wt[1]) {
+      const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
       // 4 x 4 tile: whole 32-byte sectors on both sides.  Three CTAs per SM
       // and the rest of the SM's memory as L1: the pencil-side gathers of
       // neighbouring threads share sectors (measured: a quarter faster than
@@ -648,8 +642,8 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-     if (g.Nz == L / 3 * 2) {
-      const size_t sm = ((size_t)L + 16 * (wlen<C>(L) + 1)) * sizeof(C);
+     if (g.Nz == L / 3 * 2 && tab.wt[1]) {
+      const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
       dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
@@ -674,9 +668,9 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
       const long long nrows = (long long)g.Py * g.Pz;
       // four rows per CTA within one wall-normal plane; a warp's 8 staged
       // rows of 128 bins fit in its 4 lines
-      if (g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
+      if (tab.wt[1] && tab.wt[2] && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
           in.fs % 2 == 0) {
-        const size_t sm = ((size_t)L + 12 * (size_t)wlen<C>(L)) * sizeof(C) + 64;
+        const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
         cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
         return cudaGetLastError();

@@ -74,6 +74,13 @@ double check() {
       buf[l * LW + wsw<C>(n)] = in[l * L + n];
     }
   typedef typename WPlan<L, NL, FftMaxRadix<C>::v>::R RS;
+  // FP32 passes read the plan's pass-by-pass table, FP64 passes W_L^j
+  if (FftMaxRadix<C>::v != 8) {
+    std::vector<C> wt;
+    wtw_table<C, L, NL>(wt);
+    wt.push_back(cmk<C>(0.0, 0.0));  // never empty
+    tw = wt;
+  }
   if (IO) {
     auto ld = [&](int l, int n) { return in[l * L + n]; };
     auto st = [&](int l, int k, C v) { outv[l * L + k] = v; };
