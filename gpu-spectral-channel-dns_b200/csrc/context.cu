@@ -158,7 +158,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   mark();
   if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->status, c->st))) return e;
   mark();
-  if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st))) return e;
+  if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status))) return e;
   mark();
   if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st))) return e;
   mark();

@@ -276,40 +276,40 @@ struct WDo<C, L, NL, INV, Radices<Rs...>> {
 
 // Variant with the input and output fused into the first and last passes:
 // the first pass reads ld(line, n), the last hands st(line, k, value) every
-// output; buf (NL lines, wlen(L) apart) holds the intermediate passes only.
+// output; buf (NL lines, ls >= wlen(L) apart) holds the intermediate passes only.
 template <typename C, int L, int NL, bool INV, int Ns, bool FIRST, int R, int... Rest>
 struct WRunIO {
   template <class LD, class ST>
-  __device__ __forceinline__ static void go(C* buf, const C* tw, int lane, LD& ld, ST& st) {
+  __device__ __forceinline__ static void go(C* buf, int ls, const C* tw, int lane, LD& ld, ST& st) {
     typedef WPass<C, L, NL, INV, R, Ns> P;
     constexpr bool LAST = sizeof...(Rest) == 0;
     C v[P::B][R];
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
       if constexpr (FIRST) P::template load_fn<LD>(ld, lane, q, v[q]);
-      else P::load(buf, wlen<C>(L), tw, lane, q, v[q]);
+      else P::load(buf, ls, tw, lane, q, v[q]);
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
       if constexpr (LAST) P::template store_fn<ST>(st, lane, q, v[q]);
-      else P::store(buf, wlen<C>(L), lane, q, v[q]);
+      else P::store(buf, ls, lane, q, v[q]);
     }
     __syncwarp();
-    if constexpr (!LAST) WRunIO<C, L, NL, INV, Ns * R, false, Rest...>::go(buf, tw, lane, ld, st);
+    if constexpr (!LAST) WRunIO<C, L, NL, INV, Ns * R, false, Rest...>::go(buf, ls, tw, lane, ld, st);
   }
 };
 template <typename C, int L, int NL, bool INV, typename RS> struct WDoIO;
 template <typename C, int L, int NL, bool INV, int... Rs>
 struct WDoIO<C, L, NL, INV, Radices<Rs...>> {
   template <class LD, class ST>
-  __device__ __forceinline__ static void go(C* buf, const C* tw, int lane, LD& ld, ST& st) {
-    WRunIO<C, L, NL, INV, 1, true, Rs...>::go(buf, tw, lane, ld, st);
+  __device__ __forceinline__ static void go(C* buf, int ls, const C* tw, int lane, LD& ld, ST& st) {
+    WRunIO<C, L, NL, INV, 1, true, Rs...>::go(buf, ls, tw, lane, ld, st);
   }
 };
 template <typename C, int L, int NL, bool INV, class LD, class ST>
-__device__ __forceinline__ void wfft_io(C* buf, const C* __restrict__ tw, LD ld, ST st) {
-  WDoIO<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, tw, threadIdx.x & 31, ld, st);
+__device__ __forceinline__ void wfft_io(C* buf, const C* __restrict__ tw, LD ld, ST st, int ls = wlen<C>(L)) {
+  WDoIO<C, L, NL, INV, typename WPlan<L, NL, FftMaxRadix<C>::v>::R>::go(buf, ls, tw, threadIdx.x & 31, ld, st);
 }
 
 // Transform the NL lines at buf (line stride ls >= wlen(L), positions wsw(i)) by

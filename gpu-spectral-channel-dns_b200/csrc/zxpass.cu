@@ -17,6 +17,8 @@
 // Streamwise pass: two real rows share one complex FFT (a + i b).
 #include "fftline.cuh"
 #include "kernels.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <type_traits>
 
 #include "mbar.cuh"
@@ -192,6 +194,85 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
   const int ni = min(TY, Py - y0) * Pz;
   C* rowb = prow<C>(out, f, (long long)y0 * Pz) + kx;
   const C* lb = lines + kxl * TY * LS;
+  constexpr int ZB = 8;
+  for (int i0 = threadIdx.x / TX; i0 < ni; i0 += ZB * ST::IS) {
+    C v[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int i = i0 + u * ST::IS;
+      const int yl = i / Pz, zp = i - yl * Pz;
+      v[u] = (i < ni) ? lb[yl * LS + wsw<C>(zp)] : cmk<C>(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int i = i0 + u * ST::IS;
+      if (i < ni) rowb[(long long)i * out.rs] = v[u];
+    }
+  }
+}
+
+// The same inverse pass with the pencils staged by the tensor-memory
+// accelerator: warp w owns lines 2w, 2w+1 (one kx, two consecutive y) and
+// loads their Nz spanwise values with one tiled 4-D copy (box y 2 x kx 1 x
+// kz Nz x field 1, 4 KB at Nz = 256) into its own line buffer; the first FFT
+// pass reads them there (padding, Nyquist and streamwise-Nyquist zeros
+// applied in the read) before it writes the lines.  Rows beyond Py and
+// columns beyond Kx read as the copy's zero fill.  No per-element global
+// loads, no L1 dependence.
+template <typename C, int L, int NW, int TX, int TY>
+__global__ void __launch_bounds__(32 * NW, 4) k_zbt(const __grid_constant__ CUtensorMap tin, RowArr out,
+                                                 DnsGeom g, FftTab<C> tab, int* status) {
+  typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
+  constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
+  static_assert(NL == 2 * NW && TY % 2 == 0, "two lines per warp, a y pair each");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bars[NW];
+  C* lines = (C*)smem_raw;
+  constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
+  constexpr int hz = Nz / 2;
+  const int Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li0 = 2 * warp;                       // lines (kxl, yl0), (kxl, yl0 + 1)
+  const int kxl = li0 / TY, yl0 = li0 % TY;
+  C* wl = lines + (size_t)li0 * LS;
+  // the staged values [kz][y pair] at the first 128-byte boundary of the warp's lines
+  C* tile = (C*)(((uintptr_t)wl + 127) & ~(uintptr_t)127);
+  uint64_t* bar = bars + warp;
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(bar, (uint32_t)(2 * Nz * sizeof(C)));
+    tma_load_4d(tile, &tin, y0 + yl0, kx0 + kxl, 0, f, bar);
+  }
+  __syncwarp();
+  // a wait that runs out is reported and waited once more (bounded); the
+  // warp then goes on, so that every warp reaches the block barriers
+  if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, 1LL << 31, status))) {
+    if (lane == 0) {
+      atomicOr(status, 1);
+      mbar_wait_bounded(bar, 0, 1LL << 31, nullptr);
+    }
+    __syncwarp();
+  }
+  // the streamwise Nyquist column (kx = Kx - 1) stays zero
+  const bool kxok = kx0 + kxl < Kx - 1;
+  auto ld = [&](int l, int n) -> C {
+    const int kz = (n < hz) ? n : (n > Pz - hz ? n - (Pz - Nz) : -1);
+    return (kxok && kz >= 0) ? tile[2 * kz + l] : cmk<C>(0.0, 0.0);
+  };
+  auto st = [&](int l, int k, C v) { wl[(size_t)l * LS + wsw<C>(k)] = v; };
+  wfft_io<C, L, 2, true>(wl, tab.wt[1], ld, st, LS);
+  __syncthreads();
+  // row side: this thread's kx, flat index i = yl * Pz + zp
+  const int kxr = threadIdx.x % TX;
+  const int kx = kx0 + kxr;
+  if (kx >= Kx || y0 >= Py) return;
+  const int ni = min(TY, Py - y0) * Pz;
+  C* rowb = prow<C>(out, f, (long long)y0 * Pz) + kx;
+  const C* lb = lines + kxr * TY * LS;
   constexpr int ZB = 8;
   for (int i0 = threadIdx.x / TX; i0 < ni; i0 += ZB * ST::IS) {
     C v[ZB];
@@ -438,12 +519,14 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     const int fa = q == 0 ? 0 : (q == 1 ? 3 : 2), fb = q == 0 ? 1 : (q == 1 ? 4 : 5);
     bulk_g2s(zw + (size_t)lane * SR, prow<C>(in, (lane & 1) ? fb : fa, row), SR * sizeof(C), bar);
   }
+  // a wait that runs out is reported and waited once more (bounded); the
+  // warp then goes on, so that every warp reaches the block barriers
   if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, 1LL << 31, status))) {
     if (lane == 0) {
       atomicOr(status, 1);
-      mbar_wait_bounded(bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+      mbar_wait_bounded(bar, 0, 1LL << 31, nullptr);
     }
-    return;
+    __syncwarp();
   }
   __syncthreads();
   {
@@ -610,12 +693,54 @@ template <typename C> struct ZTile;
 template <> struct ZTile<double2> { enum { TX = 4, TY = 2 }; };
 template <> struct ZTile<float2> { enum { TX = 8, TY = 2 }; };
 
+namespace {
+// cuTensorMapEncodeTiled from the driver, looked up once (no -lcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+// 4-D map (y, kx, kz, field) over 8-byte pencil elements, box 2 x 1 x Nz x 1
+bool pencil_tmap(const PencilArr& in, int nf, const DnsGeom& g, size_t esz, CUtensorMap* m) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc || esz != 8 || !aligned16(in.base) || (in.ps * esz) % 16 || (in.fs * esz) % 16 || g.Nz > 256)
+    return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.Py, (cuuint64_t)g.Kx, (cuuint64_t)g.Nz, (cuuint64_t)nf};
+  const cuuint64_t strides[3] = {(cuuint64_t)(in.ps * esz), (cuuint64_t)((long long)g.Kx * in.ps * esz),
+                                 (cuuint64_t)(in.fs * esz)};
+  const cuuint32_t box[4] = {2, 1, (cuuint32_t)g.Nz, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, in.base, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace
+
 template <typename C>
-cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
+cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
+                      int* status) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     CUtensorMap tm;
+     constexpr int LS = wlen<C>(L) + 1;
+     if (status && g.Nz == L / 3 * 2 && tab.wt[1] && (size_t)g.Nz * 16 + 128 <= (size_t)2 * LS * sizeof(C) &&
+         pencil_tmap(in, nf, g, sizeof(C), &tm)) {
+      // pencils staged by tensor copies, 4 x 4 tile (whole 32-byte sectors
+      // on the row side)
+      const size_t sm = ((size_t)16 * LS) * sizeof(C);
+      cudaFuncSetAttribute(k_zbt<C, L, 8, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
+      k_zbt<C, L, 8, 4, 4><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
+      return cudaGetLastError();
+     }
      if (g.Nz == L / 3 * 2 && tab.wt[1]) {
       const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
       // 4 x 4 tile: whole 32-byte sectors on both sides.  Three CTAs per SM
@@ -713,7 +838,7 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
 }
 
 #define INST_Z(C)                                                                                  \
-  template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
+  template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*); \
   template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
                                          double, int*, cudaStream_t);                             \

@@ -3,7 +3,8 @@
 #include "kernels.cuh"
 
 template <typename C>
-cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st);
+cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
+                      int* status = nullptr);
 template <typename C>
 cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st);
 template <typename C>
