@@ -162,7 +162,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   mark();
   if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st))) return e;
   mark();
-  if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st))) return e;
+  if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status))) return e;
   mark();
   const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
   const size_t nv = c->wd.nv, no = c->wd.no;

@@ -355,6 +355,78 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   }
 }
 
+// The same forward pass with the rows staged by tensor copies: lines are
+// numbered y-major (li = yl * 4 + kxl), warp w owns lines 2w, 2w+1 (one y,
+// a kx pair) and loads their Pz values with two tiled 4-D copies (box kx 2
+// x zp Pz/2 x y 1 x field 1) into its own line buffer, [zp][kx pair]; the
+// first FFT pass reads them there.  Rows beyond Py and columns beyond Kx
+// read as the copy's zero fill.
+template <typename C, int L, int NW>
+__global__ void __launch_bounds__(32 * NW, 4) k_zft(const __grid_constant__ CUtensorMap tin, PencilArr out,
+                                                    DnsGeom g, FftTab<C> tab, int* status) {
+  constexpr int TX = 4, TY = 4;
+  typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
+  constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
+  static_assert(NL == 2 * NW && Pz % 2 == 0, "two lines per warp, a kx pair each");
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // the tile is rounded up to 128 bytes
+  __shared__ uint64_t bars[NW];
+  C* lines = (C*)smem_raw;
+  constexpr int Nz = L / 3 * 2;  // my / 3 * 2 (the launcher checks g.Nz)
+  constexpr int hz = Nz / 2;
+  const int Kx = g.Kx, Py = g.Py;
+  const int kx0 = blockIdx.x * TX;
+  const int y0 = blockIdx.y * TY;
+  const int f = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li0 = 2 * warp;
+  const int yl = li0 / TX, kxl0 = li0 % TX;
+  C* wl = lines + (size_t)li0 * LS;
+  C* tile = (C*)(((uintptr_t)wl + 127) & ~(uintptr_t)127);
+  uint64_t* bar = bars + warp;
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_expect_tx(bar, (uint32_t)(2 * Pz * sizeof(C)));
+    tma_load_4d(tile, &tin, kx0 + kxl0, 0, y0 + yl, f, bar);
+    tma_load_4d(tile + Pz, &tin, kx0 + kxl0, Pz / 2, y0 + yl, f, bar);
+  }
+  __syncwarp();
+  // a wait that runs out is reported and waited once more (bounded); the
+  // warp then goes on, so that every warp reaches the block barriers
+  if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, 1LL << 31, status))) {
+    if (lane == 0) {
+      atomicOr(status, 1);
+      mbar_wait_bounded(bar, 0, 1LL << 31, nullptr);
+    }
+    __syncwarp();
+  }
+  auto ld = [&](int l, int n) -> C { return tile[2 * n + l]; };
+  auto st = [&](int l, int k, C v) { wl[(size_t)l * LS + wsw<C>(k)] = v; };
+  wfft_io<C, L, 2, false>(wl, tab.wt[1], ld, st, LS);
+  __syncthreads();
+  // pencil side: line li = (yl, kxl) of this thread, wavenumbers kz
+  constexpr int ZB = 8;
+  const int li = threadIdx.x % NL;
+  const int kx = kx0 + li % TX, y = y0 + li / TX;
+  if (kx >= Kx || y >= Py) return;
+  const C* lsrc = lines + li * LS;
+  C* dst = ppen<C>(out, f, kx) + y;
+  const long long kzs = (long long)Kx * out.ps;
+  for (int kz0 = threadIdx.x / NL; kz0 < Nz; kz0 += ZB * ST::KS) {
+    C v[ZB];
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int kz = kz0 + u * ST::KS;
+      v[u] = (kz < Nz) ? lsrc[wsw<C>(kz <= hz ? kz : kz + (Pz - Nz))] : cmk<C>(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < ZB; ++u) {
+      const int kz = kz0 + u * ST::KS;
+      if (kz < Nz) dst[kz * kzs] = v[u];
+    }
+  }
+}
+
 namespace {
 // Hermitian half-spectra a, b (bins 0..Kx-1, Nyquist and padding zero) packed
 // as Z = A + iB over the full length Px, so that IFFT(Z) = a(x) + i b(x).
@@ -720,6 +792,21 @@ bool pencil_tmap(const PencilArr& in, int nf, const DnsGeom& g, size_t esz, CUte
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
+// 4-D map (kx, zp, y, field) over 8-byte row elements, box 2 x Pz/2 x 1 x 1
+bool row_tmap(const RowArr& in, int nf, const DnsGeom& g, size_t esz, CUtensorMap* m) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc || esz != 8 || !aligned16(in.base) || (in.rs * esz) % 16 || (in.fs * esz) % 16 || g.Pz % 2 ||
+      g.Pz / 2 > 256)
+    return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.Kx, (cuuint64_t)g.Pz, (cuuint64_t)g.Py, (cuuint64_t)nf};
+  const cuuint64_t strides[3] = {(cuuint64_t)(in.rs * esz), (cuuint64_t)((long long)g.Pz * in.rs * esz),
+                                 (cuuint64_t)(in.fs * esz)};
+  const cuuint32_t box[4] = {2, (cuuint32_t)(g.Pz / 2), 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, in.base, dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 }  // namespace
 
 template <typename C>
@@ -762,11 +849,23 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
   });
 }
 template <typename C>
-cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st) {
+cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
+                      int* status) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
   return with_len_xz(g.Pz, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     CUtensorMap tm;
+     constexpr int LS = wlen<C>(L) + 1;
+     if (status && g.Nz == L / 3 * 2 && tab.wt[1] && (size_t)L * 16 + 128 <= (size_t)2 * LS * sizeof(C) &&
+         row_tmap(in, nf, g, sizeof(C), &tm)) {
+      // rows staged by tensor copies, 4 x 4 tile
+      const size_t sm = ((size_t)16 * LS) * sizeof(C);
+      cudaFuncSetAttribute(k_zft<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
+      k_zft<C, L, 8><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
+      return cudaGetLastError();
+     }
      if (g.Nz == L / 3 * 2 && tab.wt[1]) {
       const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
       cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -839,7 +938,7 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
 
 #define INST_Z(C)                                                                                  \
   template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*); \
-  template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t);    \
+  template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*); \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
                                          double, int*, cudaStream_t);                             \
   template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \
