@@ -379,8 +379,8 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   static_assert((size_t)3 * ((Ny * 16 + 15) / 16 * 16) <= (size_t)6 * MW * sizeof(C), "derivatives do not fit the lines");
   Carve cd(lines);
   double2* Dw = cd.take<double2>(Ny);
-  double2* Du = cd.take<double2>(Ny);
-  double2* Dv = cd.take<double2>(Ny);
+  double2* D2w = cd.take<double2>(Ny);
+  double2* Doz = cd.take<double2>(Ny);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -406,27 +406,35 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
     }
     return;
   }
+  // derivatives: D w, D^2 w (warp 0) and D omega_z (warp 1); then, by
+  // linearity, u = i(ia Dw - ib oz)/k^2, v = i(ib Dw + ia oz)/k^2 and their
+  // derivatives from D^2 w, D oz (source/velocity.cu:90-170).  The mean
+  // mode holds u0, w0 in (w, oz): u = w, v = oz, omega_x = D oz, omega_y = -D w.
   const int warp = threadIdx.x >> 5;
-  if (!zero && warp == 0) ddz_warp(w, Dw, Ny);
-  __syncthreads();
-  for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    if (zero) {
-      u[n] = w[n];
-      v[n] = oz[n];
-    } else {
-      const double2 d = Dw[n], o = oz[n];
-      u[n] = muli(d * (ia * kmn1)) - muli(o * (ib * kmn1));
-      v[n] = muli(d * (ib * kmn1)) + muli(o * (ia * kmn1));
-    }
+  if (warp == 0) {
+    ddz_warp(w, Dw, Ny);
+    __syncwarp();
+    if (!zero) ddz_warp(Dw, D2w, Ny);
+  } else if (warp == 1) {
+    ddz_warp(oz, Doz, Ny);
   }
   __syncthreads();
-  if (warp == 0) ddz_warp(v, Dv, Ny);
-  if (warp == 1) ddz_warp(u, Du, Ny);
-  __syncthreads();
   for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    const double2 wn = w[n];
-    ox[n] = Dv[n] - muli(wn * ib);
-    oy[n] = muli(wn * ia) - Du[n];
+    const double2 wn = w[n], on = oz[n], d1 = Dw[n], dz = Doz[n];
+    if (zero) {
+      u[n] = wn;
+      v[n] = on;
+      ox[n] = dz;
+      oy[n] = make_double2(-d1.x, -d1.y);
+    } else {
+      const double2 d2 = D2w[n];
+      u[n] = muli(d1 * (ia * kmn1)) - muli(on * (ib * kmn1));
+      v[n] = muli(d1 * (ib * kmn1)) + muli(on * (ia * kmn1));
+      const double2 du = muli(d2 * (ia * kmn1)) - muli(dz * (ib * kmn1));
+      const double2 dv = muli(d2 * (ib * kmn1)) + muli(dz * (ia * kmn1));
+      ox[n] = dv - muli(wn * ib);
+      oy[n] = muli(wn * ia) - du;
+    }
   }
   __syncthreads();
   // this warp's two lines: fields 2 warp, 2 warp + 1; the first FFT pass
