@@ -365,22 +365,20 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
                                            int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int Ny = M / 4 + 1;  // the launcher checks g.Ny, g.Py against M
-  Carve cv(smem_raw);
-  double2* w = cv.take<double2>(Ny);
-  double2* oz = cv.take<double2>(Ny);
-  double2* u = cv.take<double2>(Ny);
-  double2* v = cv.take<double2>(Ny);
-  double2* ox = cv.take<double2>(Ny);
-  double2* oy = cv.take<double2>(Ny);
+  // everything lives in the six line buffers: warp w's two lines hold the
+  // two vectors its transforms read (u, v | w, omega_x | omega_y, omega_z),
+  // which the first FFT pass reads before it writes the lines; the
+  // derivatives share slots with the vectors computed from them element by
+  // element (D w -> u, D^2 w -> v, D omega_z -> omega_x)
   constexpr int MW = wlen<C>(M);
-  C* lines = cv.take<C>((size_t)6 * MW);
-  // the derivatives live in the line buffers: dead before the transforms
-  // write them (a block barrier between)
-  static_assert((size_t)3 * ((Ny * 16 + 15) / 16 * 16) <= (size_t)6 * MW * sizeof(C), "derivatives do not fit the lines");
-  Carve cd(lines);
-  double2* Dw = cd.take<double2>(Ny);
-  double2* D2w = cd.take<double2>(Ny);
-  double2* Doz = cd.take<double2>(Ny);
+  C* lines = (C*)smem_raw;
+  static_assert((size_t)2 * ((Ny * 16 + 15) / 16 * 16) <= (size_t)2 * MW * sizeof(C), "vectors do not fit the lines");
+  constexpr size_t VS = (Ny * 16 + 15) / 16;  // vector slot (double2, 16-byte multiple)
+  double2* r0 = (double2*)lines;
+  double2* r1 = (double2*)(lines + (size_t)2 * MW);
+  double2* r2 = (double2*)(lines + (size_t)4 * MW);
+  double2 *u = r0, *v = r0 + VS, *w = r1, *ox = r1 + VS, *oy = r2, *oz = r2 + VS;
+  double2 *Dw = u, *D2w = v, *Doz = ox;
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -997,7 +995,7 @@ cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom
     // register footprint is smaller)
     if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
      if (bulk_ok) {
-      const size_t sm = 6 * (((size_t)g.Ny * 16 + 15) & ~(size_t)15) + (size_t)6 * wlen<C>(L) * sizeof(C);
+      const size_t sm = (size_t)6 * wlen<C>(L) * sizeof(C);
       cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab, status);
       return cudaGetLastError();
