@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 // also differentiate theirs), while warps 3 and 4 build the derivative
 // chains of v and omega_y; no block barrier inside the transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
@@ -741,8 +741,6 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
   constexpr int N = Ny - 1;
   const int LB = Ny + 8;
   Carve cv(smem_raw);
-  double2* lc = cv.take<double2>((size_t)3 * Ny);  // lambda coefficients, then fv, fo
-  double2* D1 = cv.take<double2>((size_t)2 * Ny);  // D lambda_x, D lambda_y
   double2* Vc = cv.take<double2>(Ny);
   double2* Oc = cv.take<double2>(Ny);
   double2* nvc = cv.take<double2>(Ny);
@@ -757,6 +755,16 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
   const size_t bytesL = (size_t)3 * wlen<C>(M) * sizeof(C), bytesI = (size_t)4 * LB * 16;
   unsigned char* region = cv.take<unsigned char>(bytesL > bytesI ? bytesL : bytesI);
   C* lines = (C*)region;
+  // in the line buffer of warp w < 3, after its transform: the coefficients
+  // of lambda_w, then (w < 2) their derivative; fv and fo later take the
+  // slots of lambda_x, lambda_y element by element
+  constexpr size_t VS = (Ny * 16 + 15) / 16;  // vector slot (double2)
+  static_assert((size_t)2 * VS * 16 <= (size_t)wlen<C>(M) * sizeof(C), "vectors do not fit a line");
+  double2* lx = (double2*)lines;
+  double2* ly = (double2*)(lines + (size_t)wlen<C>(M));
+  double2* lz = (double2*)(lines + (size_t)2 * wlen<C>(M));
+  double2* D1x = lx + VS;
+  double2* D1y = ly + VS;
 
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
@@ -800,7 +808,7 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
   if (warp < 3) {
     C* wline = lines + (size_t)warp * wlen<C>(M);
     const C* src = wline;  // staged pencil
-    double2* lf = lc + (size_t)warp * Ny;
+    double2* lf = (double2*)wline;  // coefficients over the consumed lines
     auto ld = [&](int, int n) -> C { return (n < Py) ? src[n] : src[M - n]; };
     auto st = [&](int, int k, C val) {
       if (k < Ny) {
@@ -810,7 +818,7 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
       }
     };
     wfft_io<C, M, 1, false>(wline, tabP.wt[0], ld, st);
-    if (warp < 2) ddz_warp(lf, D1 + (size_t)warp * Ny, Ny);
+    if (warp < 2) ddz_warp(lf, lf + VS, Ny);
   } else if (!boot && warp == 3) {
     ddz_warp(Vc, DV, Ny);
     __syncwarp();
@@ -828,16 +836,16 @@ __global__ void __launch_bounds__(160, 5) k_y1w(PencilArr lam, const double2* __
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
   const double dt = ph.dt, Re = ph.Re, gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
-  double2* fv = lc;
-  double2* fo = lc + Ny;
+  double2* fv = lx;
+  double2* fo = ly;
   for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
     double2 hv, ho;
     if (zero) {
-      hv = lc[k];
-      ho = lc[Ny + k];
+      hv = lx[k];
+      ho = ly[k];
     } else {
-      hv = lc[2 * Ny + k] * kmn + muli(D1[k] * ia) + muli(D1[Ny + k] * ib);
-      ho = muli(lc[Ny + k] * ia) - muli(lc[k] * ib);
+      hv = lz[k] * kmn + muli(D1x[k] * ia) + muli(D1y[k] * ib);
+      ho = muli(ly[k] * ia) - muli(lx[k] * ib);
     }
     Nvp[p * Ny + k] = hv;
     Nop[p * Ny + k] = ho;
@@ -1027,8 +1035,7 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
      if (bulk_ok) {
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
       const size_t bl = (size_t)3 * wlen<C>(L) * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
-      const size_t sm = a((size_t)3 * g.Ny * 16) + a((size_t)2 * g.Ny * 16) + 9 * a((size_t)g.Ny * 16) +
-                        a(8 * 16) + a(bl > bi ? bl : bi);
+      const size_t sm = 9 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
       cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot,
                                                     status);
