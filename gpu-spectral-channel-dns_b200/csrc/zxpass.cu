@@ -820,12 +820,12 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
      constexpr int LS = wlen<C>(L) + 1;
      if (status && g.Nz == L / 3 * 2 && tab.wt[1] && (size_t)g.Nz * 16 + 128 <= (size_t)2 * LS * sizeof(C) &&
          pencil_tmap(in, nf, g, sizeof(C), &tm)) {
-      // pencils staged by tensor copies, 4 x 4 tile (whole 32-byte sectors
-      // on the row side)
+      // pencils staged by tensor copies (a y pair per line pair), 8 x 2
+      // tile: 64-byte runs on the row side
       const size_t sm = ((size_t)16 * LS) * sizeof(C);
-      cudaFuncSetAttribute(k_zbt<C, L, 8, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
-      k_zbt<C, L, 8, 4, 4><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
+      cudaFuncSetAttribute(k_zbt<C, L, 8, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      dim3 grid((g.Kx + 7) / 8, (g.Py + 1) / 2, nf);
+      k_zbt<C, L, 8, 8, 2><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
       return cudaGetLastError();
      }
      if (g.Nz == L / 3 * 2 && tab.wt[1]) {
