@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(32 * NW, 4) k_zbt(const __grid_constant__ CUte
                                                  DnsGeom g, FftTab<C> tab, int* status) {
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
   constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
-  static_assert(NL == 2 * NW && TY % 2 == 0, "two lines per warp, a y pair each");
+  static_assert(NL == 2 * NW && TY % 2 == 0 && ST::KS > 0, "two lines per warp, a y pair each");
   extern __shared__ __align__(16) unsigned char smem_raw[];  // the tile is rounded up to 128 bytes
   __shared__ uint64_t bars[NW];
   C* lines = (C*)smem_raw;
