@@ -399,16 +399,22 @@ dns_status dns_memory_bytes(const dns_ctx* c, size_t* b) {
   return DNS_OK;
 }
 
+// enqueue one field's copy between the caller's pencils (pitch) and the
+// library's (Ny complex, unpadded); one linear copy when the pitches agree
 static dns_status copy_pencils(dns_ctx* c, double2* dev, const void* src, void* dst, size_t pitch,
                                int where, bool to_dev) {
   const size_t w = (size_t)c->g.Ny * 16;
   if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
-  if (to_dev)
-    CK(cudaMemcpy2DAsync(dev, w, src, pitch, w, (size_t)c->g.H, kind_of(where, true), c->st));
-  else
-    CK(cudaMemcpy2DAsync(dst, pitch, dev, w, w, (size_t)c->g.H, kind_of(where, false), c->st));
-  CK(cudaStreamSynchronize(c->st));
+  const cudaMemcpyKind k = kind_of(where, to_dev);
+  if (pitch == w) {
+    if (to_dev) CK(cudaMemcpyAsync(dev, src, w * (size_t)c->g.H, k, c->st));
+    else CK(cudaMemcpyAsync(dst, dev, w * (size_t)c->g.H, k, c->st));
+  } else if (to_dev) {
+    CK(cudaMemcpy2DAsync(dev, w, src, pitch, w, (size_t)c->g.H, k, c->st));
+  } else {
+    CK(cudaMemcpy2DAsync(dst, pitch, dev, w, w, (size_t)c->g.H, k, c->st));
+  }
   return DNS_OK;
 }
 
@@ -417,6 +423,7 @@ dns_status dns_set_state(dns_ctx* c, const void* v, const void* o, size_t pitch,
   CK(cudaSetDevice(c->P.device));
   dns_status s = copy_pencils(c, c->V, v, nullptr, pitch, where, true);
   if (s == DNS_OK) s = copy_pencils(c, c->O, o, nullptr, pitch, where, true);
+  if (s == DNS_OK) CK(cudaStreamSynchronize(c->st));
   if (s == DNS_OK) c->have_state = true;
   return s;
 }
@@ -426,6 +433,7 @@ dns_status dns_get_state(dns_ctx* c, void* v, void* o, size_t pitch, int where) 
   CK(cudaSetDevice(c->P.device));
   dns_status s = copy_pencils(c, c->V, nullptr, v, pitch, where, false);
   if (s == DNS_OK) s = copy_pencils(c, c->O, nullptr, o, pitch, where, false);
+  if (s == DNS_OK) CK(cudaStreamSynchronize(c->st));
   return s;
 }
 
