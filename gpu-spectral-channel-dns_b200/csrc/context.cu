@@ -345,10 +345,17 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
     wall::cardinal_rows(N, N, 2, no, &tab[4 * (size_t)nv + no]);
     const long double PI = 3.141592653589793238462643383279502884L;
     for (int k = 0; k <= N; ++k) tab[4 * (size_t)nv + 2 * (size_t)no + k] = (double)cosl(PI * k / N);
-    // rows of B^4 (from row 4) and B^2 (from row 2) as 5- and 3-point stencils
+    // rows of B^4 (from row 4) and B^2 (from row 2) as 5- and 3-point
+    // stencils, stored weight-major ([d][r]: a warp's rows read consecutive
+    // entries)
+    std::vector<double> s4((size_t)5 * nv), s2((size_t)3 * nv);
+    wall::integration_stencils(N, nv, s4.data(), s2.data());
     double* b4 = &tab[4 * (size_t)nv + 2 * (size_t)no + Ny];
     double* b2 = b4 + 5 * (size_t)nv;
-    wall::integration_stencils(N, nv, b4, b2);
+    for (int r = 0; r < nv; ++r) {
+      for (int d = 0; d < 5; ++d) b4[(size_t)d * nv + r] = s4[(size_t)5 * r + d];
+      for (int d = 0; d < 3; ++d) b2[(size_t)d * nv + r] = s2[(size_t)3 * r + d];
+    }
     cudaMemcpy(c->rtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice);
   }
   cudaMemset(c->status, 0, sizeof(int));

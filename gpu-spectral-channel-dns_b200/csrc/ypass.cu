@@ -895,7 +895,7 @@ __global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __
     }
   }
   auto fget = [&](const double2* f, int k) { return (k >= 0 && k <= N) ? f[k] : make_double2(0.0, 0.0); };
-  constexpr int RPT = 2;  // rows per thread (n <= 2 * blockDim = 256)
+  constexpr int RPT = (Ny + 2 + 159) / 160;  // rows per thread (n <= Ny + 2, 160 threads)
   double2 iv[RPT], io[RPT];
 #pragma unroll
   for (int t = 0; t < RPT; ++t) {
@@ -905,15 +905,15 @@ __global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __
     if (r < rd.nv) {
       if (zero) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) iv[t] = iv[t] + fget(fv, r + 2 + 2 * d - 2) * __ldg(tb.b2 + 3 * r + d);
+        for (int d = 0; d < 3; ++d) iv[t] = iv[t] + fget(fv, r + 2 + 2 * d - 2) * __ldg(tb.b2 + (size_t)d * rd.nv + r);
       } else {
 #pragma unroll
-        for (int d = 0; d < 5; ++d) iv[t] = iv[t] + fget(fv, r + 4 + 2 * d - 4) * __ldg(tb.b4 + 5 * r + d);
+        for (int d = 0; d < 5; ++d) iv[t] = iv[t] + fget(fv, r + 4 + 2 * d - 4) * __ldg(tb.b4 + (size_t)d * rd.nv + r);
       }
     }
     if (r < rd.no) {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) io[t] = io[t] + fget(fo, r + 2 + 2 * d - 2) * __ldg(tb.b2 + 3 * r + d);
+      for (int d = 0; d < 3; ++d) io[t] = io[t] + fget(fo, r + 2 + 2 * d - 2) * __ldg(tb.b2 + (size_t)d * rd.nv + r);
     }
   }
   __syncthreads();

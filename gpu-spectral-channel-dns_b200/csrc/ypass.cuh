@@ -24,8 +24,8 @@ struct RhsTabs {
   const double* bkcv;  // 4 x nv: rows 4.. of B^4 C_m, m = 0, 1, N-1, N (C_m cardinal polynomial of y_m)
   const double* bkco;  // 2 x no: rows 2.. of B^2 C_m, m = 0, N
   const double* cosk;  // cos(k pi / N), k = 0..N
-  const double* b4;    // nv x 5: row r of B^4 restricted to rows 4..: weights of f_{r+4+d}, d = -4,-2,0,2,4
-  const double* b2;    // nv x 3: row r of B^2 restricted to rows 2..: weights of f_{r+2+d}, d = -2,0,2
+  const double* b4;    // 5 x nv: [d][r], row r of B^4 restricted to rows 4..: weight of f_{r+4+2d-4}
+  const double* b2;    // 3 x nv: [d][r], row r of B^2 restricted to rows 2..: weight of f_{r+2+2d-2}
 };
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
