@@ -869,29 +869,29 @@ __global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __
   }
   if (boot) return;
   __syncthreads();
-  // 4. values at the points the equations leave out (warps 0, 1) and the
-  //    K-fold integrals of fv, fo by their banded stencils (all threads)
-  if (warp < 2) {
-    const double2* f = warp ? fo : fv;
-    double2 s0 = make_double2(0.0, 0.0), sN = s0, s1 = s0, sN1 = s0;
+  // 4. values at the points the equations leave out and the K-fold
+  //    integrals of fv, fo by their banded stencils (all threads); the
+  //    values by three warps, two sums each: warp 0 fv at y = +-1, warp 2
+  //    fv at y_1, y_{N-1}, warp 1 fo at y = +-1 (omega does not use y_1,
+  //    y_{N-1})
+  if (warp < 3) {
+    const double2* f = (warp == 1) ? fo : fv;
+    const bool inner = warp == 2;
+    double2 sa = make_double2(0.0, 0.0), sb = sa;
     for (int k = lane; k < Ny; k += 32) {
       const double2 v = f[k];
-      const double cs = __ldg(tb.cosk + k);
       const double sg = (k & 1) ? -1.0 : 1.0;
-      s0 = s0 + v;
-      sN = sN + v * sg;
-      s1 = s1 + v * cs;
-      sN1 = sN1 + v * (sg * cs);
+      const double cs = inner ? __ldg(tb.cosk + k) : 1.0;
+      sa = sa + v * cs;
+      sb = sb + v * (sg * cs);
     }
-    s0 = warp_sum(s0);
-    sN = warp_sum(sN);
-    s1 = warp_sum(s1);
-    sN1 = warp_sum(sN1);
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
     if (lane == 0) {
-      red[4 * warp + 0] = s0;   // y = 1
-      red[4 * warp + 1] = s1;   // y_1
-      red[4 * warp + 2] = sN1;  // y_{N-1}
-      red[4 * warp + 3] = sN;   // y = -1
+      const int ia0 = inner ? 1 : 4 * warp;      // y = 1 or y_1
+      const int ib0 = inner ? 2 : 4 * warp + 3;  // y = -1 or y_{N-1}
+      red[ia0] = sa;
+      red[ib0] = sb;
     }
   }
   auto fget = [&](const double2* f, int k) { return (k >= 0 && k <= N) ? f[k] : make_double2(0.0, 0.0); };
