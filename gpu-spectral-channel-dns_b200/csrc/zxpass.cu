@@ -123,9 +123,11 @@ __global__ void __launch_bounds__(256, 3) k_zf(RowArr in, PencilArr out, DnsGeom
 }
 
 // Same spanwise passes with warp FFTs: a TX x TY tile of 16 lines
-// (streamwise modes x wall-normal points; both passes use 4 x 4: 32-byte
-// runs, whole sectors, on both sides), NW warps with
-// 16/NW lines each, no block barrier inside the transforms.
+// (streamwise modes x wall-normal points), NW warps with 16/NW lines each,
+// no block barrier inside the transforms.  The kernels below that read
+// through L1 (k_zbw, k_zfw) use 4 x 4 tiles: 32-byte runs, whole sectors, on
+// both sides; the tensor-staged ones (k_zbt 8 x 2, k_zft 4 x 4) are chosen
+// for their row side.
 //
 // Index arithmetic: on the pencil side a thread keeps one line (its kx and
 // y) and walks the spanwise wavenumbers kz = t/16 + 16 m; on the row side it
