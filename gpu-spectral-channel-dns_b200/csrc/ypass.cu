@@ -365,20 +365,27 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
                                            int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int Ny = M / 4 + 1;  // the launcher checks g.Ny, g.Py against M
-  // everything lives in the six line buffers: warp w's two lines hold the
-  // two vectors its transforms read (u, v | w, omega_x | omega_y, omega_z),
-  // which the first FFT pass reads before it writes the lines; the
-  // derivatives share slots with the vectors computed from them element by
-  // element (D w -> u, D^2 w -> v, D omega_z -> omega_x)
+  // everything lives in the six line buffers (two per warp): the FP64 state
+  // and derivatives (w, omega_z; D w, D^2 w, D omega_z), then the six
+  // fields in the transform's precision, ready for the even extension
+  // (c_0, c_n / 2), two in the lines of the warp that transforms them
+  // (u, v | w, omega_x | omega_y, omega_z), which its first FFT pass reads
+  // before it writes the lines
   constexpr int MW = wlen<C>(M);
   C* lines = (C*)smem_raw;
-  static_assert((size_t)2 * ((Ny * 16 + 15) / 16 * 16) <= (size_t)2 * MW * sizeof(C), "vectors do not fit the lines");
-  constexpr size_t VS = (Ny * 16 + 15) / 16;  // vector slot (double2, 16-byte multiple)
-  double2* r0 = (double2*)lines;
-  double2* r1 = (double2*)(lines + (size_t)2 * MW);
-  double2* r2 = (double2*)(lines + (size_t)4 * MW);
-  double2 *u = r0, *v = r0 + VS, *w = r1, *ox = r1 + VS, *oy = r2, *oz = r2 + VS;
-  double2 *Dw = u, *D2w = v, *Doz = ox;
+  constexpr size_t VS = (Ny * 16 + 15) / 16;             // FP64 vector slot (double2)
+  constexpr size_t FS = (Ny * sizeof(C) + 15) / 16 * 16;  // field slot (bytes)
+  static_assert(2 * VS * 16 + 2 * FS <= (size_t)2 * MW * sizeof(C), "vectors do not fit the lines");
+  unsigned char* rb0 = (unsigned char*)lines;
+  unsigned char* rb1 = (unsigned char*)(lines + (size_t)2 * MW);
+  unsigned char* rb2 = (unsigned char*)(lines + (size_t)4 * MW);
+  double2 *Dw = (double2*)rb0, *D2w = Dw + VS, *w = (double2*)rb1, *Doz = w + VS, *oz = (double2*)rb2;
+  C* fu = (C*)(rb0 + 2 * VS * 16);
+  C* fv = (C*)(rb0 + 2 * VS * 16 + FS);
+  C* fw = (C*)(rb1 + 2 * VS * 16);
+  C* fox = (C*)(rb1 + 2 * VS * 16 + FS);
+  C* foy = (C*)(rb2 + 2 * VS * 16);
+  C* foz = (C*)(rb2 + 2 * VS * 16 + FS);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
   const int kz = (int)(p / g.Kx);
@@ -419,39 +426,46 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   __syncthreads();
   for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
     const double2 wn = w[n], on = oz[n], d1 = Dw[n], dz = Doz[n];
+    double2 u, v, ox, oy;
     if (zero) {
-      u[n] = wn;
-      v[n] = on;
-      ox[n] = dz;
-      oy[n] = make_double2(-d1.x, -d1.y);
+      u = wn;
+      v = on;
+      ox = dz;
+      oy = make_double2(-d1.x, -d1.y);
     } else {
       const double2 d2 = D2w[n];
-      u[n] = muli(d1 * (ia * kmn1)) - muli(on * (ib * kmn1));
-      v[n] = muli(d1 * (ib * kmn1)) + muli(on * (ia * kmn1));
+      u = muli(d1 * (ia * kmn1)) - muli(on * (ib * kmn1));
+      v = muli(d1 * (ib * kmn1)) + muli(on * (ia * kmn1));
       const double2 du = muli(d2 * (ia * kmn1)) - muli(dz * (ib * kmn1));
       const double2 dv = muli(d2 * (ib * kmn1)) + muli(dz * (ia * kmn1));
-      ox[n] = dv - muli(wn * ib);
-      oy[n] = muli(wn * ia) - du;
+      ox = dv - muli(wn * ib);
+      oy = muli(wn * ia) - du;
     }
+    const double h = n ? 0.5 : 1.0;  // even extension: c_0, then c_n / 2
+    fu[n] = from_d2<C>(u * h);
+    fv[n] = from_d2<C>(v * h);
+    fw[n] = from_d2<C>(wn * h);
+    fox[n] = from_d2<C>(ox * h);
+    foy[n] = from_d2<C>(oy * h);
+    foz[n] = from_d2<C>(on * h);
   }
   __syncthreads();
   // this warp's two lines: fields 2 warp, 2 warp + 1; the first FFT pass
   // reads the even extensions e[0] = c_0, e[n] = e[M-n] = c_n / 2 (n < Ny),
   // zero elsewhere, the last one writes the Py values
   C* wl = lines + (size_t)2 * warp * MW;
-  const double2* s0 = (warp == 0) ? u : (warp == 1 ? w : oy);
-  const double2* s1 = (warp == 0) ? v : (warp == 1 ? ox : oz);
+  const C* s0 = (warp == 0) ? fu : (warp == 1 ? fw : foy);
+  const C* s1 = (warp == 0) ? fv : (warp == 1 ? fox : foz);
   // w (line 2) and omega_z (line 5) vanish for the mean mode
   const bool z0 = zero && warp == 1, z1 = zero && warp == 2;
   auto ld = [&](int l, int n) -> C {
-    const double2* src = l ? s1 : s0;
-    double2 e = make_double2(0.0, 0.0);
+    const C* src = l ? s1 : s0;
+    C e = cmk<C>(0.0, 0.0);
     if (!(l ? z1 : z0)) {
-      if (n == 0) e = src[0];
-      else if (n < Ny) e = src[n] * 0.5;
-      else if (n > M - Ny) e = src[M - n] * 0.5;
+      if (n < Ny) e = src[n];
+      else if (n > M - Ny) e = src[M - n];
     }
-    return from_d2<C>(e);
+    return e;
   };
   constexpr int Py = M / 2 + 1;
   C* d0 = pencil_ptr<C>(out, 2 * warp, p);
