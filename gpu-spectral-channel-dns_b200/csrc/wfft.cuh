@@ -70,6 +70,7 @@ WPLAN(384, 2, 8, 8, 8, 6)
 WPLAN(512, 2, 8, 8, 8, 8)
 WPLAN(768, 2, 8, 8, 8, 4, 3)
 WPLAN(384, 3, 8, 6, 4, 4, 4)
+WPLAN(384, 4, 8, 8, 8, 6)
 #undef WPLAN
 
 // One pass, split into the load (inputs of the lane's butterfly q, twiddled,

@@ -560,7 +560,7 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
 // warp forward-transforms two of them, and the half spectra are unpacked to
 // the output rows.
 template <typename C, int L>
-__global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
+__global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
                                           const double* __restrict__ Uy, double Ro, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     const C* stg = zw;
     auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
     auto st = [&](int l, int k, C v) { zw[(size_t)l * LW + wsw<C>(k)] = v; };
-    wfft_io<C, L, 4, true>(zw, tab.wt[2], ld, st);
+    wfft_io<C, L, 4, true>(zw, FftMaxRadix<C>::v == 8 ? tab.tw : tab.wt[2], ld, st);
   }
   __syncthreads();
   const T ro = (T)Ro;
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(96, 5) k_xw(RowArr in, RowArr out, DnsGeom g, 
     z[(size_t)5 * LW + op] = B1;
   }
   __syncthreads();
-  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, tab.wt[1]);
+  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, FftMaxRadix<C>::v == 8 ? tab.tw : tab.wt[1]);
   __syncthreads();
   // unpack: output row o = 3 rl + fl (field fl of row rl) by warp o mod 3,
   // lanes over the bins k; shared loads of a batch before its stores
@@ -889,13 +889,14 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
                            double Ro, int* status, cudaStream_t st) {
   return with_len_xz(g.Px, [&](auto LL) {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 4, FftMaxRadix<C>::v>::ok &&
-                  WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+    if constexpr (L > 0 && WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
       const long long nrows = (long long)g.Py * g.Pz;
       // four rows per CTA within one wall-normal plane; a warp's 8 staged
       // rows of 128 bins fit in its 4 lines
-      if (tab.wt[1] && tab.wt[2] && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) && in.rs >= 128 && in.rs % 2 == 0 &&
-          in.fs % 2 == 0) {
+      // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
+      const bool tw_ok = FftMaxRadix<C>::v == 8 ? tab.tw != nullptr : (tab.wt[1] && tab.wt[2]);
+      if (tw_ok && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) &&
+          in.rs >= 128 && (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0) {
         const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
         cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);

@@ -120,6 +120,6 @@ int main() {
   CASE(float2, 512, 2) CASE(float2, 768, 2) CASE(float2, 384, 3) CASE(float2, 384, 4)
   CASE(double2, 128, 1) CASE(double2, 256, 1) CASE(double2, 384, 1) CASE(double2, 512, 1) CASE(double2, 768, 1)
   CASE(double2, 128, 2) CASE(double2, 192, 2) CASE(double2, 256, 2) CASE(double2, 384, 2)
-  CASE(double2, 512, 2) CASE(double2, 768, 2) CASE(double2, 384, 3)
+  CASE(double2, 512, 2) CASE(double2, 768, 2) CASE(double2, 384, 3) CASE(double2, 384, 4)
   return 0;
 }
