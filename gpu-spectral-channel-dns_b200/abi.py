@@ -29,6 +29,7 @@ EXPORTS = [
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
+    "dns_solve_wall",
 ]
 
 
@@ -109,6 +110,7 @@ def load_library(path: str | None = None):
         "dns_rhs_nonlinear": [vp, vp, vp, vp, sz],
         "dns_solve_eq": [vp, vp, vp, i, sz],
         "dns_init_aux_matrix": [vp, vp, vp, i],
+        "dns_solve_wall": [vp, vp, vp, sz, i],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -295,6 +297,21 @@ class Context:
 
     def solve_eq(self, inv, rhs, N, tpitch):
         self._call("dns_solve_eq", C.c_void_p(inv), C.c_void_p(rhs), int(N), tpitch)
+
+    def solve_wall(self, v, omega, tpitch, where=DEVICE):
+        """solveEq of both wall-normal systems with the banded factors, in place.
+
+        Device pointers (ints) with where=DEVICE; with where=HOST, numpy
+        arrays of shape (Nz, Kx, L >= Ny) complex128, overwritten."""
+        if where == HOST:
+            for a in (v, omega):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.complex128 and a.ndim == 3
+                        and a.shape[:2] == (self.Nz, self.Kx) and a.shape[2] * 16 == tpitch
+                        and a.flags.c_contiguous):
+                    raise ValueError("host arrays must be C-contiguous (Nz, Kx, tpitch/16) complex128")
+            self._call("dns_solve_wall", v.ctypes.data, omega.ctypes.data, tpitch, HOST)
+        else:  # device pointers; 0 or None leaves that system alone
+            self._call("dns_solve_wall", C.c_void_p(v or None), C.c_void_p(omega or None), tpitch, DEVICE)
 
     def init_aux_matrix(self, inv_v, inv_o, where=DEVICE):
         if where == HOST:

@@ -373,7 +373,7 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->status};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -676,6 +676,49 @@ dns_status dns_solve_eq(dns_ctx* c, const void* inv, void* rhs, int N, size_t tp
   CK(cudaSetDevice(c->P.device));
   CK(launch_solve_eq((const double2*)inv, (double2*)rhs, (long long)(tpitch / 16), N, c->g.H, c->st));
   return DNS_OK;
+}
+
+dns_status dns_solve_wall(dns_ctx* c, void* v, void* omega, size_t tpitch, int where) {
+  if (!c || (!v && !omega)) return fail(DNS_ERR_ARG, "null argument");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
+  const DnsGeom& g = c->g;
+  const size_t row = (size_t)g.Ny * 16;
+  if (tpitch % 16 || tpitch < row) return fail(DNS_ERR_ARG, "bad tpitch");
+  CK(cudaSetDevice(c->P.device));
+  dns_status s = build_wall_solver(c);
+  if (s != DNS_OK) return s;
+  const size_t hn = (size_t)g.H * g.Ny;
+  if (!c->solve_io) CK(c->alloc(&c->solve_io, 2 * hn + 6 * (size_t)g.H));
+  double2* Xv = c->solve_io;
+  double2* Xo = Xv + hn;
+  double2* pbc = Xo + hn;
+  // a missing system is solved for a zero right-hand side and not written
+  const double2 *bv = (const double2*)v, *bo = (const double2*)omega;
+  long long bp = (long long)(tpitch / 16);
+  if (where == DNS_HOST || !v || !omega) {
+    if (v) CK(cudaMemcpy2DAsync(Xv, row, v, tpitch, row, g.H, kind_of(where, true), c->st));
+    else CK(cudaMemsetAsync(Xv, 0, hn * 16, c->st));
+    if (omega) CK(cudaMemcpy2DAsync(Xo, row, omega, tpitch, row, g.H, kind_of(where, true), c->st));
+    else CK(cudaMemsetAsync(Xo, 0, hn * 16, c->st));
+    bv = Xv;
+    bo = Xo;
+    bp = g.Ny;
+  }
+  const double* cosk = c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no;
+  CK(launch_colloc_rhs(bv, bo, bp, c->rv, c->ro, pbc, c->wd, cosk, c->Ut, c->ddUt, g, c->ph, c->st));
+  WallDims wd = c->wd;
+  wd.tilt = 0;
+  CK(launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph,
+                       c->status, c->st));
+  if (where == DNS_HOST) {
+    CK(launch_colloc_finish(Xv, Xo, pbc, Xv, Xo, g.Ny, g, c->st));
+    if (v) CK(cudaMemcpy2DAsync(v, tpitch, Xv, row, row, g.H, cudaMemcpyDeviceToHost, c->st));
+    if (omega) CK(cudaMemcpy2DAsync(omega, tpitch, Xo, row, row, g.H, cudaMemcpyDeviceToHost, c->st));
+  } else {
+    CK(launch_colloc_finish(Xv, Xo, pbc, (double2*)v, (double2*)omega, (long long)(tpitch / 16), g,
+                            c->st));
+  }
+  return check_status(c);
 }
 
 dns_status dns_init_aux_matrix(dns_ctx* c, void* inv_v, void* inv_o, int where) {

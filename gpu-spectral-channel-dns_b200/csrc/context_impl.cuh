@@ -43,6 +43,7 @@ struct dns_ctx {
   void* G6 = nullptr;
   size_t F6_bytes = 0;
   double2* scratch = nullptr;
+  double2* solve_io = nullptr;  // solve-only entry: both systems' vectors + wall polynomials
   int* status = nullptr;
   bool have_state = false, booted = false, wall_ready = false;
   cudaGraphExec_t graph = nullptr;

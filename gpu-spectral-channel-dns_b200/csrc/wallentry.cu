@@ -1,0 +1,194 @@
+// Solve-only entry of the wall-normal systems: the reference's solveEq
+// (source/solver.cpp:107-123) for the v and the omega_y system of every
+// Fourier mode, with the banded factors of wallsolve.h in place of the
+// explicit inverses (source/matrix_op.cpp:68-78).
+//
+// The right-hand sides arrive in the reference's collocation form
+// (source/coefficient.cu:7-86): for v, rows 0..3 are the wall values v(1),
+// v(-1), v'(1), v'(-1) and rows 4..N the values at the Gauss-Lobatto points
+// y_2..y_{N-2}; for omega_y and for the mean modes (pencil (0,0) of both
+// arrays) rows 0..1 are the wall values and rows 2..N the values at
+// y_1..y_{N-1}.  Per pencil:
+//   1. p = the Chebyshev polynomial of lowest degree that meets the wall rows
+//      (cubic for v, linear otherwise);
+//   2. f = the interior rows minus (A p) at their points, zero at the points
+//      the equation leaves out, and the coefficients of its interpolant
+//      (DCT-I over the Gauss-Lobatto points);
+//   3. rows K .. K+n-1 of the K-fold Chebyshev integral (K = 4 for v, 2
+//      otherwise), the input of the banded solve, which then runs without
+//      the tilting term;
+//   4. x = the banded solution + p, written over the right-hand side.
+// A p is evaluated from the operator rows of the reference's matrices:
+//   v:     Re part  (1 + k^2 dt/Re) p'' - k^2 (1 + k^2 dt/(2Re)) p   (p'''' = 0)
+//          Im part  a dt/2 U p'' - (k^2 a dt/2 U + a dt/2 U'') p
+//   omega: (1 + k^2 dt/(2Re)) p + i a dt/2 U p                       (p'' = 0)
+//   mean:  p                                                          (p'' = 0)
+// with a = kx/aphi the streamwise wavenumber and k^2 = a^2 + b^2.
+#include "kernels.cuh"
+#include "wallsolve_dev.cuh"
+
+namespace {
+
+__device__ __forceinline__ double2 cx(double a, double b) { return make_double2(a, b); }
+
+__global__ void __launch_bounds__(128) k_colloc_rhs(const double2* __restrict__ bv,
+                                                    const double2* __restrict__ bo, long long bp,
+                                                    double2* gv, double2* go, double2* pbc,
+                                                    int nv, int no, long long gp,
+                                                    const double* __restrict__ cosk,
+                                                    const double* __restrict__ Ut,
+                                                    const double* __restrict__ ddUt, DnsGeom g,
+                                                    PhysParams ph) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Ny = g.Ny, N = Ny - 1, LB = Ny + 8;
+  const long long p = blockIdx.x;
+  const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
+  const bool zero = p == 0;
+  double2* rv = (double2*)smem_raw;  // raw rows, then interpolant coefficients
+  double2* ro = rv + Ny;
+  double2* av = ro + Ny;  // integration buffers, LB each
+  double2* sv = av + LB;
+  double2* ao = sv + LB;
+  double2* so = ao + LB;
+  double* cs = (double*)(so + LB);  // cos(k pi / N), k = 0..N
+  __shared__ double2 pc[6];
+  for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
+    rv[k] = bv[p * bp + k];
+    ro[k] = bo[p * bp + k];
+    cs[k] = cosk[k];
+  }
+  __syncthreads();
+  // 1. wall polynomial: T_j(+-1) = (+-1)^j, T_j'(1) = j^2, T_j'(-1) = (-1)^(j+1) j^2
+  if (threadIdx.x == 0) {
+    const double2 e = (rv[0] + rv[1]) * 0.5, o = (rv[0] - rv[1]) * 0.5;
+    if (zero) {
+      pc[0] = e; pc[1] = o; pc[2] = cx(0, 0); pc[3] = cx(0, 0);
+    } else {
+      const double2 c2 = (rv[2] - rv[3]) * 0.125;
+      const double2 c3 = ((rv[2] + rv[3]) * 0.5 - o) * 0.125;
+      pc[0] = e - c2; pc[1] = o - c3; pc[2] = c2; pc[3] = c3;
+    }
+    pc[4] = (ro[0] + ro[1]) * 0.5;
+    pc[5] = (ro[0] - ro[1]) * 0.5;
+    for (int j = 0; j < 6; ++j) pbc[p * 6 + j] = pc[j];
+  }
+  __syncthreads();
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = ia * ia + ib * ib, dt = ph.dt, Re = ph.Re;
+  // 2. point values minus A p (zero where the equation has no row)
+  for (int m = threadIdx.x; m < LB; m += blockDim.x) {
+    double2 fv = cx(0, 0), fo = cx(0, 0);
+    if (m <= N) {
+      const double y = cs[m];
+      if (zero) {
+        if (m >= 1 && m <= N - 1) {
+          fv = rv[m + 1] - (pc[0] + pc[1] * y);
+          fo = ro[m + 1] - (pc[4] + pc[5] * y);
+        }
+      } else {
+        if (m >= 2 && m <= N - 2) {
+          const double2 P0 = pc[0] + pc[1] * y + pc[2] * (2 * y * y - 1) + pc[3] * (y * (4 * y * y - 3));
+          const double2 P2 = pc[2] * 4.0 + pc[3] * (24.0 * y);
+          const double U = Ut[m], ddU = ddUt[m];
+          const double2 re = P2 * (1 + kmn * dt / Re) - P0 * (kmn * (1 + kmn * dt * 0.5 / Re));
+          const double2 im = P2 * (ia * dt * 0.5 * U) - P0 * (kmn * ia * dt * 0.5 * U + ia * dt * 0.5 * ddU);
+          fv = rv[m + 2] - (re + muli(im));
+        }
+        if (m >= 1 && m <= N - 1) {
+          const double2 P0 = pc[4] + pc[5] * y;
+          fo = ro[m + 1] - (P0 * (1 + kmn * dt * 0.5 / Re) + muli(P0 * (ia * dt * 0.5 * Ut[m])));
+        }
+      }
+    }
+    av[m] = fv;
+    ao[m] = fo;
+  }
+  __syncthreads();
+  // interpolant: a_k = 2/(N c_k) sum_m f_m cos(k m pi/N), c_0 = c_N = 2 (f_0 = f_N = 0)
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) {
+    double2 s1 = cx(0, 0), s2 = cx(0, 0);
+    int j = 0;
+    for (int m = 1; m < N; ++m) {
+      j += k;
+      if (j >= 2 * N) j -= 2 * N;
+      const double c = cs[j <= N ? j : 2 * N - j];
+      s1 = s1 + av[m] * c;
+      s2 = s2 + ao[m] * c;
+    }
+    const double w = ((k == 0 || k == N) ? 1.0 : 2.0) / N;
+    rv[k] = s1 * w;
+    ro[k] = s2 * w;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < LB; k += blockDim.x) {
+    av[k] = k <= N ? rv[k] : cx(0, 0);
+    ao[k] = k <= N ? ro[k] : cx(0, 0);
+  }
+  __syncthreads();
+  // 3. Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  const int Kv = zero ? 2 : 4;
+  for (int it = 0; it < Kv; ++it) {
+    const int nf = (it < 2) ? 2 : 1;
+    for (int t = threadIdx.x; t < nf * LB; t += blockDim.x) {
+      const int f = t / LB;
+      const int k = t - f * LB;
+      const double2* x = f ? ao : av;
+      double2* y = f ? so : sv;
+      double2 r = cx(0, 0);
+      if (k >= 1) {
+        const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
+        const double2 xp = (k + 1 < LB) ? x[k + 1] : cx(0, 0);
+        r = (xm - xp) * (1.0 / (2.0 * k));
+      }
+      y[k] = r;
+    }
+    __syncthreads();
+    double2* tmp = av; av = sv; sv = tmp;
+    if (it < 2) { tmp = ao; ao = so; so = tmp; }
+  }
+  for (int r = threadIdx.x; r < nv; r += blockDim.x) gv[p * gp + r] = (Kv + r < LB) ? av[Kv + r] : cx(0, 0);
+  for (int r = threadIdx.x; r < no; r += blockDim.x) go[p * gp + r] = (2 + r < LB) ? ao[2 + r] : cx(0, 0);
+}
+
+// 4. x = banded solution + wall polynomial, into the caller's pencils
+__global__ void __launch_bounds__(256) k_colloc_finish(const double2* __restrict__ Xv,
+                                                       const double2* __restrict__ Xo,
+                                                       const double2* __restrict__ pbc, double2* ov,
+                                                       double2* oo, long long op, int Ny, long long H) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= H * Ny) return;
+  const long long p = i / Ny;
+  const int k = (int)(i - p * Ny);
+  double2 a = Xv[i], b = Xo[i];
+  if (k < 4) a = a + pbc[p * 6 + k];
+  if (k < 2) b = b + pbc[p * 6 + 4 + k];
+  if (ov) ov[p * op + k] = a;
+  if (oo) oo[p * op + k] = b;
+}
+
+}  // namespace
+
+size_t colloc_rhs_smem(int Ny) { return (size_t)16 * (2 * Ny + 4 * (Ny + 8)) + 8 * (size_t)Ny; }
+
+cudaError_t launch_colloc_rhs(const double2* bv, const double2* bo, long long bp, double2* gv,
+                              double2* go, double2* pbc, const WallDims& wd, const double* cosk,
+                              const double* Ut, const double* ddUt, const DnsGeom& g,
+                              const PhysParams& ph, cudaStream_t st) {
+  const size_t sm = colloc_rhs_smem(g.Ny);
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_colloc_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return e;
+  }
+  k_colloc_rhs<<<(unsigned)g.H, 128, sm, st>>>(bv, bo, bp, gv, go, pbc, wd.nv, wd.no, wd.gp, cosk, Ut,
+                                               ddUt, g, ph);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
+                                 double2* ov, double2* oo, long long op, const DnsGeom& g,
+                                 cudaStream_t st) {
+  const long long n = g.H * g.Ny;
+  k_colloc_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(Xv, Xo, pbc, ov, oo, op, g.Ny, g.H);
+  return cudaGetLastError();
+}

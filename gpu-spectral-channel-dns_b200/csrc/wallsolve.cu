@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   const bool zero = valid && slot == 0;
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-  const double kap = zero ? 0.0 : -0.5 * ib * ph.dt;  // tilting weight of this pencil
+  const double kap = (zero || !wd.tilt) ? 0.0 : -0.5 * ib * ph.dt;  // tilting weight of this pencil
   const int N = g.Ny - 1, Ny = g.Ny;
   // this lane's vector (right-hand side, intermediate solution, tilting
   // term) in the group's scratch, rows interleaved over the 32 lanes: a

@@ -11,6 +11,7 @@ struct WallDims {
   long long nslots;        // operator slots Kx * (Nz/2 + 1)
   long long ngroups;       // groups of 16 slots = CTAs
   long long group_complex; // packed factor values per group
+  int tilt = 1;            // 0: no tilting term (the solve-only entry)
 };
 
 // band instance (v lower/upper, omega lower/upper) for base-flow degree delta
@@ -21,3 +22,16 @@ size_t wall_scratch_complex(const WallDims& wd);
 cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const double2* gv,
                               const double2* go, const double* Q, double2* Sw, const WallDims& wd,
                               const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st);
+
+// Solve-only entry (wallentry.cu): collocation right-hand sides in the
+// reference's pencil layout -> integrated right-hand sides of the banded
+// systems plus the wall polynomial (6 complex per pencil); and the solution
+// plus that polynomial back into pencils of pitch op (complex).
+size_t colloc_rhs_smem(int Ny);
+cudaError_t launch_colloc_rhs(const double2* bv, const double2* bo, long long bp, double2* gv,
+                              double2* go, double2* pbc, const WallDims& wd, const double* cosk,
+                              const double* Ut, const double* ddUt, const DnsGeom& g,
+                              const PhysParams& ph, cudaStream_t st);
+cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
+                                 double2* ov, double2* oo, long long op, const DnsGeom& g,
+                                 cudaStream_t st);

@@ -207,6 +207,21 @@ dns_status dns_rhs_nonlinear(dns_ctx* ctx, void* lamb_x, void* lamb_y, const voi
 /* solveEq (source/solver.cpp:107-123): rhs <- inv * rhs for every pencil;
  * inv row-major [ky][kx][N][N] complex, rhs pitched pencils. */
 dns_status dns_solve_eq(dns_ctx* ctx, const void* inv, void* rhs, int N, size_t tpitch);
+/* solveEq (source/solver.cpp:107-123) for both wall-normal systems of every
+ * pencil, without the explicit inverses: the banded factors of the time step
+ * (built on first use) solve the reference's collocation systems
+ * (source/coefficient.cu:7-86) exactly.  v and omega hold the right-hand
+ * sides in the reference's layout ([Nz][Kx] pencils of tpitch bytes, Ny
+ * complex used: v rows 0..3 wall values v(1), v(-1), v'(1), v'(-1), rows
+ * 4..N values at y_2..y_{N-2}; omega rows 0..1 wall values, rows 2..N values
+ * at y_1..y_{N-1}; pencil (0,0) the u0 / w0 systems) and are overwritten by
+ * the Chebyshev coefficients of the solutions, as solveEq overwrites rhs.
+ * No tilting term is added (that is part of the step's right-hand side).
+ * Either pointer may be NULL: that system is not touched (the reference
+ * solves v before it forms the omega_y right-hand side).  where = DNS_HOST
+ * or DNS_DEVICE.  Synchronous; allocates its vectors (2 H Ny + 6 H complex)
+ * on first use. */
+dns_status dns_solve_wall(dns_ctx* ctx, void* v, void* omega, size_t tpitch, int where);
 /* initAuxMatrix (source/solver.cpp:260-320): explicit inverses of the v and
  * omega operators of every pencil, row-major [ky][kx][nz][nz] complex. */
 dns_status dns_init_aux_matrix(dns_ctx* ctx, void* inv_v, void* inv_omega, int where);

@@ -315,3 +315,60 @@ def test_step_mixed_close_to_fp64(pkg, case):
     assert relL2(V, hist[-1][0]) < 1e-6
     assert relL2(Om, hist[-1][1]) < 1e-6
     ctx.close()
+
+
+# The 48-run ensemble (12 runs each of 32x33x32, 64x49x64, 96x65x96 and
+# 128x97x128 modes; Re ~ U[500, 3000], Ro ~ U[0, 0.3], dt 0.002, seeded field
+# of amplitude 0.1, seeds 1000 + m; the runs are independent replicas): the
+# first member of each size, FP64 step against the oracle at every step and
+# the mixed form at the last.  Few steps: the oracle takes ~20 s a step at
+# 128x97x128.
+ENSEMBLE_SIZES = [(48, 48, 128), (96, 96, 192), (144, 144, 256), (192, 192, 384)]
+_ensemble_cache = {}
+
+
+def ensemble_member(m):
+    mx, my, mz = ENSEMBLE_SIZES[m // 12]
+    r = np.random.default_rng(1000 + m)
+    return dict(mx=mx, my=my, mz=mz, Re=float(r.uniform(500.0, 3000.0)),
+                Ro=float(r.uniform(0.0, 0.3)), dt=0.002, seed=1000 + m,
+                steps=2 if m // 12 == 3 else 3)
+
+
+def ensemble_oracle(m):
+    if m not in _ensemble_cache:
+        c = ensemble_member(m)
+        _ensemble_cache[m] = oracle_run(c["mx"], c["my"], c["mz"], c["steps"], amp=0.1,
+                                        seed=c["seed"], Re=c["Re"], Ro=c["Ro"], dt=c["dt"])
+    return _ensemble_cache[m]
+
+
+@pytest.mark.parametrize("m", [0, 12, 24, 36])
+def test_ensemble_member_fp64(pkg, m):
+    c = ensemble_member(m)
+    (V0, O0), hist, _ = ensemble_oracle(m)
+    ctx = pkg.Context(pkg.make_params(c["mx"], c["my"], c["mz"], Re=c["Re"], Ro=c["Ro"], dt=c["dt"]))
+    ctx.set_state(V0, O0)
+    ctx.bootstrap()
+    for k in range(c["steps"]):
+        ctx.step(1)
+        ctx.synchronize()
+        V, Om = ctx.get_state()
+        eV, eO = relL2(V, hist[k][0]), relL2(Om, hist[k][1])
+        assert eV < 1e-11 and eO < 1e-11, (m, k, eV, eO)
+    ctx.close()
+
+
+@pytest.mark.parametrize("m", [12, 24, 36])
+def test_ensemble_member_mixed(pkg, m):
+    c = ensemble_member(m)
+    (V0, O0), hist, _ = ensemble_oracle(m)
+    ctx = pkg.Context(pkg.make_params(c["mx"], c["my"], c["mz"], Re=c["Re"], Ro=c["Ro"], dt=c["dt"],
+                                      precision=pkg.PREC_MIXED))
+    ctx.set_state(V0, O0)
+    ctx.bootstrap()
+    ctx.step(c["steps"])
+    ctx.synchronize()
+    V, Om = ctx.get_state()
+    assert relL2(V, hist[-1][0]) < 1e-6 and relL2(Om, hist[-1][1]) < 1e-6, m
+    ctx.close()

@@ -1,0 +1,194 @@
+"""GPU: the solve-only entry dns_solve_wall against the oracle's dense systems.
+
+The reference's solveEq multiplies the collocation right-hand sides by
+explicit inverses of the matrices of source/coefficient.cu:7-86;
+dns_solve_wall solves the same systems with the banded factors of the time
+step.  Checked against numpy's dense solve of the oracle's matrices (which
+equal the reference's bit for bit): the forward error, and the normwise
+backward error ||A x - b|| / (||A||_2 ||x|| + ||b||), which must be a small
+multiple of the unit roundoff.  The residual relative to b alone is bounded
+loosely and reported: the v matrices hold fourth-derivative entries of
+order N^8, so a forward error of 1e-13 in the highest coefficients already
+leaves a residual of ~1e-10 (the reference's explicit inverses leave up to
+~3e-10 at N = 192).  Small grids: every pencil, wall
+rows non-zero, both host and device buffers.  384x193x384 modes (74 112 v /
+omega_y pairs, Ny = 193, Re 3000, dt 0.001, Couette base flow): right-hand
+side coefficients 0.9^n N(0,1) (complex, seed 3), checked on a sample of
+pencils.
+"""
+import time
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from oracle import rpcf_oracle as O  # noqa: E402
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _dense(p, sz, kx, ky):
+    """The oracle's v and omega_y collocation matrices of pencil (ky, kx)."""
+    N = sz.nz - 1
+    T0, T2, T4 = O.get_T_matrix(N)
+    U, _, ddU = O.get_U(sz.nz, p.prof)
+    ia, ib = O.ialpha_ibeta(kx, ky, sz.ny, p.n_pi_x / 2, p.n_pi_y / 2)
+    ia, ib = float(ia), float(ib)
+    kmn = ia * ia + ib * ib
+    if kx == 0 and ky == 0:
+        A = O.coef_u0(N, T0, T2, p.Re, p.dt)
+        return A, A
+    return (O.coef_v(N, U, ddU, T0, T2, T4, p.Re, p.dt, kmn, ia),
+            O.coef_omega(N, U, T0, T2, p.Re, p.dt, kmn, ia))
+
+
+def _check_pencil(Av, Ao, bv, bo, xv, xo):
+    """Forward errors against the dense solve, normwise backward errors and
+    residuals relative to b, for v and omega_y: (fv, fo, bwv, bwo, rsv, rso)."""
+    out = []
+    for A, b, x in ((Av, bv, xv), (Ao, bo, xo)):
+        ref = np.linalg.solve(A, b)
+        r = np.linalg.norm(A @ x - b)
+        out.append((np.linalg.norm(x - ref) / np.linalg.norm(ref),
+                    r / (np.linalg.norm(A, 2) * np.linalg.norm(x) + np.linalg.norm(b)),
+                    r / np.linalg.norm(b)))
+    (fv, bwv, rsv), (fo, bwo, rso) = out
+    return fv, fo, bwv, bwo, rsv, rso
+
+
+def _check_all(p, sz, pencils, bv, bo, xv, xo):
+    worst = np.zeros(6)
+    for kx, ky in pencils:
+        Av, Ao = _dense(p, sz, kx, ky)
+        e = _check_pencil(Av, Ao, bv[ky, kx], bo[ky, kx], xv[ky, kx], xo[ky, kx])
+        worst = np.maximum(worst, e)
+        fv, fo, bwv, bwo, rsv, rso = e
+        assert fv < 1e-8 and fo < 1e-11, (ky, kx, e)
+        assert bwv < 1e-14 and bwo < 1e-14, (ky, kx, e)
+        assert rsv < 1e-7 and rso < 1e-11, (ky, kx, e)
+    return worst
+
+
+def _report(worst):
+    return ("fwd v %.1e omega %.1e, backward v %.1e omega %.1e, |Ax-b|/|b| v %.1e omega %.1e"
+            % tuple(worst))
+
+
+def _solve(pkg, ctx, bv, bo, L, where):
+    sh = bv.shape
+    if where == "host":
+        hv = np.zeros(sh[:2] + (L,), dtype=np.complex128)
+        ho = np.zeros_like(hv)
+        hv[..., :sh[2]] = bv
+        ho[..., :sh[2]] = bo
+        ctx.solve_wall(hv, ho, L * 16, where=pkg.HOST)
+        return hv[..., :sh[2]], ho[..., :sh[2]]
+    tv = torch.zeros(sh[:2] + (L,), dtype=torch.complex128)
+    to = torch.zeros_like(tv)
+    tv[..., :sh[2]] = torch.from_numpy(bv)
+    to[..., :sh[2]] = torch.from_numpy(bo)
+    tv, to = tv.cuda(), to.cuda()
+    torch.cuda.synchronize()
+    ctx.solve_wall(tv.data_ptr(), to.data_ptr(), L * 16)
+    return tv.cpu().numpy()[..., :sh[2]], to.cpu().numpy()[..., :sh[2]]
+
+
+CASES = [
+    dict(mx=24, my=24, mz=32, Re=500.0, Ro=0.0, dt=0.01),
+    dict(mx=48, my=48, mz=128, Re=1300.0, Ro=0.1, dt=0.005),
+    dict(mx=36, my=48, mz=64, Re=2000.0, Ro=0.2, dt=0.002, U=(0.0, 1.0, 0.0)),
+    dict(mx=48, my=36, mz=64, Re=8400.0, Ro=0.0, dt=0.002, U=(1.0, 0.0, -1.0)),
+]
+
+
+@pytest.mark.parametrize("where", ["device", "host"])
+@pytest.mark.parametrize("case", CASES)
+def test_solve_wall_every_pencil(pkg, case, where):
+    case = dict(case)
+    U = case.pop("U", (0.5, 0.5, 0.0))
+    p = O.Params(case["mx"], case["my"], case["mz"], Re=case["Re"], Ro=case["Ro"],
+                 dt=case["dt"], prof=U)
+    sz = O.Sizes(p.mx, p.my, p.mz)
+    rng = np.random.default_rng(5)
+    shape = (sz.ny, sz.hnx, sz.nz)
+    bv = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    bo = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ctx = pkg.Context(pkg.make_params(p.mx, p.my, p.mz, Re=p.Re, Ro=p.Ro, dt=p.dt, U=U))
+    xv, xo = _solve(pkg, ctx, bv, bo, sz.mz, where)
+    ctx.close()
+    pencils = [(kx, ky) for ky in range(sz.ny) for kx in range(sz.hnx)]
+    worst = _check_all(p, sz, pencils, bv, bo, xv, xo)
+    print(f"\n{case} {where}: {_report(worst)}")
+
+
+def test_solve_wall_384x193x384(pkg):
+    """The solve-only workload: 74 112 pencil pairs at Ny = 193."""
+    p = O.Params(576, 576, 768, Re=3000.0, Ro=0.0, dt=0.001)
+    sz = O.Sizes(p.mx, p.my, p.mz)
+    assert (sz.nx, sz.nz, sz.ny, sz.hnx) == (384, 193, 384, 193)
+    rng = np.random.default_rng(3)
+    shape = (sz.ny, sz.hnx, sz.nz)
+    damp = 0.9 ** np.arange(sz.nz)
+    z = rng.standard_normal((4,) + shape)
+    bv = (z[0] + 1j * z[1]) * damp
+    bo = (z[2] + 1j * z[3]) * damp
+    del z
+    ctx = pkg.Context(pkg.make_params(p.mx, p.my, p.mz, Re=p.Re, Ro=p.Ro, dt=p.dt))
+    L = sz.nz  # unpadded pencils
+    tv = torch.from_numpy(bv).cuda()
+    to = torch.from_numpy(bo).cuda()
+    wv, wo = tv.clone(), to.clone()
+    torch.cuda.synchronize()
+    ctx.solve_wall(wv.data_ptr(), wo.data_ptr(), L * 16)  # first call: factors, buffers
+    ms = []
+    for _ in range(3):
+        wv.copy_(tv)
+        wo.copy_(to)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.solve_wall(wv.data_ptr(), wo.data_ptr(), L * 16)
+        ms.append((time.perf_counter() - t0) * 1e3)
+    xv = wv.cpu().numpy()
+    xo = wo.cpu().numpy()
+    # host buffers give the same result
+    hv, ho = bv.copy(), bo.copy()
+    ctx.solve_wall(hv, ho, L * 16, where=pkg.HOST)
+    ctx.close()
+    assert np.array_equal(hv, xv) and np.array_equal(ho, xo)
+    r = np.random.default_rng(7)
+    picks = [(0, 0), (1, 0), (0, 1), (sz.hnx - 1, 0), (0, sz.ny // 2), (3, sz.ny - 1),
+             (sz.hnx - 1, sz.ny // 2)]
+    picks += [(int(r.integers(sz.hnx)), int(r.integers(sz.ny))) for _ in range(25)]
+    worst = _check_all(p, sz, picks, bv, bo, xv, xo)
+    print(f"\n384x193x384 solve: {min(ms):.2f} ms per call (both systems, 74 112 pencils, "
+          f"synchronous); {_report(worst)}")
+
+
+def test_solve_wall_one_system(pkg):
+    """A NULL system is left alone and does not change the other's solution
+    (the reference solves v before it forms the omega_y right-hand side)."""
+    p = O.Params(48, 48, 128, Re=1300.0, Ro=0.1, dt=0.005)
+    sz = O.Sizes(p.mx, p.my, p.mz)
+    rng = np.random.default_rng(9)
+    shape = (sz.ny, sz.hnx, sz.mz)
+    bv = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    bo = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    ctx = pkg.Context(pkg.make_params(p.mx, p.my, p.mz, Re=p.Re, Ro=p.Ro, dt=p.dt))
+    xv, xo = bv.copy(), bo.copy()
+    ctx.solve_wall(xv, xo, sz.mz * 16, where=pkg.HOST)
+    tv = torch.from_numpy(bv).cuda()
+    to = torch.from_numpy(bo).cuda()
+    torch.cuda.synchronize()
+    ctx.solve_wall(tv.data_ptr(), 0, sz.mz * 16)
+    ctx.solve_wall(0, to.data_ptr(), sz.mz * 16)
+    ctx.close()
+    n = sz.nz
+    assert np.array_equal(tv.cpu().numpy()[..., :n], xv[..., :n])
+    assert np.array_equal(to.cpu().numpy()[..., :n], xo[..., :n])
+    assert np.array_equal(tv.cpu().numpy()[..., n:], bv[..., n:])  # padding untouched
