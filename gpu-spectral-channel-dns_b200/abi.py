@@ -29,7 +29,7 @@ EXPORTS = [
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
-    "dns_solve_wall",
+    "dns_solve_wall", "dns_step_many",
 ]
 
 
@@ -111,6 +111,7 @@ def load_library(path: str | None = None):
         "dns_solve_eq": [vp, vp, vp, i, sz],
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
+        "dns_step_many": [C.POINTER(vp), i, i],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -149,6 +150,16 @@ def read_parameter_file(path):
 def _ptrs(seq):
     arr = (C.c_void_p * len(seq))(*[C.c_void_p(int(x)) for x in seq])
     return arr
+
+
+def step_many(contexts, n=1):
+    """n steps of each of several independent runs, concurrently (one stream
+    per run); asynchronous like Context.step."""
+    ctxs = list(contexts)
+    if not ctxs:
+        raise ValueError("no contexts")
+    lib = ctxs[0].lib
+    _check(lib, lib.dns_step_many(_ptrs([c.h.value for c in ctxs]), len(ctxs), int(n)))
 
 
 class Context:

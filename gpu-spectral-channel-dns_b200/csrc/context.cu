@@ -503,9 +503,10 @@ dns_status dns_bootstrap(dns_ctx* c) {
   return s;
 }
 
-dns_status dns_step(dns_ctx* c, int nsteps) {
+namespace {
+// checks, factors and the captured step graph of one context
+dns_status step_ready(dns_ctx* c) {
   if (!c) return fail(DNS_ERR_ARG, "null context");
-  if (nsteps < 0) return fail(DNS_ERR_ARG, "nsteps < 0");
   if (!c->have_state || !c->booted)
     return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step");
   CK(cudaSetDevice(c->P.device));
@@ -521,7 +522,34 @@ dns_status dns_step(dns_ctx* c, int nsteps) {
     CK(cudaGraphInstantiate(&c->graph, gr, 0));
     cudaGraphDestroy(gr);
   }
+  return DNS_OK;
+}
+}  // namespace
+
+dns_status dns_step(dns_ctx* c, int nsteps) {
+  if (nsteps < 0) return fail(DNS_ERR_ARG, "nsteps < 0");
+  dns_status s = step_ready(c);
+  if (s != DNS_OK) return s;
   for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps) {
+  if (!ctxs || n < 1) return fail(DNS_ERR_ARG, "no contexts");
+  if (nsteps < 0) return fail(DNS_ERR_ARG, "nsteps < 0");
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i)
+      if (ctxs[i] == ctxs[j]) return fail(DNS_ERR_ARG, "a context is listed twice");
+    dns_status s = step_ready(ctxs[j]);
+    if (s != DNS_OK) return s;
+  }
+  // step by step across the runs, each run on its own stream: the graphs of
+  // different runs overlap on the GPU, one run's steps stay in order
+  for (int i = 0; i < nsteps; ++i)
+    for (int j = 0; j < n; ++j) {
+      CK(cudaSetDevice(ctxs[j]->P.device));
+      CK(cudaGraphLaunch(ctxs[j]->graph, ctxs[j]->st));
+    }
   return DNS_OK;
 }
 

@@ -153,6 +153,13 @@ dns_status dns_bootstrap(dns_ctx* ctx);
  * side with the tilting term, omega solve -- one CUDA graph per step, no
  * host round trip. */
 dns_status dns_step(dns_ctx* ctx, int nsteps);
+/* No counterpart in the reference.  nsteps steps of each of n independent
+ * runs (an ensemble: any grids, parameters and precisions), issued step by
+ * step across the runs, each on its own context stream, so that the step
+ * graphs of different runs execute concurrently and small grids share the
+ * GPU.  Asynchronous like dns_step: synchronise each context (or the device)
+ * before reading results.  A context may appear once. */
+dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps);
 
 /* The same steps without the graph, with CUDA events recorded around each
  * of the DNS_NUM_KERNELS kernels of a step on the context stream;

@@ -372,3 +372,42 @@ def test_ensemble_member_mixed(pkg, m):
     V, Om = ctx.get_state()
     assert relL2(V, hist[-1][0]) < 1e-6 and relL2(Om, hist[-1][1]) < 1e-6, m
     ctx.close()
+
+
+def test_step_many_equals_one_by_one(pkg):
+    """Concurrent stepping of independent runs (one stream each) gives every
+    run exactly the state it reaches alone: one member of each ensemble size,
+    both precisions."""
+    runs = []
+    for m in (0, 12, 24, 36):
+        c = ensemble_member(m)
+        for prec in (pkg.PREC_MIXED, pkg.PREC_FP64):
+            Nx, Nz, Ny = c["mx"] // 3 * 2, c["my"] // 3 * 2, c["mz"] // 4 + 1
+            V0, O0 = pkg.seeded_state(Nx, Ny, Nz, 4.0, 2.0, 0.1, c["seed"])
+            runs.append((c, prec, V0, O0))
+
+    def make(c, prec, V0, O0):
+        ctx = pkg.Context(pkg.make_params(c["mx"], c["my"], c["mz"], Re=c["Re"], Ro=c["Ro"],
+                                          dt=c["dt"], precision=prec))
+        ctx.set_state(V0, O0)
+        ctx.bootstrap()
+        return ctx
+
+    alone = []
+    for r in runs:
+        ctx = make(*r)
+        ctx.step(4)
+        ctx.synchronize()
+        alone.append(ctx.get_state())
+        ctx.close()
+    ctxs = [make(*r) for r in runs]
+    pkg.step_many(ctxs, 4)
+    for ctx, (Va, Oa) in zip(ctxs, alone):
+        ctx.synchronize()
+        V, Om = ctx.get_state()
+        assert np.array_equal(V, Va) and np.array_equal(Om, Oa)
+        ctx.close()
+    dup = make(*runs[0])
+    with pytest.raises(pkg.DnsError):
+        pkg.step_many([dup, dup], 1)
+    dup.close()
