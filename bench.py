@@ -459,6 +459,49 @@ def run_ensemble(args):
     }
 
 
+def run_solve(args):
+    """The solve-only workload: both wall-normal systems of every pencil
+    (dns_solve_wall, the banded factors of the step), Re 3000, dt 0.001,
+    Couette base flow, right-hand sides 0.9^n N(0,1) (complex, seed 3) on
+    the device; CUDA events on the library's stream around each call."""
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    torch.cuda.set_device(0)
+    mx, my, mz = (int(v) for v in args.solve_grid.split(","))
+    ctx = pkg.Context(pkg.make_params(mx, my, mz, Re=3000.0, Ro=0.0, dt=0.001))
+    Nz, Kx, Ny = ctx.Nz, ctx.Kx, ctx.Ny
+    rng = np.random.default_rng(3)
+    damp = 0.9 ** np.arange(Ny)
+    z = rng.standard_normal((4, Nz, Kx, Ny))
+    bv = torch.from_numpy((z[0] + 1j * z[1]) * damp).cuda()
+    bo = torch.from_numpy((z[2] + 1j * z[3]) * damp).cuda()
+    del z
+    wv, wo = bv.clone(), bo.clone()
+    s = torch.cuda.ExternalStream(ctx.stream)
+    ms = []
+    for i in range(args.warmup + args.steps):
+        wv.copy_(bv)
+        wo.copy_(bo)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.solve_wall(wv.data_ptr(), wo.data_ptr(), Ny * 16)  # the first call also builds the factors
+        e1.record(s)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    ctx.close()
+    t = float(np.median(ms))
+    H = Kx * Nz
+    return {"metric": f"wall-normal solves (v and omega_y pairs) per second at {Kx * 2 - 2}x{Ny}x{Nz} modes",
+            "value": round(H / (t * 1e-3), 1), "unit": "pairs/s", "ms_per_call": round(t, 4),
+            "pairs": H, "Ny": Ny, "steps": args.steps, "warmup": args.warmup,
+            "rhs_and_solution_bytes": 4 * H * Ny * 16,
+            "timing": "CUDA events on the library stream around each synchronous call, median"}
+
+
 def measured_traffic(kernel, config, prec):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
     of one ncu capture, from the committed summary profiles/dram_traffic.json
@@ -493,6 +536,10 @@ def main():
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="run one precision only (bootstrap + warm-up + timed steps), for "
                          "profiling captures; prints per-kernel times, not the bench line")
+    ap.add_argument("--solve", action="store_true",
+                    help="the solve-only workload (dns_solve_wall): prints its own line")
+    ap.add_argument("--solve-grid", default="576,576,768",
+                    help="mx,my,mz of --solve (default 384x193x384 modes)")
     ap.add_argument("--ensemble", action="store_true",
                     help="the 48-run ensemble (concurrent runs, one GPU): prints its own line")
     args = ap.parse_args()
@@ -516,6 +563,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.only:
         print(json.dumps(run_one(args)))
+        return
+    if args.solve:
+        if rank == 0:
+            print(json.dumps(run_solve(args)))
         return
     if args.ensemble:
         if rank == 0:
