@@ -502,6 +502,27 @@ def run_solve(args):
             "timing": "CUDA events on the library stream around each synchronous call, median"}
 
 
+def other_workloads(args):
+    """The solve-only workload (384x193x384) and the 48-run ensemble, each
+    with its own metric (not the headline); a failure is reported, not
+    raised, so the headline line is always printed."""
+    import copy
+    res = {}
+    for name, fn, steps, keys in (
+            ("solve_384x193x384", run_solve, 5, ("metric", "value", "unit", "ms_per_call", "pairs", "timing")),
+            ("ensemble_48_runs", run_ensemble, 10, ("metric", "value", "unit", "steps", "ms_all_runs_K_steps",
+                                                    "one_after_another", "max_rel_l2_err_vs_own_fp64_run",
+                                                    "clocks"))):
+        a = copy.copy(args)
+        a.steps, a.warmup, a.solve_grid = steps, 3, "576,576,768"
+        try:
+            r = fn(a)
+            res[name] = {k: r[k] for k in keys}
+        except Exception as e:  # noqa: BLE001
+            res[name] = {"error": f"{type(e).__name__}: {e}"}
+    return res
+
+
 def measured_traffic(kernel, config, prec):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
     of one ncu capture, from the committed summary profiles/dram_traffic.json
@@ -532,6 +553,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the solve-only and ensemble workloads appended to the line")
     ap.add_argument("--config", default="256x129x256", choices=sorted(CONFIGS))
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="run one precision only (bootstrap + warm-up + timed steps), for "
@@ -626,6 +649,8 @@ def main():
             "setup_seconds": round(r["setup_s"], 2),
             "device_bytes": r["mem"],
         }
+        if world == 1 and args.config == "256x129x256" and not args.no_extras:
+            out["other_workloads"] = other_workloads(args)
         print(json.dumps(out))
     if world > 1:
         import torch
