@@ -62,3 +62,34 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
                         "--gpus", "2"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_ensemble_members_match_the_parity_tests():
+    """bench.py's 48-run ensemble draws the same grids, Re, Ro and seeds as
+    the ensemble parity tests (run m: default_rng(1000 + m))."""
+    b = _bench()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    mem = b.ensemble_members()
+    assert len(mem) == 48
+    for m in (0, 12, 24, 36, 47):
+        c = mem[m]
+        mx, my, mz = b.ENSEMBLE_SIZES[m // 12]
+        r = np.random.default_rng(1000 + m)
+        assert (c["mx"], c["my"], c["mz"], c["seed"], c["dt"]) == (mx, my, mz, 1000 + m, 0.002)
+        assert c["Re"] == r.uniform(500.0, 3000.0) and c["Ro"] == r.uniform(0.0, 0.3)
+
+
+def test_other_workloads_report_failures(monkeypatch):
+    """A failing extra workload leaves an error entry instead of losing the
+    headline line."""
+    b = _bench()
+
+    def boom(args):
+        raise RuntimeError("no device")
+    monkeypatch.setattr(b, "run_solve", boom)
+    monkeypatch.setattr(b, "run_ensemble", boom)
+    import argparse
+    res = b.other_workloads(argparse.Namespace(steps=5, warmup=3, solve_grid="576,576,768"))
+    assert res == {"solve_384x193x384": {"error": "RuntimeError: no device"},
+                   "ensemble_48_runs": {"error": "RuntimeError: no device"}}
