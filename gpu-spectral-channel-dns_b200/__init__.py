@@ -7,6 +7,6 @@ the CUDA library; this package only moves buffers and parameters.
 from .abi import (  # noqa: F401
     BACKWARD, DEVICE, FORWARD, HOST, NO_PADDING, PADDING, PREC_FP64, PREC_MIXED,
     Context, DnsError, DnsParams, EXPORTS, LIB_PATH, load_library, make_params,
-    read_parameter_file, step_many,
+    read_parameter_file, step_many, SLAB_PENCILS, SLAB_PLANES, slab_ranges, slab_segments,
 )
 from .seed import seeded_state  # noqa: F401

@@ -29,8 +29,15 @@ EXPORTS = [
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
-    "dns_solve_wall", "dns_step_many",
+    "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments",
 ]
+
+SLAB_PENCILS, SLAB_PLANES = 0, 1
+
+
+class SlabSegment(C.Structure):
+    _fields_ = [("peer", C.c_int), ("kz0", C.c_int), ("nkz", C.c_int), ("local_row0", C.c_int),
+                ("y0", C.c_int), ("ny", C.c_int)]
 
 
 class DnsParams(C.Structure):
@@ -112,6 +119,8 @@ def load_library(path: str | None = None):
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
         "dns_step_many": [C.POINTER(vp), i, i],
+        "dns_slab_ranges": [i, i, i, i, i, C.POINTER(C.c_int)],
+        "dns_slab_segments": [i, i, i, i, i, i, C.POINTER(SlabSegment), i, C.POINTER(C.c_int)],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -150,6 +159,24 @@ def read_parameter_file(path):
 def _ptrs(seq):
     arr = (C.c_void_p * len(seq))(*[C.c_void_p(int(x)) for x in seq])
     return arr
+
+
+def slab_ranges(mx, my, mz, nranks, rank):
+    """(slot0, slot1, y0, y1, pencils) of one rank of a slab decomposition."""
+    lib = load_library()
+    out = (C.c_int * 5)()
+    _check(lib, lib.dns_slab_ranges(mx, my, mz, nranks, rank, out))
+    return tuple(out)
+
+
+def slab_segments(mx, my, mz, nranks, rank, role):
+    """The exchange segments of one rank as dicts (peer, kz0, nkz, local_row0, y0, ny)."""
+    lib = load_library()
+    n = C.c_int()
+    _check(lib, lib.dns_slab_segments(mx, my, mz, nranks, rank, role, None, 0, C.byref(n)))
+    arr = (SlabSegment * max(n.value, 1))()
+    _check(lib, lib.dns_slab_segments(mx, my, mz, nranks, rank, role, arr, n.value, C.byref(n)))
+    return [{f: getattr(arr[k], f) for f, _ in SlabSegment._fields_} for k in range(n.value)]
 
 
 def step_many(contexts, n=1):

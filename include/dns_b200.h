@@ -233,6 +233,30 @@ dns_status dns_solve_wall(dns_ctx* ctx, void* v, void* omega, size_t tpitch, int
  * omega operators of every pencil, row-major [ky][kx][nz][nz] complex. */
 dns_status dns_init_aux_matrix(dns_ctx* ctx, void* inv_v, void* inv_omega, int where);
 
+/* ---- slab decomposition plan (host only, no device work) --------------
+ * No counterpart in the reference.  For R ranks: rank r owns the operator
+ * slots kz' in [slot0, slot1) with both pencils kz' and Nz - kz' of each
+ * (the per-pencil passes and the solve) and the wall-normal planes
+ * [y0, y1) of the Py physical planes (the spanwise and streamwise passes).
+ * out = {slot0, slot1, y0, y1, pencils owned}. */
+dns_status dns_slab_ranges(int mx, int my, int mz, int nranks, int rank, int out[5]);
+enum { DNS_SLAB_PENCILS = 0, DNS_SLAB_PLANES = 1 };
+/* One block of an exchange: pencils p = kz * Kx + kx for kz in
+ * [kz0, kz0 + nkz) and all kx (rows local_row0 .. of the pencil owner's
+ * local buffer, which holds its runs in increasing kz), times the planes
+ * [y0, y0 + ny) of the plane owner.  peer = the other rank. */
+typedef struct {
+  int peer, kz0, nkz, local_row0, y0, ny;
+} dns_slab_segment;
+/* The segments of this rank in role DNS_SLAB_PENCILS (its pencils, one
+ * list per plane owner) or DNS_SLAB_PLANES (its planes, one list per pencil
+ * owner), ordered by peer, then by kz: the backward exchange after the
+ * first wall-normal pass sends each field's segments pencil owner -> plane
+ * owner in that order, the forward exchange after the spanwise forward pass
+ * sends them back.  seg may be NULL to get the count. */
+dns_status dns_slab_segments(int mx, int my, int mz, int nranks, int rank, int role,
+                             dns_slab_segment* seg, int cap, int* count);
+
 #ifdef __cplusplus
 }
 #endif
