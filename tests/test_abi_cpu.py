@@ -39,6 +39,10 @@ def test_argument_errors_without_gpu(pkg):
     assert b"mz" in lib.dns_last_error()
     p = pkg.make_params(50, 48, 128)  # mx = 50 is not 2^a 3^b
     assert lib.dns_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    # solve-only and ensemble entries reject missing arguments before any device work
+    assert lib.dns_solve_wall(None, None, None, 16, 0) == 1
+    assert lib.dns_step_many(None, 0, 1) == 1
+    assert b"no contexts" in lib.dns_last_error()
 
 
 def test_parameter_file(pkg, tmp_path):
