@@ -6,7 +6,10 @@ of the two exchanges of a step.  Checked here on the CPU: every (pencil,
 plane) pair travels exactly once, both ends list the same segments in the
 same order, and a backward (6 fields) plus forward (3 fields) exchange
 executed from the plan over gloo all_to_all with two and three ranks
-reproduces the global arrays.  The device step does not use the plan yet.
+reproduces the global arrays, and the oracle's nonlinear phase run
+decomposed by the plan (wall-normal transforms on each rank's pencils,
+spanwise/streamwise transforms and the Lamb vector on its planes) equals the
+undecomposed one.  The device step does not use the plan yet.
 """
 import datetime
 import os
@@ -72,76 +75,158 @@ def test_plan_rejects_bad_arguments():
         pkg.slab_segments(48, 48, 130, 2, 0, pkg.SLAB_PENCILS)
 
 
-def _exchange(pkg, grid, R, r, G, dist, torch):
-    """Backward then forward exchange of rank r, executed from the plan."""
+def _a2a(dist, torch, send_parts, recv_sizes):
+    sb = torch.from_numpy(np.concatenate([np.ravel(x) for x in send_parts]))
+    rb = torch.empty(sum(recv_sizes), dtype=sb.dtype)
+    dist.all_to_all_single(rb, sb, output_split_sizes=recv_sizes,
+                           input_split_sizes=[int(np.size(x)) for x in send_parts])
+    return rb.numpy()
+
+
+def pencils_to_planes(pkg, grid, R, r, loc, dist, torch):
+    """Backward exchange executed from the plan: loc[f][local pencil][Py]
+    -> planes[f][pencil][ny of this rank]."""
     Kx, Nz, Py = _geom(*grid)
     pen = pkg.slab_segments(*grid, R, r, pkg.SLAB_PENCILS)
     pla = pkg.slab_segments(*grid, R, r, pkg.SLAB_PLANES)
-    s0, s1, y0, y1, npen = pkg.slab_ranges(*grid, R, r)
-    # local pencil buffer [f][local pencil][Py], runs in increasing kz
-    runs = sorted({(g["kz0"], g["nkz"], g["local_row0"]) for g in pen})
-    loc = np.zeros((6, npen, Py))
-    for kz0, nkz, row0 in runs:
-        loc[:, row0:row0 + nkz * Kx] = G[:, kz0 * Kx:(kz0 + nkz) * Kx]
-
-    def a2a(send_parts, recv_sizes):
-        sb = torch.from_numpy(np.concatenate([p.ravel() for p in send_parts]))
-        rb = torch.empty(sum(recv_sizes), dtype=torch.float64)
-        dist.all_to_all_single(rb, sb, output_split_sizes=recv_sizes,
-                               input_split_sizes=[p.size for p in send_parts])
-        return rb.numpy()
-
-    # backward: pencils -> planes, 6 fields
-    nf = 6
+    nf = loc.shape[0]
     send = []
     for s in range(R):
         blocks = [loc[f, g["local_row0"]:g["local_row0"] + g["nkz"] * Kx, g["y0"]:g["y0"] + g["ny"]]
                   for f in range(nf) for g in pen if g["peer"] == s]
-        send.append(np.concatenate([b.ravel() for b in blocks]) if blocks else np.zeros(0))
+        send.append(np.concatenate([x.ravel() for x in blocks]) if blocks else np.zeros(0, loc.dtype))
     rsz = [nf * sum(g["nkz"] * Kx * g["ny"] for g in pla if g["peer"] == s) for s in range(R)]
-    buf = a2a(send, rsz)
-    ny = y1 - y0
-    planes = np.full((6, Kx * Nz, ny), np.nan)
+    buf = _a2a(dist, torch, send, rsz)
+    _, _, y0, y1, _ = pkg.slab_ranges(*grid, R, r)
+    planes = np.full((nf, Kx * Nz, y1 - y0), np.nan, dtype=loc.dtype)
     off = 0
     for s in range(R):
         for f in range(nf):
             for g in (g for g in pla if g["peer"] == s):
                 n = g["nkz"] * Kx * g["ny"]
-                planes[f, g["kz0"] * Kx:(g["kz0"] + g["nkz"]) * Kx, :] = buf[off:off + n].reshape(-1, ny)
+                planes[f, g["kz0"] * Kx:(g["kz0"] + g["nkz"]) * Kx] = buf[off:off + n].reshape(-1, y1 - y0)
                 off += n
     assert off == buf.size
-    assert np.array_equal(planes, G[:, :, y0:y1])
-    # forward: planes -> pencils, 3 fields (the spanwise pass's output)
-    nf = 3
+    return planes
+
+
+def planes_to_pencils(pkg, grid, R, r, planes, dist, torch):
+    """Forward exchange executed from the plan: planes[f][pencil][ny] ->
+    loc[f][local pencil][Py]."""
+    Kx, Nz, Py = _geom(*grid)
+    pen = pkg.slab_segments(*grid, R, r, pkg.SLAB_PENCILS)
+    pla = pkg.slab_segments(*grid, R, r, pkg.SLAB_PLANES)
+    nf = planes.shape[0]
     send = []
     for s in range(R):
-        blocks = [planes[f, g["kz0"] * Kx:(g["kz0"] + g["nkz"]) * Kx, :]
+        blocks = [planes[f, g["kz0"] * Kx:(g["kz0"] + g["nkz"]) * Kx]
                   for f in range(nf) for g in pla if g["peer"] == s]
-        send.append(np.concatenate([b.ravel() for b in blocks]) if blocks else np.zeros(0))
+        send.append(np.concatenate([x.ravel() for x in blocks]) if blocks else np.zeros(0, planes.dtype))
     rsz = [nf * sum(g["nkz"] * Kx * g["ny"] for g in pen if g["peer"] == s) for s in range(R)]
-    buf = a2a(send, rsz)
-    back = np.full((3, npen, Py), np.nan)
+    buf = _a2a(dist, torch, send, rsz)
+    npen = pkg.slab_ranges(*grid, R, r)[4]
+    loc = np.full((nf, npen, Py), np.nan, dtype=planes.dtype)
     off = 0
     for s in range(R):
         for f in range(nf):
             for g in (g for g in pen if g["peer"] == s):
                 n = g["nkz"] * Kx * g["ny"]
-                back[f, g["local_row0"]:g["local_row0"] + g["nkz"] * Kx, g["y0"]:g["y0"] + g["ny"]] = \
+                loc[f, g["local_row0"]:g["local_row0"] + g["nkz"] * Kx, g["y0"]:g["y0"] + g["ny"]] = \
                     buf[off:off + n].reshape(-1, g["ny"])
                 off += n
+    assert off == buf.size
+    return loc
+
+
+def local_pencils(pkg, grid, R, r):
+    """Global pencil indices of rank r's local buffer rows, in order."""
+    Kx = _geom(*grid)[0]
+    runs = sorted({(g["kz0"], g["nkz"], g["local_row0"])
+                   for g in pkg.slab_segments(*grid, R, r, pkg.SLAB_PENCILS)}, key=lambda t: t[2])
+    return np.concatenate([np.arange(kz0 * Kx, (kz0 + nkz) * Kx) for kz0, nkz, _ in runs])
+
+
+def _exchange(pkg, grid, R, r, G, dist, torch):
+    """Backward then forward exchange of rank r, executed from the plan."""
+    rows = local_pencils(pkg, grid, R, r)
+    loc = G[:, rows]
+    y0, y1 = pkg.slab_ranges(*grid, R, r)[2:4]
+    planes = pencils_to_planes(pkg, grid, R, r, loc, dist, torch)
+    assert np.array_equal(planes, G[:, :, y0:y1])
+    back = planes_to_pencils(pkg, grid, R, r, planes[:3], dist, torch)
     assert np.array_equal(back, loc[:3])
 
 
-def _worker(rank, world, port, grid, q):
+def decomposed_nonlinear(pkg, pb, R, r, dist, torch):
+    """The oracle's nonlinear phase run as the slab decomposition would run
+    the step: wall-normal transforms on this rank's pencils only, the
+    spanwise/streamwise transforms and the Lamb vector on its planes only
+    (other planes zero), data moved between the two by the plan's exchanges.
+    Returns (rows, Nv, No) for this rank's pencils."""
+    from oracle import rpcf_oracle as O
+    sz, p = pb.sz, pb.p
+    grid = (sz.mx, sz.my, sz.mz)
+    rows = local_pencils(pkg, grid, R, r)
+    H = sz.ny * sz.hnx
+    fields = pb.spectral_fields()
+    loc = np.zeros((6, rows.size, sz.pz), dtype=np.complex128)
+    for f, F in enumerate(fields):
+        S = np.zeros((rows.size, sz.mz), dtype=np.complex128)
+        S[:, :sz.nz] = F.reshape(H, sz.nz)[rows]
+        loc[f] = O.cheby_s2p(S, sz.mz, pad=True)[:, :sz.pz]
+    planes = pencils_to_planes(pkg, grid, R, r, loc, dist, torch)
+    y0, y1 = pkg.slab_ranges(*grid, R, r)[2:4]
+    phys = []
+    for f in range(6):
+        S = np.zeros((sz.ny, sz.hnx, sz.mz), dtype=np.complex128)
+        S[:, :, y0:y1] = planes[f].reshape(sz.ny, sz.hnx, y1 - y0)
+        C = O.set_zeros(O.transpose_backward(S, sz), sz)
+        phys.append(O.c2r_2d(C, sz))
+    lx, ly, lz = O.lamb(*phys, sz, p.Ro, p.prof)
+    out = np.zeros((3, H, y1 - y0), dtype=np.complex128)
+    for f, L in enumerate((lx, ly, lz)):
+        S = O.transpose_forward(O.r2c_2d(L, sz), sz)
+        out[f] = S[:, :, y0:y1].reshape(H, y1 - y0)
+    back = planes_to_pencils(pkg, grid, R, r, out, dist, torch)
+    tl = []
+    for f in range(3):
+        S = np.zeros((rows.size, sz.mz), dtype=np.complex128)
+        S[:, :sz.pz] = back[f]
+        T = np.zeros((H, sz.mz), dtype=np.complex128)
+        T[rows] = O.cheby_p2s(S, sz.mz, pad=True)
+        tl.append(T.reshape(sz.ny, sz.hnx, sz.mz))
+    hv, ho = O.rhs_nonlinear(*tl, sz, pb.aphi, pb.beta)
+    res = []
+    for h in (hv, ho):
+        Hh = np.zeros((rows.size, sz.mz), dtype=np.complex128)
+        Hh[:, :sz.nz] = h.reshape(H, sz.nz)[rows]
+        res.append(O.cheby_s2p(Hh, sz.mz, pad=False)[:, :sz.nz])
+    return rows, res[0], res[1]
+
+
+def _worker(rank, world, port, grid, q, mode="exchange"):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import torch
     import torch.distributed as dist
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         pkg = load_package()
-        Kx, Nz, Py = _geom(*grid)
-        G = np.random.default_rng(5).standard_normal((6, Kx * Nz, Py))
-        _exchange(pkg, grid, world, rank, G, dist, torch)
+        if mode == "exchange":
+            Kx, Nz, Py = _geom(*grid)
+            G = np.random.default_rng(5).standard_normal((6, Kx * Nz, Py))
+            _exchange(pkg, grid, world, rank, G, dist, torch)
+        else:
+            from oracle import rpcf_oracle as O
+            pb = O.Problem(O.Params(*grid, Re=1300.0, Ro=0.1, dt=0.005))
+            sz = pb.sz
+            V0, O0 = pkg.seeded_state(sz.nx, sz.nz, sz.ny, 4.0, 2.0, 0.05, 0)
+            pb.set_state(V0, O0)
+            rows, Nv, No = decomposed_nonlinear(pkg, pb, world, rank, dist, torch)
+            Nv_ref, No_ref = pb.nonlinear()
+            H = sz.ny * sz.hnx
+            ev = np.max(np.abs(Nv - Nv_ref.reshape(H, -1)[rows])) / np.max(np.abs(Nv_ref))
+            eo = np.max(np.abs(No - No_ref.reshape(H, -1)[rows])) / np.max(np.abs(No_ref))
+            assert ev < 1e-13 and eo < 1e-13, (ev, eo)
         q.put((rank, "ok"))
     except Exception as e:  # noqa: BLE001
         q.put((rank, repr(e)))
@@ -155,16 +240,28 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world,grid", [(2, (48, 48, 128)), (3, (24, 36, 64))])
-def test_exchange_round_trip_gloo(world, grid):
+def _spawn(world, grid, mode):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, grid, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, grid, q, mode)) for r in range(world)]
     for p in procs:
         p.start()
-    res = dict(q.get(timeout=120) for _ in range(world))
+    res = dict(q.get(timeout=180) for _ in range(world))
     for p in procs:
         p.join(timeout=60)
     assert res == {r: "ok" for r in range(world)}
+
+
+@pytest.mark.parametrize("world,grid", [(2, (48, 48, 128)), (3, (24, 36, 64))])
+def test_exchange_round_trip_gloo(world, grid):
+    _spawn(world, grid, "exchange")
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_decomposed_nonlinear_matches_oracle_gloo(world):
+    """The nonlinear phase decomposed by the plan (pencil passes on the
+    rank's pencils, plane passes on its planes, the two exchanges between)
+    equals the undecomposed oracle on every rank's pencils."""
+    _spawn(world, (48, 48, 128), "nonlinear")
