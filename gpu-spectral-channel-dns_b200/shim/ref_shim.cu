@@ -133,14 +133,12 @@ int initAuxMatrix(problem& pb, bool inversed) {
 int nextStep(problem& pb) {
   check(dns_step(g_ctx, 1));
   check(dns_get_state(g_ctx, pb.rhs_v, pb.rhs_omega_y, pb.tPitch, DNS_HOST));
-  pb.currenStep++;
-  return 0;
+  return 0;  // the caller's loop advances pb.currenStep, as in the reference
 }
 
 // source/RPCFKernels.cu:358
 __host__ int initFlow(problem& pb) {
-  check(dns_init_flow(g_ctx));
-  check(dns_bootstrap(g_ctx));
+  check(dns_init_flow(g_ctx));  // state only; dns_bootstrap replaces the extra previous step
   check(dns_get_state(g_ctx, pb.rhs_v, pb.rhs_omega_y, pb.tPitch, DNS_HOST));
   return 0;
 }
