@@ -15,6 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdnsb200.so")
+DRIVER_SRC = os.path.join(HERE, "driver", "dns_run.cpp")
+DRIVER = os.path.join(HERE, "dns_run")
 BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -40,8 +42,24 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_driver(force: bool = False) -> str:
+    """The parameter.txt driver executable, linked against the library."""
+    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(
+            os.path.getmtime(DRIVER_SRC), os.path.getmtime(LIB)):
+        return DRIVER
+    cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-o", DRIVER + ".tmp", DRIVER_SRC, "-L", HERE, "-ldnsb200",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stderr}")
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
+        build_driver()
         return LIB
     nvcc = _nvcc()
     os.makedirs(BUILD, exist_ok=True)
@@ -65,6 +83,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_driver(force=True)
     return LIB
 
 
