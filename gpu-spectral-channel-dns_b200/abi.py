@@ -29,7 +29,7 @@ EXPORTS = [
     "dns_cheby_p2s", "dns_get_uvw", "dns_compute_lamb", "dns_rhs_nonlinear", "dns_solve_eq",
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
-    "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments",
+    "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
 ]
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1
@@ -119,6 +119,7 @@ def load_library(path: str | None = None):
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
         "dns_step_many": [C.POINTER(vp), i, i],
+        "dns_check_state": [vp],
         "dns_slab_ranges": [i, i, i, i, i, C.POINTER(C.c_int)],
         "dns_slab_segments": [i, i, i, i, i, i, C.POINTER(SlabSegment), i, C.POINTER(C.c_int)],
     }
@@ -291,6 +292,10 @@ class Context:
 
     def bootstrap(self):
         self._call("dns_bootstrap")
+
+    def check_state(self):
+        """Raise DnsError (DNS_ERR_NONFINITE) if the state holds NaN or Inf."""
+        self._call("dns_check_state")
 
     def step(self, n=1):
         self._call("dns_step", int(n))

@@ -373,7 +373,7 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->probe, c->status};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -703,6 +703,20 @@ dns_status dns_solve_eq(dns_ctx* c, const void* inv, void* rhs, int N, size_t tp
   if (N < 1 || N > 4096 || tpitch % 16 || tpitch < (size_t)N * 16) return fail(DNS_ERR_ARG, "bad N or tpitch");
   CK(cudaSetDevice(c->P.device));
   CK(launch_solve_eq((const double2*)inv, (double2*)rhs, (long long)(tpitch / 16), N, c->g.H, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_check_state(dns_ctx* c) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  if (!c->have_state) return fail(DNS_ERR_STATE, "no state to check");
+  CK(cudaSetDevice(c->P.device));
+  if (!c->probe) CK(c->alloc(&c->probe, 1));
+  CK(cudaMemsetAsync(c->probe, 0, sizeof(int), c->st));
+  CK(launch_nonfinite(c->V, c->O, c->g.H * c->g.Ny, c->probe, c->st));
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->probe, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (bad) return fail(DNS_ERR_NONFINITE, "the state holds NaN or Inf");
   return DNS_OK;
 }
 

@@ -44,6 +44,7 @@ struct dns_ctx {
   size_t F6_bytes = 0;
   double2* scratch = nullptr;
   double2* solve_io = nullptr;  // solve-only entry: both systems' vectors + wall polynomials
+  int* probe = nullptr;         // dns_check_state: set when the state holds NaN or Inf
   int* status = nullptr;
   bool have_state = false, booted = false, wall_ready = false;
   cudaGraphExec_t graph = nullptr;

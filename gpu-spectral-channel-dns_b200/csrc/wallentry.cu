@@ -24,6 +24,8 @@
 //   omega: (1 + k^2 dt/(2Re)) p + i a dt/2 U p                       (p'' = 0)
 //   mean:  p                                                          (p'' = 0)
 // with a = kx/aphi the streamwise wavenumber and k^2 = a^2 + b^2.
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "wallsolve_dev.cuh"
 
@@ -167,7 +169,27 @@ __global__ void __launch_bounds__(256) k_colloc_finish(const double2* __restrict
   if (oo) oo[p * op + k] = b;
 }
 
+// any non-finite real or imaginary part in a or b sets *flag
+__global__ void __launch_bounds__(256) k_nonfinite(const double2* __restrict__ a,
+                                                   const double2* __restrict__ b, long long n,
+                                                   int* flag) {
+  bool bad = false;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 x = a[i], y = b[i];
+    bad |= !(isfinite(x.x) && isfinite(x.y) && isfinite(y.x) && isfinite(y.y));
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
 }  // namespace
+
+cudaError_t launch_nonfinite(const double2* a, const double2* b, long long n, int* flag,
+                             cudaStream_t st) {
+  const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 8);
+  k_nonfinite<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, st>>>(a, b, n, flag);
+  return cudaGetLastError();
+}
 
 size_t colloc_rhs_smem(int Ny) { return (size_t)16 * (2 * Ny + 4 * (Ny + 8)) + 8 * (size_t)Ny; }
 

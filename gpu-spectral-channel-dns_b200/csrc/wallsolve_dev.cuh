@@ -35,3 +35,6 @@ cudaError_t launch_colloc_rhs(const double2* bv, const double2* bo, long long bp
 cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
                                  double2* ov, double2* oo, long long op, const DnsGeom& g,
                                  cudaStream_t st);
+// *flag |= 1 if any of the n complex values of a or b is not finite
+cudaError_t launch_nonfinite(const double2* a, const double2* b, long long n, int* flag,
+                             cudaStream_t st);

@@ -12,7 +12,7 @@
 // save_recovery_internal steps (not at step 0).  Each step prints its time
 // and the mean; v-hat of mode (0,0), wall-normal coefficient 0, is printed at
 // output steps and every --print-every steps (reading it copies the state to
-// the host).
+// the host).  A state that turns NaN or Inf ends the run (exit status 3).
 #include <chrono>
 #include <complex>
 #include <cstdio>
@@ -96,6 +96,11 @@ int main(int argc, char** argv) {
     check(dns_step(ctx, 1), "step");
     check(dns_synchronize(ctx), "step");
     const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (dns_check_state(ctx) == DNS_ERR_NONFINITE) {
+      std::fprintf(stderr, "dns_run: the state holds NaN or Inf after step %d\n", i);
+      dns_destroy(ctx);
+      return 3;
+    }
     total += t;
     ++count;
     std::printf("Time cost of current step:%g\nMean time cost per step:%g\n", t, total / count);

@@ -115,6 +115,11 @@ dns_status dns_get_state(dns_ctx* ctx, void* v, void* omega, size_t pitch, int w
 dns_status dns_get_history(dns_ctx* ctx, void* nv, void* nomega, size_t pitch, int where);
 dns_status dns_set_history(dns_ctx* ctx, const void* nv, const void* nomega, size_t pitch, int where);
 
+/* Failure detection (no counterpart in the reference): DNS_ERR_NONFINITE if
+ * the current state holds a NaN or an Inf, else DNS_OK.  One pass over the
+ * state on the device (about 0.02 ms at 256x129x256); synchronous. */
+dns_status dns_check_state(dns_ctx* ctx);
+
 /* Recovery file in the reference's format (source/output.cpp:105-178):
  * int mx, my, mz; size_t pSize, tSize (the reference's allocator sizes,
  * source/operation.cpp:152-180, pitches from cudaMalloc3D on this device);

@@ -43,6 +43,7 @@ def test_argument_errors_without_gpu(pkg):
     assert lib.dns_solve_wall(None, None, None, 16, 0) == 1
     assert lib.dns_step_many(None, 0, 1) == 1
     assert b"no contexts" in lib.dns_last_error()
+    assert lib.dns_check_state(None) == 1
 
 
 def test_parameter_file(pkg, tmp_path):
