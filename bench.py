@@ -267,6 +267,27 @@ def run_ours(args, rank, world):
     def rel(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
+    def components(ctx, V, Om):
+        """getUVW of a state through the library (FP64 kernel): the six
+        velocity / vorticity coefficient fields, in standard axis names."""
+        Nz, Kx, Ny = V.shape
+        mz = CFG["mz"]
+        f = [torch.zeros((Nz, Kx, mz), dtype=torch.complex128, device="cuda") for _ in range(6)]
+        f[2][..., :Ny] = torch.from_numpy(V).cuda()
+        f[5][..., :Ny] = torch.from_numpy(Om).cuda()
+        torch.cuda.synchronize()
+        ctx.get_uvw([t.data_ptr() for t in f], mz * 16)
+        ctx.synchronize()
+        ref = [t[..., :Ny].cpu().numpy() for t in f]
+        # reference axes (u, v span, w wall-normal, omega_x, omega_y span,
+        # omega_z wall-normal) -> standard (u, v wall-normal, w span, ...)
+        return {"u": ref[0], "v": ref[2], "w": ref[1], "omega_x": ref[3], "omega_y": ref[5],
+                "omega_z": ref[4]}
+
+    def comp_errors(ctx, A, B):
+        ca, cb = components(ctx, *A), components(ctx, *B)
+        return {k: rel(ca[k], cb[k]) for k in ca}
+
     K, W = args.steps, args.warmup
     t_setup = time.perf_counter()
     c64 = make(pkg.PREC_FP64)
@@ -280,7 +301,7 @@ def run_ours(args, rank, world):
     cmx.step(ACC)
     V64, O64 = c64.get_state()
     Vmx, Omx = cmx.get_state()
-    acc_v, acc_o = rel(Vmx, V64), rel(Omx, O64)
+    acc = comp_errors(c64, (Vmx, Omx), (V64, O64))
     Nv64, No64 = c64.get_history()
     cmx.set_state(V64, O64)
     cmx.set_history(Nv64, No64)
@@ -288,7 +309,7 @@ def run_ours(args, rank, world):
     cmx.step(1)
     V64, O64 = c64.get_state()
     Vmx, Omx = cmx.get_state()
-    err_v, err_o = rel(Vmx, V64), rel(Omx, O64)
+    err = comp_errors(c64, (Vmx, Omx), (V64, O64))
     # timing, each form from the seeded state again
     for ctx in (c64, cmx):
         ctx.set_state(V0, O0)
@@ -328,7 +349,7 @@ def run_ours(args, rank, world):
     geo = dict(Kx=cmx.Kx, Nz=cmx.Nz, Ny=cmx.Ny, Py=cmx.Py, Pz=cmx.Pz)
     mem = cmx.memory_bytes()
     cmx.close()
-    return dict(ms64=ms64, msmx=msmx, err_v=err_v, err_o=err_o, acc_v=acc_v, acc_o=acc_o, acc_steps=ACC,
+    return dict(ms64=ms64, msmx=msmx, err=err, acc=acc, acc_steps=ACC,
                 kms64=kms64, kmsmx=kmsmx,
                 e2e_ms=e2e_ms, geo=geo, clocks=clk.summary(), setup_s=setup_s, mem=mem,
                 state_bytes=2 * geo["Kx"] * geo["Nz"] * geo["Ny"] * 16)
@@ -546,6 +567,35 @@ def roofline(kms, geo, c, peak, config="256x129x256", prec="mixed"):
                  "bytes_per_launch": kb[top], "ms_per_launch": round(kms[top], 4)}
 
 
+def launch_ranks(n):
+    """Run this command as n local ranks under torch.distributed.run (one
+    process per GPU, rendezvous on 127.0.0.1) and return its exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def check_launch(rank, world):
+    """Join the process group (NCCL with GPUs, else gloo) and have rank 0
+    print the job's rank count: the launch path without device work."""
+    import datetime
+    import torch
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    t = torch.ones(1, device="cuda" if backend == "nccl" else "cpu")
+    torch.distributed.all_reduce(t)
+    if rank == 0:
+        print(json.dumps({"n_gpus": world, "ranks_joined": int(t.item()), "backend": backend}))
+    torch.distributed.barrier()
+    torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -565,12 +615,22 @@ def main():
                     help="mx,my,mz of --solve (default 384x193x384 modes)")
     ap.add_argument("--ensemble", action="store_true",
                     help="the 48-run ensemble (concurrent runs, one GPU): prints its own line")
+    ap.add_argument("--check-launch", action="store_true",
+                    help="start the ranks and print their count only (no device work)")
     args = ap.parse_args()
     global CFG
     CFG = CONFIGS[args.config]
     args.warmup = max(args.warmup, 3)
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # not started by torchrun: start the N ranks here, one process per GPU
+        sys.exit(launch_ranks(args.gpus))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}: launch one rank per GPU")
+    if args.check_launch:
+        check_launch(rank, world)
+        return
 
     if args.impl == "reference":
         # the reference's algorithm on the host (oracle port): rank 0 only
@@ -630,11 +690,11 @@ def main():
                      "roofline": roof64, "step_bytes_algorithmic": step_bytes64,
                      "step_frac_of_peak": round(step_bytes64 / (r["ms64"] * 1e-3) / 1e9 / peak, 4)},
             "mixed_vs_fp64": {"speedup": round(r["ms64"] / r["msmx"], 3),
-                              "per_step_rel_l2_err_v": r["err_v"], "per_step_rel_l2_err_omega_y": r["err_o"],
-                              "within_1e-6": bool(r["err_v"] <= 1e-6 and r["err_o"] <= 1e-6),
-                              "accumulated_rel_l2_err_v": r["acc_v"],
-                              "accumulated_rel_l2_err_omega_y": r["acc_o"],
-                              "accumulated_after_steps": r["acc_steps"]},
+                              "per_step_rel_l2_err": r["err"],
+                              "within_1e-6": bool(all(r["err"][k] <= 1e-6 for k in ("u", "v", "w", "omega_y"))),
+                              "accumulated_rel_l2_err": r["acc"],
+                              "accumulated_after_steps": r["acc_steps"],
+                              "axes": "standard: u streamwise, v wall-normal, w spanwise"},
             "roofline": dict(roofmx, peak_kind=f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"),
             "step_frac_of_peak": round(step_bytes_mx / (r["msmx"] * 1e-3) / 1e9 / peak, 4),
             "step_bytes_algorithmic": step_bytes_mx,

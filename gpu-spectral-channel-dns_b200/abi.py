@@ -30,6 +30,8 @@ EXPORTS = [
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
     "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
+    "dns_nonlinear", "dns_rhs_v", "dns_rhs_omega", "dns_rhs_mean", "dns_operator_matrices",
+    "dns_operator_tables", "dns_set_wait_limit",
 ]
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1
@@ -115,7 +117,14 @@ def load_library(path: str | None = None):
         "dns_get_uvw": [vp, C.POINTER(vp), sz],
         "dns_compute_lamb": [vp, C.POINTER(vp), C.POINTER(vp), sz],
         "dns_rhs_nonlinear": [vp, vp, vp, vp, sz],
-        "dns_solve_eq": [vp, vp, vp, i, sz],
+        "dns_solve_eq": [vp, vp, vp, i, sz, i],
+        "dns_nonlinear": [vp, vp, vp, vp, vp, sz, i],
+        "dns_rhs_v": [vp, vp, vp, vp, vp, sz, i],
+        "dns_rhs_omega": [vp, vp, vp, vp, vp, vp, sz, i],
+        "dns_rhs_mean": [vp, vp, vp, vp, vp, vp, vp, i],
+        "dns_operator_matrices": [vp, vp, vp, i],
+        "dns_operator_tables": [vp, vp, vp, vp, vp, vp, vp],
+        "dns_set_wait_limit": [vp, C.c_longlong],
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
         "dns_step_many": [C.POINTER(vp), i, i],
@@ -338,8 +347,41 @@ class Context:
     def rhs_nonlinear(self, lx, ly, lz, tpitch):
         self._call("dns_rhs_nonlinear", C.c_void_p(lx), C.c_void_p(ly), C.c_void_p(lz), tpitch)
 
-    def solve_eq(self, inv, rhs, N, tpitch):
-        self._call("dns_solve_eq", C.c_void_p(inv), C.c_void_p(rhs), int(N), tpitch)
+    def solve_eq(self, inv, rhs, N, tpitch, where=DEVICE):
+        self._call("dns_solve_eq", C.c_void_p(inv), C.c_void_p(rhs), int(N), tpitch, int(where))
+
+    def nonlinear(self, v, omega, nv, nomega, tpitch, where=DEVICE):
+        """getNonlinear + no-pad s2p: state -> nonlinear terms at the points."""
+        self._call("dns_nonlinear", C.c_void_p(v), C.c_void_p(omega), C.c_void_p(nv),
+                   C.c_void_p(nomega), tpitch, int(where))
+
+    def rhs_v(self, rhs_v, rhs_v_p, nv, nv_p, tpitch, where=DEVICE):
+        self._call("dns_rhs_v", C.c_void_p(rhs_v), C.c_void_p(rhs_v_p), C.c_void_p(nv),
+                   C.c_void_p(nv_p), tpitch, int(where))
+
+    def rhs_omega(self, rhs_omega, nomega, nomega_p, rhs_v, rhs_v_p, tpitch, where=DEVICE):
+        self._call("dns_rhs_omega", C.c_void_p(rhs_omega), C.c_void_p(nomega), C.c_void_p(nomega_p),
+                   C.c_void_p(rhs_v), C.c_void_p(rhs_v_p), tpitch, int(where))
+
+    def rhs_mean(self, u0, lx0, lx0_p, w0, lz0, lz0_p, where=DEVICE):
+        self._call("dns_rhs_mean", C.c_void_p(u0), C.c_void_p(lx0), C.c_void_p(lx0_p),
+                   C.c_void_p(w0), C.c_void_p(lz0), C.c_void_p(lz0_p), int(where))
+
+    def set_wait_limit(self, cycles=1 << 31):
+        """Bound of the staging waits (SM cycles); negative: give up at once."""
+        self._call("dns_set_wait_limit", int(cycles))
+
+    def operator_matrices(self, a_v, a_o, where=DEVICE):
+        self._call("dns_operator_matrices", C.c_void_p(a_v), C.c_void_p(a_o), int(where))
+
+    def operator_tables(self):
+        """(T0, T2, T4, U, dU, ddU) as numpy arrays."""
+        import numpy as np
+        n = self.Ny
+        T = [np.zeros((n, n)) for _ in range(3)]
+        U = [np.zeros(n) for _ in range(3)]
+        self._call("dns_operator_tables", *[a.ctypes.data_as(C.c_void_p) for a in T + U])
+        return (*T, *U)
 
     def solve_wall(self, v, omega, tpitch, where=DEVICE):
         """solveEq of both wall-normal systems with the banded factors, in place.

@@ -100,6 +100,11 @@ dns_status check_status(dns_ctx* c) {
   int s = 0;
   CK(cudaMemcpyAsync(&s, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (s) {
+    // reported once: the flag is cleared, so that the context is usable again
+    CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
   if (s & 1) return fail(DNS_ERR_TIMEOUT, "a device wait ran past its iteration limit");
   if (s & 2) return fail(DNS_ERR_SINGULAR, "an operator matrix had a zero pivot");
   return DNS_OK;
@@ -140,12 +145,17 @@ dns_status build_wall_solver(dns_ctx* c) {
   return DNS_OK;
 }
 
+// the state and AB2 history a pass sequence reads and writes
+struct StepBufs {
+  double2 *V, *O, *Nvp, *Nop;
+};
+
 // Enqueue one step (boot = 0) or the history bootstrap (boot = 1).  With
 // `ev` (7 events) an event is recorded before the first and after every
 // kernel, for per-kernel timing on the launching stream.
 template <typename C>
 cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const DevFft<C>& fx,
-                             const DevFft<C>& fyP, cudaEvent_t* ev) {
+                             const DevFft<C>& fyP, cudaEvent_t* ev, StepBufs b) {
   const DnsGeom& g = c->g;
   const long long H = g.H;
   PencilArr F6p{c->F6, c->PyS, H * c->PyS};
@@ -156,7 +166,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
   mark();
-  if ((e = launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->status, c->st))) return e;
+  if ((e = launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st))) return e;
   mark();
   if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status))) return e;
   mark();
@@ -169,22 +179,23 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   const double* t0 = c->rtab;
   const RhsTabs tb{t0, t0 + 4 * nv, t0 + 4 * nv + 2 * no, t0 + 4 * nv + 2 * no + g.Ny,
                    t0 + 4 * nv + 2 * no + g.Ny + 5 * nv};
-  if ((e = launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
+  if ((e = launch_y1<C>(F3p, b.V, b.O, b.Nvp, b.Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
                         boot, c->status, c->st)))
     return e;
   mark();
   if (!boot)
-    if ((e = launch_wall_solve(c->wfac, c->V, c->O, c->rv, c->ro, c->wQ, (double2*)c->F6, c->wd, g,
+    if ((e = launch_wall_solve(c->wfac, b.V, b.O, c->rv, c->ro, c->wQ, (double2*)c->F6, c->wd, g,
                                c->ph, c->status, c->st)))
       return e;
   mark();
   return cudaSuccess;
 }
 
-cudaError_t enqueue(dns_ctx* c, int boot, cudaEvent_t* ev = nullptr) {
+cudaError_t enqueue(dns_ctx* c, int boot, cudaEvent_t* ev = nullptr, const StepBufs* bufs = nullptr) {
+  const StepBufs b = bufs ? *bufs : StepBufs{c->V, c->O, c->Nvp, c->Nop};
   if (c->P.precision == DNS_PREC_MIXED)
-    return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f, ev);
-  return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d, ev);
+    return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f, ev, b);
+  return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d, ev, b);
 }
 
 dns_status need_scratch(dns_ctx* c) {
@@ -373,7 +384,7 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->probe, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->rhs_io, c->nl_io, c->eq_io, c->probe, c->status};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -503,6 +514,25 @@ dns_status dns_bootstrap(dns_ctx* c) {
   return s;
 }
 
+dns_status dns_nonlinear(dns_ctx* c, const void* v, const void* o, void* nv, void* no, size_t tpitch,
+                         int where) {
+  if (!c || !v || !o || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->P.device));
+  const size_t hn = (size_t)c->g.H * c->g.Ny;
+  if (!c->nl_io) CK(c->alloc(&c->nl_io, 4 * hn));
+  // the pass sequence of the bootstrap on the caller's state, into the
+  // context's own vectors: the state and history of the context are untouched
+  StepBufs b{c->nl_io, c->nl_io + hn, c->nl_io + 2 * hn, c->nl_io + 3 * hn};
+  dns_status s = copy_pencils(c, b.V, v, nullptr, tpitch, where, true);
+  if (s == DNS_OK) s = copy_pencils(c, b.O, o, nullptr, tpitch, where, true);
+  if (s != DNS_OK) return s;
+  CK(enqueue(c, 1, nullptr, &b));
+  s = check_status(c);
+  if (s == DNS_OK) s = history_out(c, b.Nvp, nv, tpitch, where);
+  if (s == DNS_OK) s = history_out(c, b.Nop, no, tpitch, where);
+  return s;
+}
+
 namespace {
 // checks, factors and the captured step graph of one context
 dns_status step_ready(dns_ctx* c) {
@@ -531,6 +561,18 @@ dns_status dns_step(dns_ctx* c, int nsteps) {
   dns_status s = step_ready(c);
   if (s != DNS_OK) return s;
   for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph, c->st));
+  return DNS_OK;
+}
+
+dns_status dns_set_wait_limit(dns_ctx* c, long long cycles) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->P.device));
+  CK(cudaStreamSynchronize(c->st));
+  c->ph.wait_limit = cycles;
+  if (c->graph) {  // the step graph holds the kernel parameters: capture it again
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
   return DNS_OK;
 }
 
@@ -698,11 +740,71 @@ dns_status dns_rhs_nonlinear(dns_ctx* c, void* lx, void* ly, const void* lz, siz
   return DNS_OK;
 }
 
-dns_status dns_solve_eq(dns_ctx* c, const void* inv, void* rhs, int N, size_t tpitch) {
+dns_status dns_solve_eq(dns_ctx* c, const void* inv, void* rhs, int N, size_t tpitch, int where) {
   if (!c || !inv || !rhs) return fail(DNS_ERR_ARG, "null argument");
   if (N < 1 || N > 4096 || tpitch % 16 || tpitch < (size_t)N * 16) return fail(DNS_ERR_ARG, "bad N or tpitch");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
   CK(cudaSetDevice(c->P.device));
-  CK(launch_solve_eq((const double2*)inv, (double2*)rhs, (long long)(tpitch / 16), N, c->g.H, c->st));
+  const long long H = c->g.H;
+  if (where == DNS_DEVICE) {
+    CK(launch_solve_eq((const double2*)inv, (double2*)rhs, (long long)(tpitch / 16), N, H, c->st));
+    return DNS_OK;
+  }
+  // host inverses and right-hand sides (the reference keeps both in host
+  // memory, source/solver.cpp:216-257): streamed through a device staging
+  // buffer in batches of pencils, at most ~512 MiB of inverses at a time
+  const size_t NN16 = (size_t)N * N * 16, row = (size_t)N * 16;
+  const long long batch = std::max(1LL, std::min<long long>(H, (512LL << 20) / (long long)NN16));
+  const size_t need = (size_t)batch * (NN16 + row);
+  if (c->eq_io_bytes < need) {
+    if (c->eq_io) cudaFree(c->eq_io);
+    c->eq_io = nullptr;
+    c->eq_io_bytes = 0;
+    CK(c->alloc(&c->eq_io, need));
+    c->eq_io_bytes = need;
+  }
+  double2* dinv = (double2*)c->eq_io;
+  double2* drhs = (double2*)(c->eq_io + (size_t)batch * NN16);
+  for (long long p0 = 0; p0 < H; p0 += batch) {
+    const long long np = std::min(batch, H - p0);
+    CK(cudaMemcpyAsync(dinv, (const char*)inv + (size_t)p0 * NN16, (size_t)np * NN16,
+                       cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpy2DAsync(drhs, row, (const char*)rhs + (size_t)p0 * tpitch, tpitch, row, (size_t)np,
+                         cudaMemcpyHostToDevice, c->st));
+    CK(launch_solve_eq(dinv, drhs, N, N, np, c->st));
+    CK(cudaMemcpy2DAsync((char*)rhs + (size_t)p0 * tpitch, tpitch, drhs, row, row, (size_t)np,
+                         cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return DNS_OK;
+}
+
+dns_status dns_operator_matrices(dns_ctx* c, void* a_v, void* a_o, int where) {
+  if (!c || !a_v || !a_o) return fail(DNS_ERR_ARG, "null argument");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
+  CK(cudaSetDevice(c->P.device));
+  const long long NN = (long long)c->g.Ny * c->g.Ny, H = c->g.H;
+  if (where == DNS_DEVICE) {
+    CK(launch_operator_matrices(0, H, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt,
+                                (double2*)a_v, (double2*)a_o, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return DNS_OK;
+  }
+  const long long batch = std::max(1LL, std::min<long long>(H, (1LL << 30) / (NN * 32)));
+  double2 *dv = nullptr, *dO = nullptr;
+  CK(cudaMalloc(&dv, (size_t)batch * NN * 16));
+  if (cudaMalloc(&dO, (size_t)batch * NN * 16)) { cudaFree(dv); return fail(DNS_ERR_CUDA, "staging"); }
+  cudaError_t e = cudaSuccess;
+  for (long long p0 = 0; p0 < H && !e; p0 += batch) {
+    const long long np = std::min(batch, H - p0);
+    e = launch_operator_matrices(p0, np, c->g, c->ph, c->T0, c->T2, c->T4, c->Ut, c->ddUt, dv, dO, c->st);
+    if (!e) e = cudaMemcpyAsync((double2*)a_v + p0 * NN, dv, (size_t)np * NN * 16, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaMemcpyAsync((double2*)a_o + p0 * NN, dO, (size_t)np * NN * 16, cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaStreamSynchronize(c->st);
+  }
+  cudaFree(dv);
+  cudaFree(dO);
+  if (e) return fail(DNS_ERR_CUDA, cudaGetErrorString(e));
   return DNS_OK;
 }
 
@@ -713,10 +815,13 @@ dns_status dns_check_state(dns_ctx* c) {
   if (!c->probe) CK(c->alloc(&c->probe, 1));
   CK(cudaMemsetAsync(c->probe, 0, sizeof(int), c->st));
   CK(launch_nonfinite(c->V, c->O, c->g.H * c->g.Ny, c->probe, c->st));
+  // the AB2 history too: it is written to recovery files, and a non-finite
+  // nonlinear term reaches the state only one step later
+  CK(launch_nonfinite(c->Nvp, c->Nop, c->g.H * c->g.Ny, c->probe, c->st));
   int bad = 0;
   CK(cudaMemcpyAsync(&bad, c->probe, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  if (bad) return fail(DNS_ERR_NONFINITE, "the state holds NaN or Inf");
+  if (bad) return fail(DNS_ERR_NONFINITE, "the state or the AB2 history holds NaN or Inf");
   return DNS_OK;
 }
 

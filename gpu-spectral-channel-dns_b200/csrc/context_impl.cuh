@@ -44,6 +44,10 @@ struct dns_ctx {
   size_t F6_bytes = 0;
   double2* scratch = nullptr;
   double2* solve_io = nullptr;  // solve-only entry: both systems' vectors + wall polynomials
+  double2* rhs_io = nullptr;    // right-hand-side drop-ins: host staging (6 H Ny)
+  double2* nl_io = nullptr;     // dns_nonlinear: state in, nonlinear terms out (4 H Ny)
+  unsigned char* eq_io = nullptr;  // dns_solve_eq on host buffers: inverse and rhs staging
+  size_t eq_io_bytes = 0;
   int* probe = nullptr;         // dns_check_state: set when the state holds NaN or Inf
   int* status = nullptr;
   bool have_state = false, booted = false, wall_ready = false;

@@ -34,10 +34,14 @@ struct RowArr {         // generic row-major [field][y][zp][kx] array
   long long fs;         // field stride (elements)
 };
 
+// default bound of a device wait, in SM clock cycles (~1 s at 2 GHz)
+#define DNS_WAIT_LIMIT (1LL << 31)
+
 struct PhysParams {
   double aphi, beta;    // box: alpha_k = kx/aphi, beta_k = kz/beta
   double Re, Ro, dt;
   double U0, U1, U2;    // base flow U(y) = U0 + U1 y + U2 y^2
+  long long wait_limit = DNS_WAIT_LIMIT;  // staging waits of the wall-normal warp passes
 };
 
 // 16-byte alignment of a device pointer (bulk-copy sources)

@@ -1,6 +1,8 @@
 // mbarrier and bulk-copy (cp.async.bulk) helpers, inline PTX for sm_100a.
 // Every wait is bounded: it gives up after `limit` SM clock cycles, or at
-// once when another CTA has already reported a timeout in *status.
+// once when another CTA has already reported a timeout in *status.  A CTA
+// that gives up waits for its own copies in flight (with the full limit)
+// before it exits.
 #pragma once
 #include <stdint.h>
 
@@ -45,8 +47,10 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
       ::"r"(smem_u32(dst)), "l"((unsigned long long)tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
+// A negative limit gives up at once (the test hook for the timeout path).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit,
                                                   const int* status) {
+  if (limit < 0) return false;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
     if (clock64() - t0 > limit) return false;

@@ -20,7 +20,8 @@
 // every entry it later reads, so nothing needs clearing, but calls that
 // overlap on the GPU (different streams, contexts or threads) race on it.
 // The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current; make that first call
+// (cudaGetSymbolAddress) with that device current, and again after the
+// device's context has been reset and created anew; make that first call
 // before any stream capture.
 #include <mutex>
 #include <string>
@@ -38,16 +39,36 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[DNS_NOALLOC_SCR
 namespace {
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[DNS_NOALLOC_MAX_DEVICES];
+void* g_noalloc_ctx[DNS_NOALLOC_MAX_DEVICES];  // the context the address belongs to
 
-// device address of g_noalloc_scratch on the current device (looked up once)
+// the driver's cuCtxGetCurrent, through the runtime (no link against libcuda)
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return (CtxGetCurrentFn)p;
+  }();
+  return fn;
+}
+
+// device address of g_noalloc_scratch on the current device, looked up once
+// per device and context: a context that was reset (cudaDeviceReset) and
+// created again loads the module again, at a possibly different address
 cudaError_t noalloc_scratch(int dev, void** out) {
   if (dev < 0 || dev >= DNS_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  void* ctx = nullptr;
+  if (CtxGetCurrentFn f = ctx_get_current()) f(&ctx);
+  if (!g_noalloc_addr[dev] || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_noalloc_addr[dev] = p;
+    g_noalloc_ctx[dev] = ctx;
   }
   *out = g_noalloc_addr[dev];
   return cudaSuccess;

@@ -335,3 +335,34 @@ cudaError_t launch_transpose_ref(int dir, double2* xyz, long long ps, double2* z
   k_transpose_ref<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(dir, xyz, ps, zxy, tps, g);
   return cudaGetLastError();
 }
+
+// The collocation operators themselves, row-major out{v,o}[p][i][j] for the
+// pencils p0 .. p0 + gridDim.x - 1 (initAuxMatrix with inversed = false,
+// source/solver.cpp:275-313): the same entries k_gj_invert inverts.
+__global__ void k_operator_matrices(long long p0, DnsGeom g, PhysParams ph, const double* T0,
+                                    const double* T2, const double* T4, const double* U,
+                                    const double* ddU, double2* outV, double2* outO) {
+  const long long lp = blockIdx.x;
+  const long long p = p0 + lp;
+  const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
+  const bool zero = (kx == 0 && kz == 0);
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = kmn_of(ia, ib);
+  const int N = g.Ny;
+  const size_t NN = (size_t)N * N;
+  for (int t = threadIdx.x; t < N * N; t += blockDim.x) {
+    const int i = t / N, j = t - i * N;
+    outV[lp * NN + t] = op_entry(0, zero, i, j, N, T0, T2, T4, U, ddU, ph.Re, ph.dt, kmn, ia);
+    outO[lp * NN + t] = op_entry(1, zero, i, j, N, T0, T2, T4, U, ddU, ph.Re, ph.dt, kmn, ia);
+  }
+}
+
+cudaError_t launch_operator_matrices(long long p0, long long np, DnsGeom g, PhysParams ph,
+                                     const double* T0, const double* T2, const double* T4,
+                                     const double* U, const double* ddU, double2* outV,
+                                     double2* outO, cudaStream_t st) {
+  if (np <= 0) return cudaSuccess;
+  k_operator_matrices<<<(unsigned)np, 256, 0, st>>>(p0, g, ph, T0, T2, T4, U, ddU, outV, outO);
+  return cudaGetLastError();
+}

@@ -11,3 +11,7 @@ cudaError_t launch_gj_invert(int mode, long long unit0, long long nunits, DnsGeo
                              double2* outV, double2* outO, int* status, cudaStream_t st);
 cudaError_t launch_transpose_ref(int dir, double2* xyz, long long ps, double2* zxy, long long tps,
                                  DnsGeom g, cudaStream_t st);
+cudaError_t launch_operator_matrices(long long p0, long long np, DnsGeom g, PhysParams ph,
+                                     const double* T0, const double* T2, const double* T4,
+                                     const double* U, const double* ddU, double2* outV,
+                                     double2* outO, cudaStream_t st);

@@ -404,10 +404,10 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
     bulk_g2s(oz, O + p * Ny, (uint32_t)(Ny * 16), &bar);
   }
   __syncthreads();
-  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, 1LL << 31, status))) {
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, ph.wait_limit, status))) {
     if (threadIdx.x == 0) {
       atomicOr(status, 1);
-      mbar_wait_bounded(&bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+      mbar_wait_bounded(&bar, 0, DNS_WAIT_LIMIT, nullptr);  // let the copies land before leaving
     }
     return;
   }
@@ -807,10 +807,10 @@ __global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __
     }
   }
   __syncthreads();
-  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, 1LL << 31, status))) {
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, ph.wait_limit, status))) {
     if (threadIdx.x == 0) {
       atomicOr(status, 1);
-      mbar_wait_bounded(&bar, 0, 1LL << 31, nullptr);  // let the copies land before leaving
+      mbar_wait_bounded(&bar, 0, DNS_WAIT_LIMIT, nullptr);  // let the copies land before leaving
     }
     return;
   }

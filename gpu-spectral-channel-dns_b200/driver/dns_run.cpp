@@ -96,11 +96,13 @@ int main(int argc, char** argv) {
     check(dns_step(ctx, 1), "step");
     check(dns_synchronize(ctx), "step");
     const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (dns_check_state(ctx) == DNS_ERR_NONFINITE) {
+    const dns_status cs = dns_check_state(ctx);
+    if (cs == DNS_ERR_NONFINITE) {
       std::fprintf(stderr, "dns_run: the state holds NaN or Inf after step %d\n", i);
       dns_destroy(ctx);
       return 3;
     }
+    check(cs, "state check");  // any other failure of the check ends the run (status 2)
     total += t;
     ++count;
     std::printf("Time cost of current step:%g\nMean time cost per step:%g\n", t, total / count);

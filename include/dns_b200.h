@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define DNS_B200_ABI_VERSION 1
+#define DNS_B200_ABI_VERSION 2
 
 typedef struct dns_ctx dns_ctx;
 
@@ -116,8 +116,9 @@ dns_status dns_get_history(dns_ctx* ctx, void* nv, void* nomega, size_t pitch, i
 dns_status dns_set_history(dns_ctx* ctx, const void* nv, const void* nomega, size_t pitch, int where);
 
 /* Failure detection (no counterpart in the reference): DNS_ERR_NONFINITE if
- * the current state holds a NaN or an Inf, else DNS_OK.  One pass over the
- * state on the device (about 0.02 ms at 256x129x256); synchronous. */
+ * the current state or the AB2 history holds a NaN or an Inf, else DNS_OK.
+ * One pass over state and history on the device (about 0.04 ms at
+ * 256x129x256); synchronous. */
 dns_status dns_check_state(dns_ctx* ctx);
 
 /* Recovery file in the reference's format (source/output.cpp:105-178):
@@ -165,6 +166,15 @@ dns_status dns_step(dns_ctx* ctx, int nsteps);
  * GPU.  Asynchronous like dns_step: synchronise each context (or the device)
  * before reading results.  A context may appear once. */
 dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps);
+
+/* No counterpart in the reference.  The bound, in SM clock cycles, after
+ * which a staging wait of the mixed form's wall-normal passes gives up: the
+ * CTA lets its copies in flight land, skips its work and the next
+ * synchronising call reports DNS_ERR_TIMEOUT once (the flag is then cleared;
+ * the state of that step is not valid).  Default 2^31 (about a second); a
+ * negative value makes those waits give up at once, for tests of the timeout
+ * path.  The next dns_step captures the step graph again. */
+dns_status dns_set_wait_limit(dns_ctx* ctx, long long cycles);
 
 /* The same steps without the graph, with CUDA events recorded around each
  * of the DNS_NUM_KERNELS kernels of a step on the context stream;
@@ -217,8 +227,12 @@ dns_status dns_compute_lamb(dns_ctx* ctx, void* const in[6], void* const out[3],
 dns_status dns_rhs_nonlinear(dns_ctx* ctx, void* lamb_x, void* lamb_y, const void* lamb_z,
                              size_t tpitch);
 /* solveEq (source/solver.cpp:107-123): rhs <- inv * rhs for every pencil;
- * inv row-major [ky][kx][N][N] complex, rhs pitched pencils. */
-dns_status dns_solve_eq(dns_ctx* ctx, const void* inv, void* rhs, int N, size_t tpitch);
+ * inv row-major [ky][kx][N][N] complex, rhs pitched pencils.  where =
+ * DNS_DEVICE: both on the device, asynchronous.  where = DNS_HOST: both in
+ * host memory, as the reference keeps them (source/solver.cpp:216-257);
+ * streamed through a device staging buffer (allocated on first use),
+ * synchronous. */
+dns_status dns_solve_eq(dns_ctx* ctx, const void* inv, void* rhs, int N, size_t tpitch, int where);
 /* solveEq (source/solver.cpp:107-123) for both wall-normal systems of every
  * pencil, without the explicit inverses: the banded factors of the time step
  * (built on first use) solve the reference's collocation systems
@@ -237,6 +251,53 @@ dns_status dns_solve_wall(dns_ctx* ctx, void* v, void* omega, size_t tpitch, int
 /* initAuxMatrix (source/solver.cpp:260-320): explicit inverses of the v and
  * omega operators of every pencil, row-major [ky][kx][nz][nz] complex. */
 dns_status dns_init_aux_matrix(dns_ctx* ctx, void* inv_v, void* inv_omega, int where);
+/* initAuxMatrix(pb, inversed = false): the operators themselves
+ * (source/coefficient.cu:7-86), same layout; pencil (0,0) holds the
+ * mean-mode operator in both.  Synchronous. */
+dns_status dns_operator_matrices(dns_ctx* ctx, void* a_v, void* a_omega, int where);
+/* The host tables initAuxMatrix fills (source/coefficient.cu:88-159):
+ * T0, T2, T4 as [nz][nz] row-major (T_j and its 2nd / 4th derivative at the
+ * Gauss-Lobatto point y_i = cos(pi i/(nz-1)) in entry [i][j]) and U, U', U''
+ * at those points.  Host pointers; any may be NULL.  Synchronous. */
+dns_status dns_operator_tables(dns_ctx* ctx, double* T0, double* T2, double* T4, double* U,
+                               double* dU, double* ddU);
+
+/* ---- the step function by function (reference-layout drop-ins) ----------
+ * For callers that run the reference's own sequence (source/solver.cpp:
+ * 35-101): get_rhs_v, solveEq(v), get_rhs_omega, solveEq(omega).  Pencils in
+ * the reference's layout ([Nz][Kx] pencils of tpitch bytes, Ny complex used);
+ * where = DNS_HOST (synchronous; staged through device vectors allocated on
+ * first use) or DNS_DEVICE (asynchronous, in place).  dns_step does all of
+ * it in one graph and is the fast path. */
+
+/* getNonlinear + the worker's post-processing (source/nonlinear.cu:25-108,
+ * source/rhs.cpp:83-127): from the state (v, omega_y coefficients) to the
+ * nonlinear terms at the Ny collocation points, the reference's
+ * nonlinear_v / nonlinear_omega_y; pencil (0,0) holds the raw lambda_x /
+ * lambda_span values (lambx0 / lambz0).  Computed in the context's
+ * precision; the context's own state and history are not touched.
+ * Synchronous; allocates 4 H Ny complex on first use. */
+dns_status dns_nonlinear(dns_ctx* ctx, const void* v, const void* omega, void* nv, void* nomega,
+                         size_t tpitch, int where);
+/* get_linear_v + the AB2 loop of get_rhs_v (source/linear.cpp:7-41,86-125,
+ * source/rhs.cpp:185-219), every pencil but (0,0): rhs_v_p <- rhs_v (v^n);
+ * rhs_v <- explicit CN v operator at y_2..y_{N-2} + dt (1.5 nv - 0.5 nv_p),
+ * rows 0..3 zero.  FP64. */
+dns_status dns_rhs_v(dns_ctx* ctx, void* rhs_v, void* rhs_v_p, const void* nv, const void* nv_p,
+                     size_t tpitch, int where);
+/* get_rhs_omega = get_linear_omega_y (source/linear.cpp:52-84,127-171),
+ * every pencil but (0,0): rhs_omega <- explicit CN omega operator at
+ * y_1..y_{N-1}, tilting -i beta U' dt/2 (rhs_v + rhs_v_p) with rhs_v = v^{n+1}
+ * (after the v solve) and rhs_v_p = v^n, + dt (1.5 nomega - 0.5 nomega_p);
+ * rows 0..1 zero.  FP64. */
+dns_status dns_rhs_omega(dns_ctx* ctx, void* rhs_omega, const void* nomega, const void* nomega_p,
+                         const void* rhs_v, const void* rhs_v_p, size_t tpitch, int where);
+/* get_linear_zero_wave_u_w (source/linear.cpp:43-50,173-205): the mean-mode
+ * right-hand sides, in place on u0 (tv0) and w0 (tomega_y_0), Ny complex
+ * each, from lambda_x / lambda_span at the collocation points (lambx0,
+ * lambz0) and their previous values. */
+dns_status dns_rhs_mean(dns_ctx* ctx, void* u0, const void* lambx0, const void* lambx0_p, void* w0,
+                        const void* lambz0, const void* lambz0_p, int where);
 
 /* ---- slab decomposition plan (host only, no device work) --------------
  * No counterpart in the reference.  For R ranks: rank r owns the operator

@@ -353,6 +353,40 @@ def get_uvw(tw, toz, sz: Sizes, aphi, beta):
     return u, v, w_out, ox, oy, oz_out
 
 
+def get_uvw_pencils(w, oz, ky, kx, sz: Sizes, aphi, beta):
+    """get_uvw on a list of pencils: w, oz of shape (P, nz) at (ky[p], kx[p]).
+
+    The same formulas as get_uvw (source/velocity.cu:90-170), pencil by
+    pencil, for checks on a sample of the pencils of a large grid.
+    """
+    w = np.asarray(w, dtype=np.complex128)
+    oz = np.asarray(oz, dtype=np.complex128)
+    ky = np.asarray(ky)
+    kx = np.asarray(kx)
+    ia, ib = ialpha_ibeta(kx, ky, sz.ny, aphi, beta)
+    kmn = ia * ia + ib * ib
+    with np.errstate(divide="ignore", invalid="ignore"):
+        kmn1 = np.where(kmn > 0, 1.0 / kmn, 0.0)
+    Dw = ddz(w)
+    c_a = (1j * (ia * kmn1))[:, None]
+    c_b = (1j * (ib * kmn1))[:, None]
+    u = c_a * Dw - c_b * oz
+    v = c_b * Dw + c_a * oz
+    ox = ddz(v) + (-1j * ib)[:, None] * w
+    oy = -ddz(u) + (1j * ia)[:, None] * w
+    w_out = w.copy()
+    oz_out = oz.copy()
+    m = (kx == 0) & (ky == 0)
+    if m.any():
+        u[m] = w[m]
+        v[m] = oz[m]
+        w_out[m] = 0.0
+        ox[m] = ddz(v[m])
+        oy[m] = -ddz(u[m])
+        oz_out[m] = 0.0
+    return u, v, w_out, ox, oy, oz_out
+
+
 # --------------------------------------------------------------------------
 # Lamb vector and rhsNonlinear (source/nonlinear.cu:146-242, 366-428)
 # --------------------------------------------------------------------------
@@ -483,27 +517,39 @@ class Problem:
         self.kmn = self.ia ** 2 + self.ib ** 2
         self._inv_v = None
         self._inv_o = None
+        self.solver = "inverse"
 
     # -- operators (source/solver.cpp:260-320) -----------------------------
-    def build_inverses(self):
+    def operators(self, ky, kx):
+        """The v and omega collocation matrices of pencils (ky[i], kx[i]).
+
+        source/solver.cpp:275-313: pencil (0,0) carries the mean-mode
+        operator (_get_coef_u0 = _get_coef_w0) in both slots.
+        """
         sz, p = self.sz, self.p
         N = sz.nz - 1
-        Av = np.zeros((sz.ny, sz.hnx, sz.nz, sz.nz), dtype=np.complex128)
+        n = len(ky)
+        Av = np.zeros((n, sz.nz, sz.nz), dtype=np.complex128)
         Ao = np.zeros_like(Av)
-        for ky in range(sz.ny):
-            for kx in range(sz.hnx):
-                if kx == 0 and ky == 0:
-                    Av[0, 0] = coef_u0(N, self.T0, self.T2, p.Re, p.dt)
-                    Ao[0, 0] = Av[0, 0]
-                    continue
-                Av[ky, kx] = coef_v(N, self.U, self.ddU, self.T0, self.T2,
-                                    self.T4, p.Re, p.dt, self.kmn[ky, kx],
-                                    self.ia[ky, kx])
-                Ao[ky, kx] = coef_omega(N, self.U, self.T0, self.T2, p.Re,
-                                        p.dt, self.kmn[ky, kx], self.ia[ky, kx])
-        self.A_v, self.A_o = Av, Ao
-        self._inv_v = np.linalg.inv(Av)
-        self._inv_o = np.linalg.inv(Ao)
+        for i, (y, x) in enumerate(zip(ky, kx)):
+            if x == 0 and y == 0:
+                Av[i] = coef_u0(N, self.T0, self.T2, p.Re, p.dt)
+                Ao[i] = Av[i]
+                continue
+            Av[i] = coef_v(N, self.U, self.ddU, self.T0, self.T2, self.T4, p.Re, p.dt,
+                           self.kmn[y, x], self.ia[y, x])
+            Ao[i] = coef_omega(N, self.U, self.T0, self.T2, p.Re, p.dt, self.kmn[y, x],
+                               self.ia[y, x])
+        return Av, Ao
+
+    def build_inverses(self):
+        sz = self.sz
+        ky, kx = np.meshgrid(np.arange(sz.ny), np.arange(sz.hnx), indexing="ij")
+        Av, Ao = self.operators(ky.ravel(), kx.ravel())
+        shape = (sz.ny, sz.hnx, sz.nz, sz.nz)
+        self.A_v, self.A_o = Av.reshape(shape), Ao.reshape(shape)
+        self._inv_v = np.linalg.inv(self.A_v)
+        self._inv_o = np.linalg.inv(self.A_o)
 
     @property
     def inv_v(self):
@@ -516,6 +562,43 @@ class Problem:
         if self._inv_o is None:
             self.build_inverses()
         return self._inv_o
+
+    def solve(self, which, rhs):
+        """solveEq (source/solver.cpp:107-123) on every pencil of ``rhs``.
+
+        ``solver`` selects how: "inverse" multiplies by the stored explicit
+        inverses, as the reference does (source/matrix_op.cpp:68-78);
+        "lu" solves the stored matrices by LU with partial pivoting;
+        "batched" / "batched-lu" form the matrices a block of pencils at a
+        time without keeping them and invert / LU-solve them (the
+        arithmetic of "inverse" / "lu" for grids whose 2 H Ny^2 matrix
+        entries do not fit in memory).  The spread
+        between "inverse" and "lu" is the oracle's own rounding floor.
+        """
+        if self.solver == "inverse":
+            inv = self.inv_v if which == "v" else self.inv_o
+            return np.einsum("yxij,yxj->yxi", inv, rhs)
+        if self.solver == "lu":
+            if self._inv_v is None and getattr(self, "A_v", None) is None:
+                self.build_inverses()
+            A = self.A_v if which == "v" else self.A_o
+            return np.linalg.solve(A, rhs[..., None])[..., 0]
+        if self.solver not in ("batched", "batched-lu"):
+            raise ValueError("solver must be inverse, lu, batched or batched-lu")
+        sz = self.sz
+        ky, kx = np.meshgrid(np.arange(sz.ny), np.arange(sz.hnx), indexing="ij")
+        ky, kx = ky.ravel(), kx.ravel()
+        flat = rhs.reshape(-1, sz.nz)
+        out = np.empty_like(flat)
+        blk = max(1, (1 << 25) // (sz.nz * sz.nz))
+        for a in range(0, len(ky), blk):
+            Av, Ao = self.operators(ky[a:a + blk], kx[a:a + blk])
+            A = Av if which == "v" else Ao
+            if self.solver == "batched":
+                out[a:a + blk] = np.einsum("pij,pj->pi", np.linalg.inv(A), flat[a:a + blk])
+            else:
+                out[a:a + blk] = np.linalg.solve(A, flat[a:a + blk, :, None])[..., 0]
+        return out.reshape(rhs.shape)
 
     # -- state -------------------------------------------------------------
     def set_state(self, V, O):
@@ -653,13 +736,13 @@ class Problem:
         rv[0, 0] = self.linear_u0(self.V[0, 0], lx0, self.lx0_p)
         ro00 = self.linear_u0(self.O[0, 0], lz0, self.lz0_p)
         # solveEq v (solver.cpp:107-123)
-        Vnew = np.einsum("yxij,yxj->yxi", self.inv_v, rv)
+        Vnew = self.solve("v", rv)
         # get_rhs_omega (linear.cpp:52-84)
         ro = self.linear_omega(self.O, Vnew, Vold)
         i = np.arange(2, nz)
         ro[..., 2:] += (No[..., i - 1] * 1.5 - self.No_p[..., i - 1] * 0.5) * dt
         ro[0, 0] = ro00
-        Onew = np.einsum("yxij,yxj->yxi", self.inv_o, ro)
+        Onew = self.solve("o", ro)
         self.V, self.O = Vnew, Onew
         self.Nv_p, self.No_p = Nv, No
         self.lx0_p, self.lz0_p = lx0, lz0

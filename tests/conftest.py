@@ -37,3 +37,20 @@ def pkg():
 def oracle():
     from oracle import rpcf_oracle
     return rpcf_oracle
+
+
+# Measured parity errors, printed in the terminal summary (also with -q), so a
+# run's log carries the numbers and not only pass/fail.
+PARITY_LOG = []
+
+
+@pytest.fixture
+def parity_log():
+    return PARITY_LOG
+
+
+def pytest_terminal_summary(terminalreporter):
+    if PARITY_LOG:
+        terminalreporter.section("measured parity errors")
+        for line in PARITY_LOG:
+            terminalreporter.write_line(line)

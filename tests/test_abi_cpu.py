@@ -21,7 +21,7 @@ def test_library_exports_every_symbol(pkg):
     lib = pkg.load_library()
     for name in declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.dns_abi_version() == 1
+    assert lib.dns_abi_version() == 2
 
 
 def test_status_strings(pkg):

@@ -93,3 +93,22 @@ def test_other_workloads_report_failures(monkeypatch):
     res = b.other_workloads(argparse.Namespace(steps=5, warmup=3, solve_grid="576,576,768"))
     assert res == {"solve_384x193x384": {"error": "RuntimeError: no device"},
                    "ensemble_48_runs": {"error": "RuntimeError: no device"}}
+
+
+def test_gpus_n_launches_n_ranks():
+    """``bench.py --gpus 2`` started without torchrun starts two ranks itself
+    (gloo here, no device work) and reports n_gpus = 2."""
+    import json
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--check-launch"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["n_gpus"] == 2 and line["ranks_joined"] == 2
+
+
+def test_gpus_n_must_match_world_size():
+    env = dict(os.environ, RANK="0", WORLD_SIZE="2", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "3", "--check-launch"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "WORLD_SIZE=2" in r.stderr

@@ -223,7 +223,7 @@ def test_init_aux_matrix_and_solve(pkg, mx, my, mz):
     R = rng_spec(sz, 11, sz.nz)
     t = spec_tensor(R, sz)
     torch.cuda.synchronize()
-    ctx.solve_eq(iv.data_ptr(), t.data_ptr(), sz.nz, sz.mz * 16)
+    ctx.solve_eq(iv.data_ptr(), t.data_ptr(), sz.nz, sz.mz * 16)  # device buffers
     ctx.synchronize()
     ref = np.einsum("yxij,yxj->yxi", gv, R)
     assert rel(t.cpu().numpy()[..., :sz.nz], ref) < 1e-13

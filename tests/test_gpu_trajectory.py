@@ -1,0 +1,128 @@
+"""FP64 trajectories against the oracle on the workloads' own grids.
+
+The oracle is the reference's algorithm in FP64 NumPy: it multiplies by
+explicit inverses, as source/solver.cpp:107-123 does.  The device solves the
+same collocation systems in banded integrated form.  The tolerance of each
+comparison is 1e-12 relative L2, or twice the oracle's own rounding floor at
+that step where that floor is higher: the spread between the oracle with
+explicit inverses and the oracle with LU solves, both correct restatements
+of the reference, which no third correct solver can be expected to beat.
+Errors are reported per component of getUVW (source/velocity.cu:90-170):
+u (streamwise), v_span, w (wall-normal velocity), omega_x, omega_y (span),
+omega_z (wall-normal vorticity), in the reference's axis names.
+
+* 48x48x128 (32x33x32 modes), U = y, Re 1300, Ro 0.1, dt 0.005, 100 steps,
+  oracle live, every pencil;
+* 192x192x256 (128x65x128 modes), Poiseuille U = 1 - y^2, Re 8400 (Re_b 5600
+  in bulk units), dt 0.002, 150 steps, against tests/golden/traj_config1.npz
+  (256 sampled pencils at steps 1, 2, 10, 50, 100, 150; full-field norms at
+  every step).  The reference's algorithm is unstable at these parameters
+  (the state overflows between steps 150 and 160, in the oracle as on the
+  device), so the workload's 200 steps have no finite end state;
+* 384x384x512 (256x129x256 modes), Couette, Re 3000, Ro 0.02, dt 0.001, 3
+  steps, against tests/golden/traj_config2.npz.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import rpcf_oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+NAMES = ("u", "v_span", "w", "omega_x", "omega_y", "omega_z")
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
+
+
+def _components(V, Om, ky, kx, sz):
+    return O.get_uvw_pencils(V, Om, ky, kx, sz, 2.0, 1.0)
+
+
+def _check(tag, step, dev, ref, spread, parity_log):
+    errs = [_rel(d, r) for d, r in zip(dev, ref)]
+    tol = [max(1e-12, 2.0 * s) for s in spread]
+    parity_log.append(f"{tag} step {step}: " + " ".join(
+        f"{n}={e:.1e}(tol {t:.0e})" for n, e, t in zip(NAMES, errs, tol)))
+    bad = [(n, e, t) for n, e, t in zip(NAMES, errs, tol) if not e <= t]
+    assert not bad, (tag, step, bad)
+
+
+def test_config0_100_steps_fp64(pkg, parity_log):
+    p = O.Params(48, 48, 128, Re=1300.0, Ro=0.1, dt=0.005, prof=(0.0, 1.0, 0.0))
+    sz = O.Sizes(48, 48, 128)
+    V0, O0 = pkg.seeded_state(sz.nx, sz.nz, sz.ny, 4.0, 2.0, 0.05, 0)
+    snaps = (1, 2, 10, 50, 100)
+    ref = {}
+    for solver in ("inverse", "lu"):
+        pb = O.Problem(p)
+        pb.solver = solver
+        pb.set_state(V0, O0)
+        pb.bootstrap()
+        for k in range(1, 101):
+            pb.step()
+            if k in snaps:
+                ref[solver, k] = (pb.V.copy(), pb.O.copy())
+    ctx = pkg.Context(pkg.make_params(48, 48, 128, Re=1300.0, Ro=0.1, dt=0.005, U=(0.0, 1.0, 0.0)))
+    ctx.set_state(V0, O0)
+    ctx.bootstrap()
+    ky, kx = np.meshgrid(np.arange(sz.ny), np.arange(sz.hnx), indexing="ij")
+    ky, kx = ky.ravel(), kx.ravel()
+    flat = lambda a: a.reshape(-1, sz.nz)  # noqa: E731
+    for k in range(1, 101):
+        ctx.step(1)
+        if k in snaps:
+            V, Om = ctx.get_state()
+            dev = _components(flat(V), flat(Om), ky, kx, sz)
+            ri = _components(flat(ref["inverse", k][0]), flat(ref["inverse", k][1]), ky, kx, sz)
+            rl = _components(flat(ref["lu", k][0]), flat(ref["lu", k][1]), ky, kx, sz)
+            spread = [_rel(a, b) for a, b in zip(ri, rl)]
+            _check("48x48x128 U=y", k, dev, ri, spread, parity_log)
+    ctx.close()
+
+
+def _fixture_run(pkg, name, parity_log):
+    path = os.path.join(GOLDEN, f"traj_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"{path} not generated")
+    f = np.load(path)
+    mx, my, mz = int(f["mx"]), int(f["my"]), int(f["mz"])
+    sz = O.Sizes(mx, my, mz)
+    prof = tuple(float(x) for x in f["prof"])
+    V0, O0 = pkg.seeded_state(sz.nx, sz.nz, sz.ny, 4.0, 2.0, float(f["amp"]), int(f["seed"]))
+    ctx = pkg.Context(pkg.make_params(mx, my, mz, Re=float(f["Re"]), Ro=float(f["Ro"]),
+                                      dt=float(f["dt"]), U=prof))
+    ctx.set_state(V0, O0)
+    ctx.bootstrap()
+    ky, kx = f["ky"], f["kx"]
+    steps = [int(s) for s in f["steps"]]
+    nsteps = int(f["nsteps"])
+    worst_norm = 0.0
+    for k in range(1, nsteps + 1):
+        ctx.step(1)
+        V, Om = ctx.get_state()
+        worst_norm = max(worst_norm, abs(np.linalg.norm(V) / f["norm_V"][k - 1] - 1),
+                         abs(np.linalg.norm(Om) / f["norm_O"][k - 1] - 1))
+        if k in steps:
+            i = steps.index(k)
+            dev = _components(V[ky, kx], Om[ky, kx], ky, kx, sz)
+            ref = _components(f["V"][i], f["O"][i], ky, kx, sz)
+            _check(f"{mx}x{my}x{mz}", k, dev, ref, f["spread"][i], parity_log)
+    norm_tol = max(1e-12, 2.0 * float(np.max(f["spread"][-1])))
+    parity_log.append(f"{mx}x{my}x{mz}: full-field L2 norms of v, omega_y over all {nsteps} "
+                      f"steps within {worst_norm:.1e} relative (tol {norm_tol:.0e})")
+    assert worst_norm <= norm_tol
+    ctx.close()
+
+
+def test_config1_poiseuille_150_steps_fp64(pkg, parity_log):
+    _fixture_run(pkg, "config1", parity_log)
+
+
+def test_config2_couette_fp64(pkg, parity_log):
+    _fixture_run(pkg, "config2", parity_log)

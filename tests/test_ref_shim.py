@@ -1,41 +1,44 @@
-"""The drop-in boundary against the reference's own declarations.
+"""The drop-in boundary against the reference's own driver and declarations.
 
 gpu-spectral-channel-dns_b200/shim/ref_shim.cu defines the reference's
-hot-path entry points (initFFT, transform_3d_one, transform, cuda_transpose,
-cheby_s2p/p2s, getUVW, computeLambVector, rhsNonlinear, solveEq,
-initAuxMatrix, nextStep, initFlow, output_velocity, write/read_recover_data,
-launch_subthread, synchronizeGPUsolver) over the C ABI.  Compiled here
-against the reference's include/ directory, every definition must match the
-reference's declaration, and linked against libdnsb200.so with no undefined
-symbol, every ABI call must resolve.  Skipped where the reference's headers
-are absent (REF_INCLUDE overrides their location).
+hot-path entry points and the set-up calls of its driver over the C ABI.
+gpu-spectral-channel-dns_b200/shim/build_ref_main.py compiles it against the
+reference's include/ directory (every definition must match the reference's
+declaration) and links it with the reference's unchanged main_loop.cpp,
+operation.cpp, data.cpp and transform_multi_gpu.cpp and with libdnsb200.so into
+two executables, with --no-undefined: every symbol the reference's driver
+needs resolves, and none is defined twice.  Skipped where the reference's
+sources are absent (REFERENCE_DIR names their location).
 """
+import importlib.util
 import os
-import shutil
 import subprocess
 
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INCLUDE = os.environ.get("REF_INCLUDE", "/root/reference/include")
-SHIM = os.path.join(ROOT, "gpu-spectral-channel-dns_b200", "shim", "ref_shim.cu")
-LIBDIR = os.path.join(ROOT, "gpu-spectral-channel-dns_b200")
+PKG = os.path.join(ROOT, "gpu-spectral-channel-dns_b200")
 
 
-def test_shim_compiles_against_reference_headers_and_links(tmp_path):
-    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    if not os.path.isdir(REF_INCLUDE) or not os.path.exists(nvcc):
-        pytest.skip("reference headers or nvcc not available")
-    if not os.path.exists(os.path.join(LIBDIR, "libdnsb200.so")):
+def _recipe():
+    spec = importlib.util.spec_from_file_location("build_ref_main",
+                                                  os.path.join(PKG, "shim", "build_ref_main.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def test_reference_driver_links_against_the_shim(tmp_path):
+    m = _recipe()
+    if m.reference_dir() is None:
+        pytest.skip("the reference's sources are not present")
+    if not os.path.exists(os.path.join(PKG, "libdnsb200.so")):
         pytest.skip("libdnsb200.so not built")
-    obj = str(tmp_path / "ref_shim.o")
-    r = subprocess.run([nvcc, "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "2464",
-                        "-gencode", "arch=compute_100a,code=sm_100a", "-c", SHIM,
-                        "-I", REF_INCLUDE, "-I", os.path.join(ROOT, "include"), "-o", obj],
-                       capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stderr[-3000:]
-    cudalib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "lib64")
-    r = subprocess.run(["g++", "-shared", "-o", str(tmp_path / "libshim.so"), obj, "-L", LIBDIR,
-                        "-ldnsb200", "-L", cudalib, "-lcudart", "-Wl,--no-undefined"],
-                       capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stderr[-3000:]
+    exes = m.build(str(tmp_path))
+    assert exes and all(os.access(e, os.X_OK) for e in exes)
+    # the executables name the reference's and the library's entry points
+    syms = subprocess.run(["nm", "-C", exes[0]], capture_output=True, text=True).stdout
+    for name in ("run_simulation()", "RPCF_Paras::read_para", "nextStep(problem&)", "initFlow(problem&)",
+                 "get_rhs_v(problem&)", "solveEq(", "allocHostMemory(problem&)", "allocDeviceMem(problem&)"):
+        assert name in syms, name
+    assert "U dns_step" in syms.replace("                 U", " U")
