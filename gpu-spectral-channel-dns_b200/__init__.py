@@ -8,5 +8,6 @@ from .abi import (  # noqa: F401
     BACKWARD, DEVICE, FORWARD, HOST, NO_PADDING, PADDING, PREC_FP64, PREC_MIXED,
     Context, DnsError, DnsParams, EXPORTS, LIB_PATH, load_library, make_params,
     read_parameter_file, step_many, SLAB_PENCILS, SLAB_PLANES, slab_ranges, slab_segments,
+    PASS_Y3, Y3_FFT, Y3_TENSOR,
 )
 from .seed import seeded_state  # noqa: F401

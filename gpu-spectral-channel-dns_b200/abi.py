@@ -31,8 +31,12 @@ EXPORTS = [
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
     "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
     "dns_nonlinear", "dns_rhs_v", "dns_rhs_omega", "dns_rhs_mean", "dns_operator_matrices",
-    "dns_operator_tables", "dns_set_wait_limit",
+    "dns_operator_tables", "dns_set_wait_limit", "dns_set_variant", "dns_get_variant",
+    "dns_autotune",
 ]
+
+PASS_Y3, NUM_PASSES, MAX_VARIANTS = 0, 1, 4
+Y3_FFT, Y3_TENSOR = 0, 1
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1
 
@@ -125,6 +129,9 @@ def load_library(path: str | None = None):
         "dns_operator_matrices": [vp, vp, vp, i],
         "dns_operator_tables": [vp, vp, vp, vp, vp, vp, vp],
         "dns_set_wait_limit": [vp, C.c_longlong],
+        "dns_set_variant": [vp, i, i],
+        "dns_get_variant": [vp, i, C.POINTER(C.c_int)],
+        "dns_autotune": [vp, C.POINTER(C.c_double)],
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
         "dns_step_many": [C.POINTER(vp), i, i],
@@ -366,6 +373,22 @@ class Context:
     def rhs_mean(self, u0, lx0, lx0_p, w0, lz0, lz0_p, where=DEVICE):
         self._call("dns_rhs_mean", C.c_void_p(u0), C.c_void_p(lx0), C.c_void_p(lx0_p),
                    C.c_void_p(w0), C.c_void_p(lz0), C.c_void_p(lz0_p), int(where))
+
+    def set_variant(self, pass_, variant):
+        self._call("dns_set_variant", int(pass_), int(variant))
+
+    def get_variant(self, pass_):
+        v = C.c_int()
+        self._call("dns_get_variant", int(pass_), C.byref(v))
+        return v.value
+
+    def autotune(self):
+        """Time every available kernel variant, keep the fastest; returns
+        {pass: {variant: ms}} for the available variants."""
+        ms = (C.c_double * (NUM_PASSES * MAX_VARIANTS))()
+        self._call("dns_autotune", ms)
+        return {p: {v: ms[p * MAX_VARIANTS + v] for v in range(MAX_VARIANTS) if ms[p * MAX_VARIANTS + v] >= 0}
+                for p in range(NUM_PASSES)}
 
     def set_wait_limit(self, cycles=1 << 31):
         """Bound of the staging waits (SM cycles); negative: give up at once."""

@@ -166,7 +166,11 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
   mark();
-  if ((e = launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st))) return e;
+  if (std::is_same<C, float2>::value && c->variant[DNS_PASS_Y3] == DNS_Y3_TENSOR)
+    e = launch_y3tc(b.V, b.O, F6p, g, c->ph, c->y3tc_tab, c->status, c->st);
+  else
+    e = launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st);
+  if (e) return e;
   mark();
   if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status))) return e;
   mark();
@@ -384,7 +388,8 @@ dns_status dns_destroy(dns_ctx* c) {
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
-                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->rhs_io, c->nl_io, c->eq_io, c->probe, c->status};
+                  c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->rhs_io, c->nl_io, c->eq_io, c->probe, c->status,
+                  c->y3tc_tab};
   for (void* q : ptrs) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -574,6 +579,94 @@ dns_status dns_set_wait_limit(dns_ctx* c, long long cycles) {
     c->graph = nullptr;
   }
   return DNS_OK;
+}
+
+namespace {
+bool variant_available(const dns_ctx* c, int pass, int v) {
+  if (pass == DNS_PASS_Y3) {
+    if (v == DNS_Y3_FFT) return true;
+    if (v == DNS_Y3_TENSOR) return c->P.precision == DNS_PREC_MIXED && c->g.Ny == 129 && c->g.Py == 257;
+  }
+  return false;
+}
+}  // namespace
+
+dns_status dns_set_variant(dns_ctx* c, int pass, int v) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  if (pass < 0 || pass >= DNS_NUM_PASSES) return fail(DNS_ERR_ARG, "unknown pass");
+  if (!variant_available(c, pass, v)) return fail(DNS_ERR_ARG, "variant not available for this context");
+  CK(cudaSetDevice(c->P.device));
+  CK(cudaStreamSynchronize(c->st));
+  if (pass == DNS_PASS_Y3 && v == DNS_Y3_TENSOR && !c->y3tc_tab) {
+    std::vector<uint32_t> w(y3tc_table_words());
+    y3tc_table(w.data());
+    CK(c->alloc(&c->y3tc_tab, w.size()));
+    CK(cudaMemcpy(c->y3tc_tab, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+  }
+  if (c->variant[pass] != v && c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  c->variant[pass] = v;
+  return DNS_OK;
+}
+
+dns_status dns_get_variant(const dns_ctx* c, int pass, int* v) {
+  if (!c || !v) return fail(DNS_ERR_ARG, "null argument");
+  if (pass < 0 || pass >= DNS_NUM_PASSES) return fail(DNS_ERR_ARG, "unknown pass");
+  *v = c->variant[pass];
+  return DNS_OK;
+}
+
+dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]) {
+  if (!c) return fail(DNS_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->P.device));
+  CK(cudaStreamSynchronize(c->st));
+  if (ms)
+    for (int i = 0; i < DNS_NUM_PASSES * DNS_MAX_VARIANTS; ++i) ms[i] = -1.0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  dns_status st = DNS_OK;
+  // y3 reads the state and writes only the transform buffer: each candidate
+  // is timed on the context's own buffers (1 warm-up + 5 launches)
+  {
+    const DnsGeom& g = c->g;
+    PencilArr F6p{c->F6, c->PyS, g.H * c->PyS};
+    double best = 1e300;
+    int pick = c->variant[DNS_PASS_Y3];
+    for (int v = 0; v < DNS_MAX_VARIANTS && st == DNS_OK; ++v) {
+      if (!variant_available(c, DNS_PASS_Y3, v)) continue;
+      if (v == DNS_Y3_TENSOR && !c->y3tc_tab) {
+        const int keep = c->variant[DNS_PASS_Y3];
+        if ((st = dns_set_variant(c, DNS_PASS_Y3, v)) != DNS_OK) break;
+        if ((st = dns_set_variant(c, DNS_PASS_Y3, keep)) != DNS_OK) break;
+      }
+      auto run = [&]() -> cudaError_t {
+        if (c->P.precision == DNS_PREC_MIXED) {
+          if (v == DNS_Y3_TENSOR) return launch_y3tc(c->V, c->O, F6p, g, c->ph, c->y3tc_tab, c->status, c->st);
+          return launch_y3<float2>(c->V, c->O, F6p, g, c->ph, c->fyP_f.tab(), c->status, c->st);
+        }
+        return launch_y3<double2>(c->V, c->O, F6p, g, c->ph, c->fyP_d.tab(), c->status, c->st);
+      };
+      cudaError_t e = run();
+      if (!e) e = cudaEventRecord(e0, c->st);
+      for (int i = 0; i < 5 && !e; ++i) e = run();
+      if (!e) e = cudaEventRecord(e1, c->st);
+      if (!e) e = cudaEventSynchronize(e1);
+      float t = 0.f;
+      if (!e) e = cudaEventElapsedTime(&t, e0, e1);
+      if (e) { st = fail(DNS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e)); break; }
+      st = check_status(c);
+      const double per = t / 5.0;
+      if (ms) ms[DNS_PASS_Y3 * DNS_MAX_VARIANTS + v] = per;
+      if (per < best) { best = per; pick = v; }
+    }
+    if (st == DNS_OK) st = dns_set_variant(c, DNS_PASS_Y3, pick);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
 }
 
 dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps) {

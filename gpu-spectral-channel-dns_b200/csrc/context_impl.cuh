@@ -51,6 +51,8 @@ struct dns_ctx {
   int* probe = nullptr;         // dns_check_state: set when the state holds NaN or Inf
   int* status = nullptr;
   bool have_state = false, booted = false, wall_ready = false;
+  int variant[DNS_NUM_PASSES] = {};  // kernel variant of each tunable pass
+  uint32_t* y3tc_tab = nullptr;      // Chebyshev table of the tensor-core y3 pass
   cudaGraphExec_t graph = nullptr;
 
   template <typename T> cudaError_t alloc(T** p, size_t n) {

@@ -31,3 +31,10 @@ template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
                       double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
                       PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st);
+// tensor-core form of y3 (y3tc.cu): Ny = 129, FP32 output; cudaErrorNotSupported
+// for other sizes
+cudaError_t launch_y3tc(const double2* V, const double2* O, PencilArr out, DnsGeom g, PhysParams ph,
+                        const uint32_t* atab, int* status, cudaStream_t st);
+// its Chebyshev table (TF32 hi/lo words, y3tc_table_words() of them)
+size_t y3tc_table_words();
+void y3tc_table(uint32_t* w);

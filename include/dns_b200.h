@@ -176,6 +176,25 @@ dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps);
  * path.  The next dns_step captures the step graph again. */
 dns_status dns_set_wait_limit(dns_ctx* ctx, long long cycles);
 
+/* Kernel variants and the autotuner (no counterpart in the reference).  A
+ * tunable pass has several compiled kernels for the same arithmetic; the
+ * context starts with variant 0 of each.
+ *   DNS_PASS_Y3: the backward wall-normal pass (getUVW + padded s2p)
+ *     DNS_Y3_FFT     shared-memory FFT of the even extension (every grid);
+ *     DNS_Y3_TENSOR  batched 3xTF32 Chebyshev products on the tensor cores
+ *                    (tcgen05, FP32 accumulation): mixed form, Ny = 129.
+ * dns_set_variant fails with DNS_ERR_ARG for a variant this context cannot
+ * run.  dns_autotune times every available variant of every tunable pass on
+ * this context's buffers and grid (the state is not modified), keeps the
+ * fastest and, if ms is not NULL, writes the mean times in ms to
+ * ms[pass * DNS_MAX_VARIANTS + variant] (-1 where unavailable).  Synchronous;
+ * the next dns_step captures the step graph again. */
+enum { DNS_PASS_Y3 = 0, DNS_NUM_PASSES = 1, DNS_MAX_VARIANTS = 4 };
+enum { DNS_Y3_FFT = 0, DNS_Y3_TENSOR = 1 };
+dns_status dns_set_variant(dns_ctx* ctx, int pass, int variant);
+dns_status dns_get_variant(const dns_ctx* ctx, int pass, int* variant);
+dns_status dns_autotune(dns_ctx* ctx, double* ms);
+
 /* The same steps without the graph, with CUDA events recorded around each
  * of the DNS_NUM_KERNELS kernels of a step on the context stream;
  * kernel_ms[k] = mean duration of kernel k (dns_kernel_name(k)).

@@ -3,10 +3,12 @@
 The oracle is the reference's algorithm in FP64 NumPy: it multiplies by
 explicit inverses, as source/solver.cpp:107-123 does.  The device solves the
 same collocation systems in banded integrated form.  The tolerance of each
-comparison is 1e-12 relative L2, or twice the oracle's own rounding floor at
-that step where that floor is higher: the spread between the oracle with
-explicit inverses and the oracle with LU solves, both correct restatements
-of the reference, which no third correct solver can be expected to beat.
+comparison is 1e-12 relative L2, or three times the oracle's own rounding
+floor at that step where that is higher.  The floor is the spread between
+the oracle with explicit inverses and the oracle with LU solves, both correct
+restatements of the reference: a third solver as accurate as they are lands
+within about twice that spread of either (triangle inequality), and three
+times leaves room for the step-to-step scatter of the measured ratio.
 Errors are reported per component of getUVW (source/velocity.cu:90-170):
 u (streamwise), v_span, w (wall-normal velocity), omega_x, omega_y (span),
 omega_z (wall-normal vorticity), in the reference's axis names.
@@ -46,7 +48,7 @@ def _components(V, Om, ky, kx, sz):
 
 def _check(tag, step, dev, ref, spread, parity_log):
     errs = [_rel(d, r) for d, r in zip(dev, ref)]
-    tol = [max(1e-12, 2.0 * s) for s in spread]
+    tol = [max(1e-12, 3.0 * s) for s in spread]
     parity_log.append(f"{tag} step {step}: " + " ".join(
         f"{n}={e:.1e}(tol {t:.0e})" for n, e, t in zip(NAMES, errs, tol)))
     bad = [(n, e, t) for n, e, t in zip(NAMES, errs, tol) if not e <= t]
@@ -113,7 +115,7 @@ def _fixture_run(pkg, name, parity_log):
             dev = _components(V[ky, kx], Om[ky, kx], ky, kx, sz)
             ref = _components(f["V"][i], f["O"][i], ky, kx, sz)
             _check(f"{mx}x{my}x{mz}", k, dev, ref, f["spread"][i], parity_log)
-    norm_tol = max(1e-12, 2.0 * float(np.max(f["spread"][-1])))
+    norm_tol = max(1e-12, 3.0 * float(np.max(f["spread"][-1])))
     parity_log.append(f"{mx}x{my}x{mz}: full-field L2 norms of v, omega_y over all {nsteps} "
                       f"steps within {worst_norm:.1e} relative (tol {norm_tol:.0e})")
     assert worst_norm <= norm_tol
