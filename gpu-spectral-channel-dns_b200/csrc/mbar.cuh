@@ -48,13 +48,17 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
       : "memory");
 }
 // A negative limit gives up at once (the test hook for the timeout path).
+// The status word (global memory, a round trip of a microsecond or so) is
+// read only every 64th retry, so that a phase that completes is seen by the
+// next try_wait rather than after a pending global load.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit,
                                                   const int* status) {
   if (limit < 0) return false;
+  if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
+  for (unsigned n = 1;; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
     if (clock64() - t0 > limit) return false;
-    if (status && (*(volatile const int*)status & 1)) return false;
+    if (status && (n & 63u) == 0 && (*(volatile const int*)status & 1)) return false;
   }
-  return true;
 }

@@ -97,11 +97,16 @@ __device__ __forceinline__ uint32_t b_off(int n, int kc) {
   return (uint32_t)kc * TC_KC_BYTES + (uint32_t)(n >> 3) * 128u + (uint32_t)(n & 7) * 16u;
 }
 
+// FP32 bits -> TF32 bits, round to nearest with ties away from zero (the
+// rounding of cvt.rna.tf32.f32) on the integer pipe: add half an ulp of the
+// 10-bit mantissa, clear the 13 low bits
+__device__ __forceinline__ uint32_t tf32_bits(uint32_t u) { return (u + 0x1000u) & ~0x1FFFu; }
+
 // x = hi + lo to FP32 rounding (~2^-24 |x| beyond the 2^-22 of the TF32 pair)
 __device__ __forceinline__ void split_f(double x, uint32_t& hi, uint32_t& lo) {
   const float xf = (float)x;
-  hi = to_tf32(xf);
-  lo = to_tf32(xf - __uint_as_float(hi));
+  hi = tf32_bits(__float_as_uint(xf));
+  lo = tf32_bits(__float_as_uint(xf - __uint_as_float(hi)));
 }
 
 __device__ __forceinline__ float2 cmul_i(float2 a, float s) { return make_float2(-a.y * s, a.x * s); }  // i s a
