@@ -293,6 +293,15 @@ def run_ours(args, rank, world):
     c64 = make(pkg.PREC_FP64)
     setup_s = time.perf_counter() - t_setup
     cmx = make(pkg.PREC_MIXED)
+    # the autotuner times every compiled variant of each tunable pass on this
+    # grid and keeps the fastest (per context, before any timed step)
+    names = {pkg.PASS_Y3: ("y3_uvw_s2p", {pkg.Y3_FFT: "fft", pkg.Y3_TENSOR: "tensor_core_3xtf32"})}
+    tune = {}
+    for tag, ctx in (("mixed", cmx), ("fp64", c64)):
+        times = ctx.autotune()
+        tune[tag] = {names[p][0]: {"ms": {names[p][1][v]: round(t, 4) for v, t in vt.items()},
+                                   "picked": names[p][1][ctx.get_variant(p)]}
+                     for p, vt in times.items()}
     # accuracy of the mixed form against the FP64 form: (1) accumulated over
     # ACC steps from the seeded state; (2) per step: both forms advance one
     # step from the FP64 state and history reached after ACC steps
@@ -349,7 +358,7 @@ def run_ours(args, rank, world):
     geo = dict(Kx=cmx.Kx, Nz=cmx.Nz, Ny=cmx.Ny, Py=cmx.Py, Pz=cmx.Pz)
     mem = cmx.memory_bytes()
     cmx.close()
-    return dict(ms64=ms64, msmx=msmx, err=err, acc=acc, acc_steps=ACC,
+    return dict(ms64=ms64, msmx=msmx, err=err, acc=acc, acc_steps=ACC, autotune=tune,
                 kms64=kms64, kmsmx=kmsmx,
                 e2e_ms=e2e_ms, geo=geo, clocks=clk.summary(), setup_s=setup_s, mem=mem,
                 state_bytes=2 * geo["Kx"] * geo["Nz"] * geo["Ny"] * 16)
@@ -366,12 +375,15 @@ def run_one(args):
     ctx = pkg.Context(pkg.make_params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"],
                                       dt=CFG["dt"], precision=prec, device=0))
     ctx.set_state(V0, O0)
+    ctx.autotune()
+    variant = ctx.get_variant(pkg.PASS_Y3)
     ctx.bootstrap()
     ctx.step(args.warmup)
     kms = ctx.step_profiled(args.steps)
     ctx.synchronize()
     ctx.close()
-    return {"only": args.only, "config": args.config, "kernel_ms": {k: round(v, 4) for k, v in kms.items()}}
+    return {"only": args.only, "config": args.config, "y3_variant": variant,
+            "kernel_ms": {k: round(v, 4) for k, v in kms.items()}}
 
 
 ENSEMBLE_SIZES = [(48, 48, 128), (96, 96, 192), (144, 144, 256), (192, 192, 384)]
@@ -699,6 +711,7 @@ def main():
             "step_frac_of_peak": round(step_bytes_mx / (r["msmx"] * 1e-3) / 1e9 / peak, 4),
             "step_bytes_algorithmic": step_bytes_mx,
             "factor_bytes_per_step": factor_bytes(r["geo"]),
+            "autotune": r["autotune"],
             "kernel_ms": {"fp64": {k: round(v, 4) for k, v in r["kms64"].items()},
                           "mixed": {k: round(v, 4) for k, v in r["kmsmx"].items()}},
             "e2e": {"value": round(replica_value(n, r["e2e_ms"]), 2), "unit": "steps/s",

@@ -208,6 +208,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (lane == 0) {
       const uint32_t idesc = tc_idesc_tf32(TC_NH, TC_N);
       const uint32_t bbase = smem_u32(bbuf);
+      // descriptors of the K steps of buffer 0 (buffer 1: + TC_BUF_BYTES >> 4
+      // in the start-address field, which stays below 2^14)
+      uint64_t dsc[2][2][TC_KP / 8];  // [par][hi|lo][s]
+#pragma unroll
+      for (int par = 0; par < 2; ++par)
+#pragma unroll
+        for (int hl = 0; hl < 2; ++hl)
+#pragma unroll
+          for (int s = 0; s < TC_KP / 8; ++s)
+            dsc[par][hl][s] = tc_sdesc(bbase + (uint32_t)(par * 2 + hl) * TC_PART_BYTES +
+                                           (uint32_t)(2 * s) * TC_KC_BYTES,
+                                       TC_KC_BYTES, 128);
       long long it = 0;
       for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
         const int b = (int)(it & 1);
@@ -215,20 +227,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (!tc_wait(&bs->full_b[b], use & 1u, bs, status)) break;
         if (!tc_wait(&bs->empty_d, ((uint32_t)it & 1u) ^ 1u, bs, status)) break;
         tc_fence_after();
-        for (int par = 0; par < 2; ++par) {
-          const uint32_t d = tbase + TC_COL_D + (uint32_t)(par * TC_N);
-          const uint32_t pb_hi = bbase + (uint32_t)b * TC_BUF_BYTES + (uint32_t)(par * 2) * TC_PART_BYTES;
-          const uint32_t pb_lo = pb_hi + TC_PART_BYTES;
-          for (int s = 0; s < TC_KP / 8; ++s) {
-            const uint32_t a_hi = tbase + TC_COL_A + (uint32_t)(par * 128 + 8 * s);
-            const uint32_t a_lo = a_hi + 64;
-            const uint64_t bh = tc_sdesc(pb_hi + (uint32_t)(2 * s) * TC_KC_BYTES, TC_KC_BYTES, 128);
-            const uint64_t bl = tc_sdesc(pb_lo + (uint32_t)(2 * s) * TC_KC_BYTES, TC_KC_BYTES, 128);
-            mma_tf32_ts(d, a_hi, bh, idesc, s > 0 ? 1u : 0u);
-            mma_tf32_ts(d, a_hi, bl, idesc, 1u);
-            mma_tf32_ts(d, a_lo, bh, idesc, 1u);
-          }
-        }
+        // the even and odd products alternate, so that consecutive MMAs
+        // accumulate into different tensor-memory tiles
+        const uint64_t boff = (uint64_t)(b * (TC_BUF_BYTES >> 4));
+#pragma unroll
+        for (int s = 0; s < TC_KP / 8; ++s)
+#pragma unroll
+          for (int k3 = 0; k3 < 3; ++k3)
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+              const uint32_t d = tbase + TC_COL_D + (uint32_t)(par * TC_N);
+              const uint32_t a = tbase + TC_COL_A + (uint32_t)(par * 128 + 8 * s + (k3 == 2 ? 64 : 0));
+              const uint64_t bd = dsc[par][k3 == 1 ? 1 : 0][s] + boff;
+              mma_tf32_ts(d, a, bd, idesc, (s > 0 || k3 > 0) ? 1u : 0u);
+            }
         umma_commit(&bs->empty_b[b]);
         umma_commit(&bs->full_d);
       }
