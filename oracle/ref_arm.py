@@ -1,9 +1,20 @@
-"""Reference arm of bench.py: the reference's step algorithm on host cores.
+"""Reference arm of bench.py.
 
 TEST / BASELINE INFRASTRUCTURE ONLY (called by ``bench.py --impl
-reference``).  The reference program itself cannot be built here (its solve
-needs Eigen, which is absent), so this times the oracle's FP64 NumPy port of
-the reference's step, with all host threads, on a bounded sample per step:
+reference``).
+
+Where the reference program has been built from its own sources
+(oracle/_ref/ref_program, oracle/ref_build/build_ref_program.py) the arm runs
+it: its own run_simulation, cuFFT on the GPU for the nonlinear phase and
+OpenMP on every host core for the right-hand sides and the explicit-inverse
+solves, and reads its own per-step timer (source/main_loop.cpp:81-102) for
+every timed step.  The reference caps Ny at MAX_NZ = 100 (include/data.h:30),
+so it runs the bench workload's horizontal grid, flow and parameters at the
+largest wall-normal resolution it supports, 256 x 97 x 256 modes (mx, my, mz =
+384, 384, 384), a smaller problem than the 256 x 129 x 256 of the bench.
+
+Otherwise it times the oracle's FP64 NumPy port of the reference's step on
+one host core, on a bounded sample per step:
 
 * pencil phase (getUVW + padded s2p of six fields, padded p2s of three Lamb
   components, rhsNonlinear, no-pad s2p, CN right-hand sides, v and omega
@@ -87,9 +98,78 @@ def _plane_phase(args):
     return [np.fft.rfft2(L, axes=(-2, -1)) / (sz.mx * sz.my) for L in (lx, ly, lz)]
 
 
+REF_PROGRAM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "ref_program")
+
+
+def run_program(args, CFG, METRIC, max_timed=20):
+    """The reference program at 256 x 97 x 256 (mz = 384): W warm-up steps and
+    min(K, max_timed) timed steps of its own loop, its own event timer."""
+    import platform
+    import subprocess
+    import tempfile
+    mx, my, mz = CFG["mx"], CFG["my"], min(CFG["mz"], 384)
+    K = max(1, min(args.steps, max_timed))
+    W = args.warmup
+    base = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory(dir=base) as d:
+        os.makedirs(os.path.join(d, "input"))
+        os.makedirs(os.path.join(d, "run", "out"))
+        with open(os.path.join(d, "input", "parameter.txt"), "w") as f:
+            f.write(f"{mx} {my} {mz}\n4.0 2.0\n{CFG['Re']} {CFG['Ro']} {CFG['dt']}\n"
+                    f"0 1 {W + K} 1000000000 1000000000\nout/o\nout/r\n")
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_PROGRAM], cwd=os.path.join(d, "run"), env=env, capture_output=True, text=True,
+                           timeout=3000)
+        wall = time.perf_counter() - t0
+    steps = [float(x.split(":")[1]) for x in r.stdout.splitlines() if x.startswith("Time cost of current step:")]
+    # the reference never joins its worker thread: std::terminate at exit
+    # (status -6) after the last step is expected
+    if len(steps) != W + K or r.returncode not in (0, -6):
+        raise RuntimeError(f"reference program: status {r.returncode}, {len(steps)} of {W + K} steps; "
+                           f"{r.stderr[-500:]}")
+    timed = steps[W:]
+    step_s = float(np.mean(timed))
+    value = 1.0 / step_s
+    cpu = platform.processor() or ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                cpu = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    sample = (f"the reference program (its own sources, cuFFT nonlinear phase on the GPU, OpenMP right-hand "
+              f"sides and explicit-inverse solves on {cores} host threads, {cpu}) at 256x97x256 modes "
+              f"(mx,my,mz={mx},{my},{mz}; Ny capped at MAX_NZ = 100), rotating Couette Re {CFG['Re']:g}, Ro "
+              f"{CFG['Ro']:g}, dt {CFG['dt']:g}: {K} timed steps after {W} warm-up, its own per-step timer; "
+              f"whole run incl. set-up {wall:.0f} s")
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "steps/s",
+        "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": round(step_s * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "the reference's analytic initial field (initFlow)",
+        "config": {"workload": (f"rotating plane Couette 256x97x256 modes (mx,my,mz={mx},{my},{mz}), "
+                                f"Re {CFG['Re']:g}, Ro {CFG['Ro']:g}, dt {CFG['dt']:g}; the reference's "
+                                f"MAX_NZ = 100 rules out the bench's 256x129x256")},
+        "cpu_baseline": {"value": round(value, 4), "unit": "steps/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_seconds_timed": [round(x, 5) for x in timed],
+    }
+
+
 def run(args, CFG, METRIC):
-    from importlib import util as _u  # noqa: F401
-    threads = os.cpu_count() or 1
+    if os.path.exists(REF_PROGRAM):
+        return run_program(args, CFG, METRIC)
+    return run_port(args, CFG, METRIC)
+
+
+def run_port(args, CFG, METRIC):
+    # one host core: NumPy's element-wise work holds the interpreter, so a
+    # thread pool over the pencils gains nothing
+    threads = 1
     p = O.Params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"], dt=CFG["dt"])
     pb = O.Problem(p)
     sz = pb.sz
@@ -133,8 +213,8 @@ def run(args, CFG, METRIC):
     value = 1.0 / step_s
     sample_desc = (f"oracle FP64 NumPy port of the reference step at {CFG['mx']}x{CFG['my']}x{CFG['mz']} "
                    f"(mx,my,mz): pencil phase on {S} of {sz.ny * sz.hnx} pencils and plane phase on "
-                   f"{P} of {sz.pz} wall-normal planes per step, scaled; {threads} host threads; "
-                   "the reference program itself needs Eigen (absent) and is not built")
+                   f"{P} of {sz.pz} wall-normal planes per step, scaled; {threads} host thread; "
+                   "the reference program is not built on this host")
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "steps/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
