@@ -295,12 +295,11 @@ def run_ours(args, rank, world):
     cmx = make(pkg.PREC_MIXED)
     # the autotuner times every compiled variant of each tunable pass on this
     # grid and keeps the fastest (per context, before any timed step)
-    names = {pkg.PASS_Y3: ("y3_uvw_s2p", {pkg.Y3_FFT: "fft", pkg.Y3_TENSOR: "tensor_core_3xtf32"})}
     tune = {}
     for tag, ctx in (("mixed", cmx), ("fp64", c64)):
         times = ctx.autotune()
-        tune[tag] = {names[p][0]: {"ms": {names[p][1][v]: round(t, 4) for v, t in vt.items()},
-                                   "picked": names[p][1][ctx.get_variant(p)]}
+        tune[tag] = {pkg.PASS_NAMES[p]: {"ms": {pkg.VARIANT_NAMES[p][v]: round(t, 4) for v, t in vt.items()},
+                                         "picked": pkg.VARIANT_NAMES[p][ctx.get_variant(p)]}
                      for p, vt in times.items()}
     # accuracy of the mixed form against the FP64 form: (1) accumulated over
     # ACC steps from the seeded state; (2) per step: both forms advance one
@@ -376,13 +375,13 @@ def run_one(args):
                                       dt=CFG["dt"], precision=prec, device=0))
     ctx.set_state(V0, O0)
     ctx.autotune()
-    variant = ctx.get_variant(pkg.PASS_Y3)
+    variant = {pkg.PASS_NAMES[p]: pkg.VARIANT_NAMES[p][ctx.get_variant(p)] for p in range(pkg.NUM_PASSES)}
     ctx.bootstrap()
     ctx.step(args.warmup)
     kms = ctx.step_profiled(args.steps)
     ctx.synchronize()
     ctx.close()
-    return {"only": args.only, "config": args.config, "y3_variant": variant,
+    return {"only": args.only, "config": args.config, "variants": variant,
             "kernel_ms": {k: round(v, 4) for k, v in kms.items()}}
 
 
@@ -525,6 +524,8 @@ def run_solve(args):
         torch.cuda.synchronize()
         if i >= args.warmup:
             ms.append(e0.elapsed_time(e1))
+    # the last call's solutions against the operators themselves
+    res = ctx.solve_residual(bv.data_ptr(), bo.data_ptr(), wv.data_ptr(), wo.data_ptr(), Ny * 16)
     ctx.close()
     t = float(np.median(ms))
     H = Kx * Nz
@@ -532,6 +533,15 @@ def run_solve(args):
             "value": round(H / (t * 1e-3), 1), "unit": "pairs/s", "ms_per_call": round(t, 4),
             "pairs": H, "Ny": Ny, "steps": args.steps, "warmup": args.warmup,
             "rhs_and_solution_bytes": 4 * H * Ny * 16,
+            "residual": {"max_pencil_rel_v": float(f"{res[0]:.3e}"), "max_pencil_rel_omega": float(f"{res[1]:.3e}"),
+                         "rel_v": float(f"{res[2]:.3e}"), "rel_omega": float(f"{res[3]:.3e}"),
+                         "max_backward_err_v": float(f"{res[4]:.3e}"),
+                         "max_backward_err_omega": float(f"{res[5]:.3e}"),
+                         "definition": "||A x - b|| / ||b|| with A the reference's collocation operators; "
+                                       "backward error ||r||inf / (||A||inf ||x||inf + ||b||inf)"},
+            "graph": "one CUDA graph per call (prep, DCT-I, integration, banded solve of all pencils, finish)",
+            "l2": f"right-hand sides re-copied before each call (2 x {H * Ny * 16 / 1e6:.0f} MB"
+                  f"{', > L2' if 2 * H * Ny * 16 > 126e6 else ''})",
             "timing": "CUDA events on the library stream around each synchronous call, median"}
 
 
@@ -542,7 +552,8 @@ def other_workloads(args):
     import copy
     res = {}
     for name, fn, steps, keys in (
-            ("solve_384x193x384", run_solve, 5, ("metric", "value", "unit", "ms_per_call", "pairs", "timing")),
+            ("solve_384x193x384", run_solve, 5, ("metric", "value", "unit", "ms_per_call", "pairs", "residual",
+                                                  "graph", "timing")),
             ("ensemble_48_runs", run_ensemble, 10, ("metric", "value", "unit", "steps", "ms_all_runs_K_steps",
                                                     "one_after_another", "max_rel_l2_err_vs_own_fp64_run",
                                                     "clocks"))):

@@ -32,11 +32,21 @@ EXPORTS = [
     "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
     "dns_nonlinear", "dns_rhs_v", "dns_rhs_omega", "dns_rhs_mean", "dns_operator_matrices",
     "dns_operator_tables", "dns_set_wait_limit", "dns_set_variant", "dns_get_variant",
-    "dns_autotune",
+    "dns_autotune", "dns_solve_residual",
 ]
 
-PASS_Y3, NUM_PASSES, MAX_VARIANTS = 0, 1, 4
-Y3_FFT, Y3_TENSOR = 0, 1
+PASS_Y3, PASS_Y1, PASS_ZB, PASS_ZF, NUM_PASSES, MAX_VARIANTS = 0, 1, 2, 3, 4, 4
+Y3_FFT, Y3_TENSOR, Y3_BLOCK = 0, 1, 2
+Y1_WARP, Y1_BLOCK = 0, 1
+Z_TENSOR_COPY, Z_WARP, Z_BLOCK = 0, 1, 2
+# names of the tunable passes and their variants (bench and test reports)
+PASS_NAMES = {PASS_Y3: "y3_uvw_s2p", PASS_Y1: "y1_p2s_rhs", PASS_ZB: "zb_span_inverse", PASS_ZF: "zf_span_forward"}
+VARIANT_NAMES = {
+    PASS_Y3: {Y3_FFT: "warp_fft", Y3_TENSOR: "tensor_core_3xtf32", Y3_BLOCK: "block_fft"},
+    PASS_Y1: {Y1_WARP: "warp_fft", Y1_BLOCK: "block_fft"},
+    PASS_ZB: {Z_TENSOR_COPY: "warp_fft_tensor_copy", Z_WARP: "warp_fft", Z_BLOCK: "block_fft"},
+    PASS_ZF: {Z_TENSOR_COPY: "warp_fft_tensor_copy", Z_WARP: "warp_fft", Z_BLOCK: "block_fft"},
+}
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1
 
@@ -132,6 +142,7 @@ def load_library(path: str | None = None):
         "dns_set_variant": [vp, i, i],
         "dns_get_variant": [vp, i, C.POINTER(C.c_int)],
         "dns_autotune": [vp, C.POINTER(C.c_double)],
+        "dns_solve_residual": [vp, vp, vp, vp, vp, sz, i, C.POINTER(C.c_double)],
         "dns_init_aux_matrix": [vp, vp, vp, i],
         "dns_solve_wall": [vp, vp, vp, sz, i],
         "dns_step_many": [C.POINTER(vp), i, i],
@@ -420,6 +431,23 @@ class Context:
             self._call("dns_solve_wall", v.ctypes.data, omega.ctypes.data, tpitch, HOST)
         else:  # device pointers; 0 or None leaves that system alone
             self._call("dns_solve_wall", C.c_void_p(v or None), C.c_void_p(omega or None), tpitch, DEVICE)
+
+    def solve_residual(self, bv, bo, xv, xo, tpitch, where=DEVICE):
+        """(max per-pencil ||Ax-b||/||b|| of v, omega; the same over all
+        pencils; max backward error of v, omega)."""
+        out = (C.c_double * 6)()
+        arrs = (bv, bo, xv, xo)
+        if where == HOST:  # numpy arrays (Nz, Kx, tpitch/16) complex128
+            for a in arrs:
+                if not (isinstance(a, np.ndarray) and a.dtype == np.complex128 and a.ndim == 3
+                        and a.shape[:2] == (self.Nz, self.Kx) and a.shape[2] * 16 == tpitch
+                        and a.flags.c_contiguous):
+                    raise ValueError("host arrays must be C-contiguous (Nz, Kx, tpitch/16) complex128")
+            ptrs = [C.c_void_p(a.ctypes.data) for a in arrs]
+        else:
+            ptrs = [C.c_void_p(int(a)) for a in arrs]
+        self._call("dns_solve_residual", *ptrs, tpitch, int(where), out)
+        return tuple(out)
 
     def init_aux_matrix(self, inv_v, inv_o, where=DEVICE):
         if where == HOST:

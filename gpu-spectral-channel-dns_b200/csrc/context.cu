@@ -166,25 +166,36 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
   mark();
+  // the context's variant of each tunable pass; a variant these buffers do
+  // not allow (cudaErrorNotSupported, nothing launched) falls back to the
+  // automatic choice
+  auto var = [&](int pass, auto&& launch) {
+    cudaError_t r = launch(c->variant[pass]);
+    return r == cudaErrorNotSupported ? launch(VAR_AUTO) : r;
+  };
   if (std::is_same<C, float2>::value && c->variant[DNS_PASS_Y3] == DNS_Y3_TENSOR)
     e = launch_y3tc(b.V, b.O, F6p, g, c->ph, c->y3tc_tab, c->status, c->st);
   else
-    e = launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st);
+    e = var(DNS_PASS_Y3, [&](int v) { return launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st, v); });
   if (e) return e;
   mark();
-  if ((e = launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status))) return e;
+  if ((e = var(DNS_PASS_ZB, [&](int v) { return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v); })))
+    return e;
   mark();
   if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st))) return e;
   mark();
-  if ((e = launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status))) return e;
+  if ((e = var(DNS_PASS_ZF, [&](int v) { return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v); })))
+    return e;
   mark();
   const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
   const size_t nv = c->wd.nv, no = c->wd.no;
   const double* t0 = c->rtab;
   const RhsTabs tb{t0, t0 + 4 * nv, t0 + 4 * nv + 2 * no, t0 + 4 * nv + 2 * no + g.Ny,
                    t0 + 4 * nv + 2 * no + g.Ny + 5 * nv};
-  if ((e = launch_y1<C>(F3p, b.V, b.O, b.Nvp, b.Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(),
-                        boot, c->status, c->st)))
+  if ((e = var(DNS_PASS_Y1, [&](int v) {
+         return launch_y1<C>(F3p, b.V, b.O, b.Nvp, b.Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(), boot,
+                             c->status, c->st, v);
+       })))
     return e;
   mark();
   if (!boot)
@@ -200,6 +211,61 @@ cudaError_t enqueue(dns_ctx* c, int boot, cudaEvent_t* ev = nullptr, const StepB
   if (c->P.precision == DNS_PREC_MIXED)
     return enqueue_pipeline<float2>(c, boot, c->fz_f, c->fx_f, c->fyP_f, ev, b);
   return enqueue_pipeline<double2>(c, boot, c->fz_d, c->fx_d, c->fyP_d, ev, b);
+}
+
+// Whether variant v of a tunable pass runs as itself on this context's
+// step buffers (the launchers' probe: nothing is launched).
+template <typename C>
+bool probe_pass(const dns_ctx* c, int pass, int v, const DevFft<C>& fz, const DevFft<C>& fyP) {
+  const DnsGeom& g = c->g;
+  const long long H = g.H;
+  PencilArr F6p{c->F6, c->PyS, H * c->PyS};
+  RowArr G6r{c->G6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
+  RowArr G3r{c->F6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
+  PencilArr F3p{c->G6, c->PyS, H * c->PyS};
+  switch (pass) {
+    case DNS_PASS_Y3:
+      if (v == DNS_Y3_TENSOR)
+        return std::is_same<C, float2>::value && g.Ny == 129 && g.Py == 257;
+      return launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->status, c->st, v, true) == cudaSuccess;
+    case DNS_PASS_Y1: {
+      const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
+      const RhsTabs tb{};
+      return launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(), 0,
+                          c->status, c->st, v, true) == cudaSuccess;
+    }
+    case DNS_PASS_ZB:
+      return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
+    case DNS_PASS_ZF:
+      return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
+  }
+  return false;
+}
+bool variant_available(const dns_ctx* c, int pass, int v) {
+  if (pass < 0 || pass >= DNS_NUM_PASSES || v < 0 || v >= DNS_MAX_VARIANTS) return false;
+  if (c->P.precision == DNS_PREC_MIXED) return probe_pass<float2>(c, pass, v, c->fz_f, c->fyP_f);
+  return probe_pass<double2>(c, pass, v, c->fz_d, c->fyP_d);
+}
+// starting variants: the first each precision's order allows
+void default_variants(dns_ctx* c) {
+  const bool mixed = c->P.precision == DNS_PREC_MIXED;
+  static const int order_mixed[DNS_NUM_PASSES][3] = {
+      {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
+      {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}, {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}};
+  static const int order_fp64[DNS_NUM_PASSES][3] = {
+      {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
+      {DNS_Z_WARP, DNS_Z_BLOCK, -1}, {DNS_Z_WARP, DNS_Z_BLOCK, -1}};
+  for (int p = 0; p < DNS_NUM_PASSES; ++p) {
+    const int* ord = mixed ? order_mixed[p] : order_fp64[p];
+    c->variant[p] = ord[0];
+    for (int i = 0; i < 3 && ord[i] >= 0; ++i)
+      if (variant_available(c, p, ord[i])) { c->variant[p] = ord[i]; break; }
+  }
+}
+// the spanwise variant of the FP64 per-function entries: the context's own
+// in the FP64 form, else the block form
+int zvar64(const dns_ctx* c, int pass) {
+  return c->P.precision == DNS_PREC_FP64 ? c->variant[pass] : DNS_Z_BLOCK;
 }
 
 dns_status need_scratch(dns_ctx* c) {
@@ -377,6 +443,7 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   cudaMemset(c->Nvp, 0, hn * 16);
   cudaMemset(c->Nop, 0, hn * 16);
   if ((e = cudaDeviceSynchronize())) return bail(fail(DNS_ERR_CUDA, cudaGetErrorString(e)));
+  default_variants(c);
   *out = c;
   return DNS_OK;
 }
@@ -385,6 +452,7 @@ dns_status dns_destroy(dns_ctx* c) {
   if (!c) return DNS_OK;
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->solve_graph) cudaGraphExecDestroy(c->solve_graph);
   free_fft(c->fz_d); free_fft(c->fx_d); free_fft(c->fyP_d); free_fft(c->fy0_d);
   free_fft(c->fz_f); free_fft(c->fx_f); free_fft(c->fyP_f);
   void* ptrs[] = {c->T0, c->T2, c->T4, c->Ut, c->dUt, c->ddUt, c->Uy, c->V, c->O, c->Nvp,
@@ -581,16 +649,6 @@ dns_status dns_set_wait_limit(dns_ctx* c, long long cycles) {
   return DNS_OK;
 }
 
-namespace {
-bool variant_available(const dns_ctx* c, int pass, int v) {
-  if (pass == DNS_PASS_Y3) {
-    if (v == DNS_Y3_FFT) return true;
-    if (v == DNS_Y3_TENSOR) return c->P.precision == DNS_PREC_MIXED && c->g.Ny == 129 && c->g.Py == 257;
-  }
-  return false;
-}
-}  // namespace
-
 dns_status dns_set_variant(dns_ctx* c, int pass, int v) {
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (pass < 0 || pass >= DNS_NUM_PASSES) return fail(DNS_ERR_ARG, "unknown pass");
@@ -620,52 +678,86 @@ dns_status dns_get_variant(const dns_ctx* c, int pass, int* v) {
 
 dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]) {
   if (!c) return fail(DNS_ERR_ARG, "null context");
+  if (!c->have_state) return fail(DNS_ERR_STATE, "dns_autotune needs a state");
   CK(cudaSetDevice(c->P.device));
   CK(cudaStreamSynchronize(c->st));
-  if (ms)
-    for (int i = 0; i < DNS_NUM_PASSES * DNS_MAX_VARIANTS; ++i) ms[i] = -1.0;
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  dns_status st = DNS_OK;
-  // y3 reads the state and writes only the transform buffer: each candidate
-  // is timed on the context's own buffers (1 warm-up + 5 launches)
-  {
-    const DnsGeom& g = c->g;
-    PencilArr F6p{c->F6, c->PyS, g.H * c->PyS};
-    double best = 1e300;
-    int pick = c->variant[DNS_PASS_Y3];
-    for (int v = 0; v < DNS_MAX_VARIANTS && st == DNS_OK; ++v) {
-      if (!variant_available(c, DNS_PASS_Y3, v)) continue;
-      if (v == DNS_Y3_TENSOR && !c->y3tc_tab) {
-        const int keep = c->variant[DNS_PASS_Y3];
-        if ((st = dns_set_variant(c, DNS_PASS_Y3, v)) != DNS_OK) break;
-        if ((st = dns_set_variant(c, DNS_PASS_Y3, keep)) != DNS_OK) break;
-      }
-      auto run = [&]() -> cudaError_t {
-        if (c->P.precision == DNS_PREC_MIXED) {
-          if (v == DNS_Y3_TENSOR) return launch_y3tc(c->V, c->O, F6p, g, c->ph, c->y3tc_tab, c->status, c->st);
-          return launch_y3<float2>(c->V, c->O, F6p, g, c->ph, c->fyP_f.tab(), c->status, c->st);
-        }
-        return launch_y3<double2>(c->V, c->O, F6p, g, c->ph, c->fyP_d.tab(), c->status, c->st);
-      };
-      cudaError_t e = run();
-      if (!e) e = cudaEventRecord(e0, c->st);
-      for (int i = 0; i < 5 && !e; ++i) e = run();
-      if (!e) e = cudaEventRecord(e1, c->st);
-      if (!e) e = cudaEventSynchronize(e1);
-      float t = 0.f;
-      if (!e) e = cudaEventElapsedTime(&t, e0, e1);
-      if (e) { st = fail(DNS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e)); break; }
-      st = check_status(c);
-      const double per = t / 5.0;
-      if (ms) ms[DNS_PASS_Y3 * DNS_MAX_VARIANTS + v] = per;
-      if (per < best) { best = per; pick = v; }
+  dns_status st = build_wall_solver(c);
+  if (st != DNS_OK) return st;
+  double t[DNS_NUM_PASSES * DNS_MAX_VARIANTS];
+  bool avail[DNS_NUM_PASSES][DNS_MAX_VARIANTS];
+  for (int p = 0; p < DNS_NUM_PASSES; ++p)
+    for (int v = 0; v < DNS_MAX_VARIANTS; ++v) {
+      t[p * DNS_MAX_VARIANTS + v] = -1.0;
+      avail[p][v] = variant_available(c, p, v);
     }
-    if (st == DNS_OK) st = dns_set_variant(c, DNS_PASS_Y3, pick);
+  if (avail[DNS_PASS_Y3][DNS_Y3_TENSOR] && !c->y3tc_tab) {
+    const int keep = c->variant[DNS_PASS_Y3];
+    if ((st = dns_set_variant(c, DNS_PASS_Y3, DNS_Y3_TENSOR)) != DNS_OK) return st;
+    if ((st = dns_set_variant(c, DNS_PASS_Y3, keep)) != DNS_OK) return st;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  // Every candidate is timed inside whole steps (its inputs as the step
+  // leaves them, its neighbours running): round r runs variant r of every
+  // pass that has one (the current variant elsewhere), one warm-up step and
+  // three timed steps with events around each kernel.  The state and the
+  // AB2 history are saved first and put back after.
+  const size_t hn = (size_t)c->g.H * c->g.Ny;
+  double2* save = nullptr;
+  CK(cudaMalloc(&save, 4 * hn * 16));
+  double2* const bufs[4] = {c->V, c->O, c->Nvp, c->Nop};
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 4 && !e; ++i) e = cudaMemcpyAsync(save + i * hn, bufs[i], hn * 16, cudaMemcpyDeviceToDevice, c->st);
+  int keep[DNS_NUM_PASSES];
+  for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = c->variant[p];
+  // kernel slot of each pass in a step's events
+  static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3};
+  const int ne = DNS_NUM_KERNELS + 1, nt = 3;
+  std::vector<cudaEvent_t> ev((size_t)ne * (nt + 1));
+  for (auto& x : ev)
+    if (!e) e = cudaEventCreate(&x);
+  for (int r = 0; r < DNS_MAX_VARIANTS && !e && st == DNS_OK; ++r) {
+    bool any = false;
+    for (int p = 0; p < DNS_NUM_PASSES; ++p) {
+      c->variant[p] = avail[p][r] ? r : keep[p];
+      any = any || avail[p][r];
+    }
+    if (!any) continue;
+    for (int i = 0; i <= nt && !e; ++i) e = enqueue(c, 0, &ev[(size_t)i * ne]);
+    if (!e) e = cudaStreamSynchronize(c->st);
+    if (!e) st = check_status(c);
+    for (int p = 0; p < DNS_NUM_PASSES && !e && st == DNS_OK; ++p) {
+      if (!avail[p][r]) continue;
+      double sum = 0.0;
+      for (int i = 1; i <= nt; ++i) {
+        float x = 0.f;
+        cudaEventElapsedTime(&x, ev[(size_t)i * ne + slot[p]], ev[(size_t)i * ne + slot[p] + 1]);
+        sum += x;
+      }
+      t[p * DNS_MAX_VARIANTS + r] = sum / nt;
+    }
+  }
+  for (auto& x : ev)
+    if (x) cudaEventDestroy(x);
+  for (int i = 0; i < 4; ++i) {
+    cudaError_t e2 = cudaMemcpyAsync(bufs[i], save + i * hn, hn * 16, cudaMemcpyDeviceToDevice, c->st);
+    if (!e) e = e2;
+  }
+  cudaError_t e3 = cudaStreamSynchronize(c->st);
+  if (!e) e = e3;
+  cudaFree(save);
+  for (int p = 0; p < DNS_NUM_PASSES; ++p) c->variant[p] = keep[p];
+  if (e) return fail(DNS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  if (st != DNS_OK) return st;
+  for (int p = 0; p < DNS_NUM_PASSES && st == DNS_OK; ++p) {
+    int pick = keep[p];
+    double best = 1e300;
+    for (int v = 0; v < DNS_MAX_VARIANTS; ++v) {
+      const double x = t[p * DNS_MAX_VARIANTS + v];
+      if (x >= 0 && x < best) { best = x; pick = v; }
+    }
+    st = dns_set_variant(c, p, pick);
+  }
+  if (ms)
+    for (int i = 0; i < DNS_NUM_PASSES * DNS_MAX_VARIANTS; ++i) ms[i] = t[i];
   return st;
 }
 
@@ -750,12 +842,12 @@ dns_status dns_transform_3d_one(dns_ctx* c, int dir, void* phys, size_t pitch, v
   if (dir == DNS_BACKWARD) {
     if (pad == DNS_PADDING) CK(launch_cheby_inplace<double2>(sp, g.H, 0, g.Ny, c->fyP_d.tab(), c->st));
     else CK(launch_cheby_inplace<double2>(sp, g.H, 1, g.Ny, c->fy0_d.tab(), c->st));
-    CK(launch_zb<double2>(sp, sr, 1, g, c->fz_d.tab(), c->st));
+    CK(launch_zb<double2>(sp, sr, 1, g, c->fz_d.tab(), c->st, nullptr, zvar64(c, DNS_PASS_ZB)));
     CK(launch_x_c2r<double2>(sr, (double*)phys, rps, nrows, g, c->fx_d.tab(), c->st));
   } else {
     CK(launch_x_r2c<double2>((const double*)phys, rps, sr, nrows, g, c->fx_d.tab(),
                              1.0 / g.Px / g.Pz, c->st));
-    CK(launch_zf<double2>(sr, sp, 1, g, c->fz_d.tab(), c->st));
+    CK(launch_zf<double2>(sr, sp, 1, g, c->fz_d.tab(), c->st, nullptr, zvar64(c, DNS_PASS_ZF)));
     if (pad == DNS_PADDING) CK(launch_cheby_inplace<double2>(sp, g.H, 2, g.Ny, c->fyP_d.tab(), c->st));
     else CK(launch_cheby_inplace<double2>(sp, g.H, 3, g.Ny, c->fy0_d.tab(), c->st));
   }
@@ -918,6 +1010,31 @@ dns_status dns_check_state(dns_ctx* c) {
   return DNS_OK;
 }
 
+namespace {
+// The solve-only sequence on the device: right-hand sides bv, bo (pitch bp,
+// either may stand for a zero system) -> solutions into ov, oo (pitch op).
+// Point values and their DCT-I go through the transform buffer F6, which the
+// banded solve then takes as its scratch.
+cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo, long long bp,
+                               double2* Xv, double2* Xo, double2* pbc, double2* ov, double2* oo,
+                               long long op) {
+  const DnsGeom& g = c->g;
+  const long long ls = c->P.mz / 2;  // no-padding DCT-I length 2N
+  double2* sv = (double2*)c->F6;
+  double2* so = sv + g.H * ls;
+  const double* cosk = c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no;
+  cudaError_t e = launch_colloc_prep(bv, bo, bp, sv, so, ls, pbc, cosk, c->Ut, c->ddUt, g, c->ph, c->st);
+  if (!e) e = launch_cheby_inplace<double2>(PencilArr{sv, ls, 0}, 2 * g.H, 3, g.Ny, c->fy0_d.tab(), c->st);
+  if (!e) e = launch_colloc_integrate(sv, so, ls, c->rv, c->ro, c->wd, g, c->st);
+  WallDims wd = c->wd;
+  wd.tilt = 0;
+  if (!e) e = launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph,
+                                c->status, c->st);
+  if (!e) e = launch_colloc_finish(Xv, Xo, pbc, ov, oo, op, g, c->st);
+  return e;
+}
+}  // namespace
+
 dns_status dns_solve_wall(dns_ctx* c, void* v, void* omega, size_t tpitch, int where) {
   if (!c || (!v && !omega)) return fail(DNS_ERR_ARG, "null argument");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
@@ -927,38 +1044,100 @@ dns_status dns_solve_wall(dns_ctx* c, void* v, void* omega, size_t tpitch, int w
   CK(cudaSetDevice(c->P.device));
   dns_status s = build_wall_solver(c);
   if (s != DNS_OK) return s;
+  if ((size_t)2 * g.H * (c->P.mz / 2) * 16 > c->F6_bytes)
+    return fail(DNS_ERR_ARG, "solve-only DCT buffer does not fit the transform buffer");
   const size_t hn = (size_t)g.H * g.Ny;
   if (!c->solve_io) CK(c->alloc(&c->solve_io, 2 * hn + 6 * (size_t)g.H));
   double2* Xv = c->solve_io;
   double2* Xo = Xv + hn;
   double2* pbc = Xo + hn;
-  // a missing system is solved for a zero right-hand side and not written
-  const double2 *bv = (const double2*)v, *bo = (const double2*)omega;
-  long long bp = (long long)(tpitch / 16);
-  if (where == DNS_HOST || !v || !omega) {
-    if (v) CK(cudaMemcpy2DAsync(Xv, row, v, tpitch, row, g.H, kind_of(where, true), c->st));
-    else CK(cudaMemsetAsync(Xv, 0, hn * 16, c->st));
-    if (omega) CK(cudaMemcpy2DAsync(Xo, row, omega, tpitch, row, g.H, kind_of(where, true), c->st));
-    else CK(cudaMemsetAsync(Xo, 0, hn * 16, c->st));
-    bv = Xv;
-    bo = Xo;
-    bp = g.Ny;
+  if (where == DNS_DEVICE && v && omega) {
+    // in place on the caller's device pencils: one captured graph per
+    // (buffers, pitch), launched on every call
+    if (!c->solve_graph || c->solve_key[0] != v || c->solve_key[1] != omega || c->solve_pitch != tpitch) {
+      if (c->solve_graph) cudaGraphExecDestroy(c->solve_graph);
+      c->solve_graph = nullptr;
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = enqueue_solve_wall(c, (const double2*)v, (const double2*)omega, (long long)(tpitch / 16),
+                                         Xv, Xo, pbc, (double2*)v, (double2*)omega, (long long)(tpitch / 16));
+      cudaError_t e2 = cudaStreamEndCapture(c->st, &gr);
+      if (e) return fail(DNS_ERR_CUDA, std::string("solve capture: ") + cudaGetErrorString(e));
+      CK(e2);
+      CK(cudaGraphInstantiate(&c->solve_graph, gr, 0));
+      cudaGraphDestroy(gr);
+      c->solve_key[0] = v;
+      c->solve_key[1] = omega;
+      c->solve_pitch = tpitch;
+    }
+    CK(cudaGraphLaunch(c->solve_graph, c->st));
+    return check_status(c);
   }
-  const double* cosk = c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no;
-  CK(launch_colloc_rhs(bv, bo, bp, c->rv, c->ro, pbc, c->wd, cosk, c->Ut, c->ddUt, g, c->ph, c->st));
-  WallDims wd = c->wd;
-  wd.tilt = 0;
-  CK(launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph,
-                       c->status, c->st));
+  // host buffers, or one system only: staged through Xv, Xo (pitch Ny); a
+  // missing system is solved for a zero right-hand side and not written
+  if (v) CK(cudaMemcpy2DAsync(Xv, row, v, tpitch, row, g.H, kind_of(where, true), c->st));
+  else CK(cudaMemsetAsync(Xv, 0, hn * 16, c->st));
+  if (omega) CK(cudaMemcpy2DAsync(Xo, row, omega, tpitch, row, g.H, kind_of(where, true), c->st));
+  else CK(cudaMemsetAsync(Xo, 0, hn * 16, c->st));
   if (where == DNS_HOST) {
-    CK(launch_colloc_finish(Xv, Xo, pbc, Xv, Xo, g.Ny, g, c->st));
+    CK(enqueue_solve_wall(c, Xv, Xo, g.Ny, Xv, Xo, pbc, Xv, Xo, g.Ny));
     if (v) CK(cudaMemcpy2DAsync(v, tpitch, Xv, row, row, g.H, cudaMemcpyDeviceToHost, c->st));
     if (omega) CK(cudaMemcpy2DAsync(omega, tpitch, Xo, row, row, g.H, cudaMemcpyDeviceToHost, c->st));
   } else {
-    CK(launch_colloc_finish(Xv, Xo, pbc, (double2*)v, (double2*)omega, (long long)(tpitch / 16), g,
-                            c->st));
+    CK(enqueue_solve_wall(c, Xv, Xo, g.Ny, Xv, Xo, pbc, (double2*)v, (double2*)omega, (long long)(tpitch / 16)));
   }
   return check_status(c);
+}
+
+dns_status dns_solve_residual(dns_ctx* c, const void* bv, const void* bo, const void* xv, const void* xo,
+                              size_t tpitch, int where, double out[6]) {
+  if (!c || !bv || !bo || !xv || !xo || !out) return fail(DNS_ERR_ARG, "null argument");
+  if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
+  const DnsGeom& g = c->g;
+  const size_t row = (size_t)g.Ny * 16, hn = (size_t)g.H * g.Ny;
+  if (tpitch % 16 || tpitch < row) return fail(DNS_ERR_ARG, "bad tpitch");
+  CK(cudaSetDevice(c->P.device));
+  double2* stage = nullptr;
+  double* per = nullptr;
+  const void* src[4] = {bv, bo, xv, xo};
+  const double2* d[4];
+  long long ps = (long long)(tpitch / 16);
+  cudaError_t e = cudaMalloc(&per, (size_t)g.H * 6 * sizeof(double));
+  if (!e && where == DNS_HOST) {
+    e = cudaMalloc(&stage, 4 * hn * 16);
+    for (int i = 0; i < 4 && !e; ++i) {
+      e = cudaMemcpy2DAsync(stage + i * hn, row, src[i], tpitch, row, g.H, cudaMemcpyHostToDevice, c->st);
+      d[i] = stage + i * hn;
+    }
+    ps = g.Ny;
+  } else {
+    for (int i = 0; i < 4; ++i) d[i] = (const double2*)src[i];
+  }
+  if (!e) e = launch_solve_residual(d[0], d[1], d[2], d[3], ps, g, c->ph, c->T0, c->T2, c->T4, c->Ut,
+                                    c->ddUt, per, c->st);
+  std::vector<double> h((size_t)g.H * 6);
+  if (!e) e = cudaMemcpyAsync(h.data(), per, h.size() * 8, cudaMemcpyDeviceToHost, c->st);
+  if (!e) e = cudaStreamSynchronize(c->st);
+  cudaFree(per);
+  cudaFree(stage);
+  if (e) return fail(DNS_ERR_CUDA, cudaGetErrorString(e));
+  // per pencil: |r_v|^2, |b_v|^2, |r_o|^2, |b_o|^2, backward error v, omega
+  double rv = 0, bvn = 0, ro = 0, bon = 0, mv = 0, mo = 0, bwv = 0, bwo = 0;
+  for (long long p = 0; p < g.H; ++p) {
+    const double* q = &h[(size_t)p * 6];
+    rv += q[0]; bvn += q[1]; ro += q[2]; bon += q[3];
+    if (q[1] > 0) mv = std::max(mv, std::sqrt(q[0] / q[1]));
+    if (q[3] > 0) mo = std::max(mo, std::sqrt(q[2] / q[3]));
+    bwv = std::max(bwv, q[4]);
+    bwo = std::max(bwo, q[5]);
+  }
+  out[0] = mv;
+  out[1] = mo;
+  out[2] = bvn > 0 ? std::sqrt(rv / bvn) : 0.0;
+  out[3] = bon > 0 ? std::sqrt(ro / bon) : 0.0;
+  out[4] = bwv;
+  out[5] = bwo;
+  return DNS_OK;
 }
 
 dns_status dns_init_aux_matrix(dns_ctx* c, void* inv_v, void* inv_o, int where) {

@@ -54,6 +54,9 @@ struct dns_ctx {
   int variant[DNS_NUM_PASSES] = {};  // kernel variant of each tunable pass
   uint32_t* y3tc_tab = nullptr;      // Chebyshev table of the tensor-core y3 pass
   cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t solve_graph = nullptr;  // dns_solve_wall on device pencils
+  const void* solve_key[2] = {nullptr, nullptr};
+  size_t solve_pitch = 0;
 
   template <typename T> cudaError_t alloc(T** p, size_t n) {
     bytes += n * sizeof(T);

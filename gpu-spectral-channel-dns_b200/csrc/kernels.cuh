@@ -12,6 +12,7 @@
 //                                         layout before its 2D C2R
 //   state arrays   [pencil][n] FP64 complex, n < Ny, pitch Ny
 #pragma once
+#include "../../include/dns_b200.h"
 #include "dns_common.cuh"
 #include "fft.cuh"
 
@@ -21,6 +22,19 @@ template <typename C> struct FftTab {
   const short* drev;    // digit-reversed position of natural index n
   const C* wt[3];       // FP32 warp-FFT twiddle tables of the plans with 1, 2, 4 lines per warp
 };
+
+// twiddles of a warp-FFT plan: FP32, the plan's own table (lines per warp
+// 1, 2, 4 -> i = 0, 1, 2); FP64, W_L^j and product recurrences
+template <typename C> DNS_HD const C* wtw_of(const FftTab<C>& t, int i) {
+  return sizeof(C) == 16 ? t.tw : t.wt[i];
+}
+
+// Pass launchers take a variant (the DNS_Y3_*, DNS_Y1_*, DNS_Z_* values of
+// the public header) or VAR_AUTO, the first form the arguments allow in the
+// order tensor copies, warp FFTs, block FFT.  With a variant they launch
+// exactly that form or return cudaErrorNotSupported; with probe = true they
+// only report which of the two it would be.
+#define VAR_AUTO (-1)
 
 struct PencilArr {      // generic pencil-major array
   void* base;

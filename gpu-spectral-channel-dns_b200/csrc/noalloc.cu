@@ -113,7 +113,7 @@ extern "C" dns_status dns_transform_3d_one_noalloc(dns_ctx* c, int dir, void* ph
       gs.Py = (g.Py - y0 < S) ? g.Py - y0 : S;
       PencilArr slab_in{(double2*)spec + y0, ps, 0};
       double* out = (double*)phys + (long long)y0 * g.Pz * rps;
-      st = ck(launch_zb<double2>(slab_in, sr, 1, gs, c->fz_d.tab(), c->st));
+      st = ck(launch_zb<double2>(slab_in, sr, 1, gs, c->fz_d.tab(), c->st, nullptr, DNS_Z_BLOCK));
       if (st == DNS_OK)
         st = ck(launch_x_c2r<double2>(sr, out, rps, (long long)gs.Py * g.Pz, gs, c->fx_d.tab(), c->st));
     }
@@ -125,7 +125,7 @@ extern "C" dns_status dns_transform_3d_one_noalloc(dns_ctx* c, int dir, void* ph
       PencilArr slab_out{(double2*)spec + y0, ps, 0};
       st = ck(launch_x_r2c<double2>(in, rps, sr, (long long)gs.Py * g.Pz, gs, c->fx_d.tab(),
                                      1.0 / g.Px / g.Pz, c->st));
-      if (st == DNS_OK) st = ck(launch_zf<double2>(sr, slab_out, 1, gs, c->fz_d.tab(), c->st));
+      if (st == DNS_OK) st = ck(launch_zf<double2>(sr, slab_out, 1, gs, c->fz_d.tab(), c->st, nullptr, DNS_Z_BLOCK));
     }
     if (st == DNS_OK) {
       if (pad == DNS_PADDING) st = ck(launch_cheby_inplace<double2>(sp, g.H, 2, g.Ny, c->fyP_d.tab(), c->st));

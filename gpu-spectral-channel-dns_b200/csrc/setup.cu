@@ -366,3 +366,86 @@ cudaError_t launch_operator_matrices(long long p0, long long np, DnsGeom g, Phys
   k_operator_matrices<<<(unsigned)np, 256, 0, st>>>(p0, g, ph, T0, T2, T4, U, ddU, outV, outO);
   return cudaGetLastError();
 }
+
+// Residual of solved collocation systems, one CTA per pencil: r = A x - b
+// with A the reference's operator (the same entries as k_gj_invert's) for
+// the v (eq 0) and omega (eq 1) systems.  per[p] = {|r_v|^2, |b_v|^2,
+// |r_o|^2, |b_o|^2, normwise backward error of v and of omega:
+// max|r| / (max_i sum_j |A_ij| max|x| + max|b|)}.
+__global__ void __launch_bounds__(128) k_solve_residual(const double2* __restrict__ bv,
+                                                        const double2* __restrict__ bo,
+                                                        const double2* __restrict__ xv,
+                                                        const double2* __restrict__ xo, long long ps,
+                                                        DnsGeom g, PhysParams ph, const double* T0,
+                                                        const double* T2, const double* T4,
+                                                        const double* U, const double* ddU, double* per) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = g.Ny;
+  double2* x = (double2*)smem_raw;  // [eq][N]
+  __shared__ double red[4][6];      // per warp: |r|^2, |b|^2, max|r|, max rowsum, max|x|, max|b|
+  const long long p = blockIdx.x;
+  const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
+  const bool zero = kx == 0 && kz == 0;
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = kmn_of(ia, ib);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int eq = 0; eq < 2; ++eq) {
+    const double2* xs = eq ? xo : xv;
+    const double2* bs = eq ? bo : bv;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) x[j] = xs[p * ps + j];
+    __syncthreads();
+    double r2 = 0, b2 = 0, rmax = 0, amax = 0, xmax = 0, bmax = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      double2 s = make_double2(0.0, 0.0);
+      double rs = 0;
+      for (int j = 0; j < N; ++j) {
+        const double2 a = op_entry(eq, zero, i, j, N, T0, T2, T4, U, ddU, ph.Re, ph.dt, kmn, ia);
+        s = s + cmul(a, x[j]);
+        rs += hypot(a.x, a.y);
+      }
+      const double2 b = bs[p * ps + i];
+      const double2 r = s - b;
+      r2 += r.x * r.x + r.y * r.y;
+      b2 += b.x * b.x + b.y * b.y;
+      rmax = fmax(rmax, hypot(r.x, r.y));
+      amax = fmax(amax, rs);
+      bmax = fmax(bmax, hypot(b.x, b.y));
+      xmax = fmax(xmax, hypot(x[i].x, x[i].y));
+    }
+    for (int o = 16; o; o >>= 1) {
+      r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+      amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+      bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    }
+    if (lane == 0) {
+      red[warp][0] = r2; red[warp][1] = b2; red[warp][2] = rmax;
+      red[warp][3] = amax; red[warp][4] = xmax; red[warp][5] = bmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t[6] = {0, 0, 0, 0, 0, 0};
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        t[0] += red[w][0]; t[1] += red[w][1];
+        for (int k = 2; k < 6; ++k) t[k] = fmax(t[k], red[w][k]);
+      }
+      const double den = t[3] * t[4] + t[5];
+      per[p * 6 + 2 * eq] = t[0];
+      per[p * 6 + 2 * eq + 1] = t[1];
+      per[p * 6 + 4 + eq] = den > 0 ? t[2] / den : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_solve_residual(const double2* bv, const double2* bo, const double2* xv, const double2* xo,
+                                  long long ps, DnsGeom g, PhysParams ph, const double* T0,
+                                  const double* T2, const double* T4, const double* U, const double* ddU,
+                                  double* per, cudaStream_t st) {
+  k_solve_residual<<<(unsigned)g.H, 128, (size_t)g.Ny * 16, st>>>(bv, bo, xv, xo, ps, g, ph, T0, T2, T4, U, ddU,
+                                                                  per);
+  return cudaGetLastError();
+}

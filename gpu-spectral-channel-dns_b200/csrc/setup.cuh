@@ -15,3 +15,7 @@ cudaError_t launch_operator_matrices(long long p0, long long np, DnsGeom g, Phys
                                      const double* T0, const double* T2, const double* T4,
                                      const double* U, const double* ddU, double2* outV,
                                      double2* outO, cudaStream_t st);
+cudaError_t launch_solve_residual(const double2* bv, const double2* bo, const double2* xv, const double2* xo,
+                                  long long ps, DnsGeom g, PhysParams ph, const double* T0,
+                                  const double* T2, const double* T4, const double* U, const double* ddU,
+                                  double* per, cudaStream_t st);

@@ -13,7 +13,8 @@
 //      (cubic for v, linear otherwise);
 //   2. f = the interior rows minus (A p) at their points, zero at the points
 //      the equation leaves out, and the coefficients of its interpolant
-//      (DCT-I over the Gauss-Lobatto points);
+//      (DCT-I over the Gauss-Lobatto points: the FFT of the even extension,
+//      the library's no-padding p2s);
 //   3. rows K .. K+n-1 of the K-fold Chebyshev integral (K = 4 for v, 2
 //      otherwise), the input of the banded solve, which then runs without
 //      the tilting term;
@@ -33,34 +34,30 @@ namespace {
 
 __device__ __forceinline__ double2 cx(double a, double b) { return make_double2(a, b); }
 
-__global__ void __launch_bounds__(128) k_colloc_rhs(const double2* __restrict__ bv,
-                                                    const double2* __restrict__ bo, long long bp,
-                                                    double2* gv, double2* go, double2* pbc,
-                                                    int nv, int no, long long gp,
-                                                    const double* __restrict__ cosk,
-                                                    const double* __restrict__ Ut,
-                                                    const double* __restrict__ ddUt, DnsGeom g,
-                                                    PhysParams ph) {
+// 1-2. wall polynomial and the point values of the interior right-hand side
+// minus A p, zero where the equation has no row; written as Gauss-Lobatto
+// values (m = 0..N, pitch sp) for the DCT-I that follows
+__global__ void __launch_bounds__(128) k_colloc_prep(const double2* __restrict__ bv,
+                                                     const double2* __restrict__ bo, long long bp,
+                                                     double2* sv, double2* so, long long sp,
+                                                     double2* pbc, const double* __restrict__ cosk,
+                                                     const double* __restrict__ Ut,
+                                                     const double* __restrict__ ddUt, DnsGeom g,
+                                                     PhysParams ph) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Ny = g.Ny, N = Ny - 1, LB = Ny + 8;
+  const int Ny = g.Ny, N = Ny - 1;
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
   const bool zero = p == 0;
-  double2* rv = (double2*)smem_raw;  // raw rows, then interpolant coefficients
+  double2* rv = (double2*)smem_raw;
   double2* ro = rv + Ny;
-  double2* av = ro + Ny;  // integration buffers, LB each
-  double2* sv = av + LB;
-  double2* ao = sv + LB;
-  double2* so = ao + LB;
-  double* cs = (double*)(so + LB);  // cos(k pi / N), k = 0..N
   __shared__ double2 pc[6];
   for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
     rv[k] = bv[p * bp + k];
     ro[k] = bo[p * bp + k];
-    cs[k] = cosk[k];
   }
   __syncthreads();
-  // 1. wall polynomial: T_j(+-1) = (+-1)^j, T_j'(1) = j^2, T_j'(-1) = (-1)^(j+1) j^2
+  // wall polynomial: T_j(+-1) = (+-1)^j, T_j'(1) = j^2, T_j'(-1) = (-1)^(j+1) j^2
   if (threadIdx.x == 0) {
     const double2 e = (rv[0] + rv[1]) * 0.5, o = (rv[0] - rv[1]) * 0.5;
     if (zero) {
@@ -78,57 +75,53 @@ __global__ void __launch_bounds__(128) k_colloc_rhs(const double2* __restrict__ 
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
   const double kmn = ia * ia + ib * ib, dt = ph.dt, Re = ph.Re;
-  // 2. point values minus A p (zero where the equation has no row)
-  for (int m = threadIdx.x; m < LB; m += blockDim.x) {
+  for (int m = threadIdx.x; m <= N; m += blockDim.x) {
     double2 fv = cx(0, 0), fo = cx(0, 0);
-    if (m <= N) {
-      const double y = cs[m];
-      if (zero) {
-        if (m >= 1 && m <= N - 1) {
-          fv = rv[m + 1] - (pc[0] + pc[1] * y);
-          fo = ro[m + 1] - (pc[4] + pc[5] * y);
-        }
-      } else {
-        if (m >= 2 && m <= N - 2) {
-          const double2 P0 = pc[0] + pc[1] * y + pc[2] * (2 * y * y - 1) + pc[3] * (y * (4 * y * y - 3));
-          const double2 P2 = pc[2] * 4.0 + pc[3] * (24.0 * y);
-          const double U = Ut[m], ddU = ddUt[m];
-          const double2 re = P2 * (1 + kmn * dt / Re) - P0 * (kmn * (1 + kmn * dt * 0.5 / Re));
-          const double2 im = P2 * (ia * dt * 0.5 * U) - P0 * (kmn * ia * dt * 0.5 * U + ia * dt * 0.5 * ddU);
-          fv = rv[m + 2] - (re + muli(im));
-        }
-        if (m >= 1 && m <= N - 1) {
-          const double2 P0 = pc[4] + pc[5] * y;
-          fo = ro[m + 1] - (P0 * (1 + kmn * dt * 0.5 / Re) + muli(P0 * (ia * dt * 0.5 * Ut[m])));
-        }
+    const double y = __ldg(cosk + m);
+    if (zero) {
+      if (m >= 1 && m <= N - 1) {
+        fv = rv[m + 1] - (pc[0] + pc[1] * y);
+        fo = ro[m + 1] - (pc[4] + pc[5] * y);
+      }
+    } else {
+      if (m >= 2 && m <= N - 2) {
+        const double2 P0 = pc[0] + pc[1] * y + pc[2] * (2 * y * y - 1) + pc[3] * (y * (4 * y * y - 3));
+        const double2 P2 = pc[2] * 4.0 + pc[3] * (24.0 * y);
+        const double U = Ut[m], ddU = ddUt[m];
+        const double2 re = P2 * (1 + kmn * dt / Re) - P0 * (kmn * (1 + kmn * dt * 0.5 / Re));
+        const double2 im = P2 * (ia * dt * 0.5 * U) - P0 * (kmn * ia * dt * 0.5 * U + ia * dt * 0.5 * ddU);
+        fv = rv[m + 2] - (re + muli(im));
+      }
+      if (m >= 1 && m <= N - 1) {
+        const double2 P0 = pc[4] + pc[5] * y;
+        fo = ro[m + 1] - (P0 * (1 + kmn * dt * 0.5 / Re) + muli(P0 * (ia * dt * 0.5 * Ut[m])));
       }
     }
-    av[m] = fv;
-    ao[m] = fo;
+    sv[p * sp + m] = fv;
+    so[p * sp + m] = fo;
   }
-  __syncthreads();
-  // interpolant: a_k = 2/(N c_k) sum_m f_m cos(k m pi/N), c_0 = c_N = 2 (f_0 = f_N = 0)
-  for (int k = threadIdx.x; k <= N; k += blockDim.x) {
-    double2 s1 = cx(0, 0), s2 = cx(0, 0);
-    int j = 0;
-    for (int m = 1; m < N; ++m) {
-      j += k;
-      if (j >= 2 * N) j -= 2 * N;
-      const double c = cs[j <= N ? j : 2 * N - j];
-      s1 = s1 + av[m] * c;
-      s2 = s2 + ao[m] * c;
-    }
-    const double w = ((k == 0 || k == N) ? 1.0 : 2.0) / N;
-    rv[k] = s1 * w;
-    ro[k] = s2 * w;
-  }
-  __syncthreads();
+}
+
+// 3. rows K .. K+n-1 of the K-fold Chebyshev integral of the interpolant
+// coefficients a_0..a_N (K = 4 for v, 2 for omega_y and the mean modes):
+// (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+__global__ void __launch_bounds__(128) k_colloc_integrate(const double2* __restrict__ cv,
+                                                          const double2* __restrict__ co, long long cp,
+                                                          double2* gv, double2* go, int nv, int no,
+                                                          long long gp, DnsGeom g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Ny = g.Ny, N = Ny - 1, LB = Ny + 8;
+  const long long p = blockIdx.x;
+  const bool zero = p == 0;
+  double2* av = (double2*)smem_raw;
+  double2* sv = av + LB;
+  double2* ao = sv + LB;
+  double2* so = ao + LB;
   for (int k = threadIdx.x; k < LB; k += blockDim.x) {
-    av[k] = k <= N ? rv[k] : cx(0, 0);
-    ao[k] = k <= N ? ro[k] : cx(0, 0);
+    av[k] = k <= N ? cv[p * cp + k] : cx(0, 0);
+    ao[k] = k <= N ? co[p * cp + k] : cx(0, 0);
   }
   __syncthreads();
-  // 3. Chebyshev integration (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
   const int Kv = zero ? 2 : 4;
   for (int it = 0; it < Kv; ++it) {
     const int nf = (it < 2) ? 2 : 1;
@@ -191,19 +184,27 @@ cudaError_t launch_nonfinite(const double2* a, const double2* b, long long n, in
   return cudaGetLastError();
 }
 
-size_t colloc_rhs_smem(int Ny) { return (size_t)16 * (2 * Ny + 4 * (Ny + 8)) + 8 * (size_t)Ny; }
-
-cudaError_t launch_colloc_rhs(const double2* bv, const double2* bo, long long bp, double2* gv,
-                              double2* go, double2* pbc, const WallDims& wd, const double* cosk,
-                              const double* Ut, const double* ddUt, const DnsGeom& g,
-                              const PhysParams& ph, cudaStream_t st) {
-  const size_t sm = colloc_rhs_smem(g.Ny);
+cudaError_t launch_colloc_prep(const double2* bv, const double2* bo, long long bp, double2* sv,
+                               double2* so, long long sp, double2* pbc, const double* cosk,
+                               const double* Ut, const double* ddUt, const DnsGeom& g,
+                               const PhysParams& ph, cudaStream_t st) {
+  const size_t sm = (size_t)32 * g.Ny;
   if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_colloc_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(k_colloc_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e) return e;
   }
-  k_colloc_rhs<<<(unsigned)g.H, 128, sm, st>>>(bv, bo, bp, gv, go, pbc, wd.nv, wd.no, wd.gp, cosk, Ut,
-                                               ddUt, g, ph);
+  k_colloc_prep<<<(unsigned)g.H, 128, sm, st>>>(bv, bo, bp, sv, so, sp, pbc, cosk, Ut, ddUt, g, ph);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_colloc_integrate(const double2* cv, const double2* co, long long cp, double2* gv,
+                                    double2* go, const WallDims& wd, const DnsGeom& g, cudaStream_t st) {
+  const size_t sm = (size_t)64 * (g.Ny + 8);
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_colloc_integrate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return e;
+  }
+  k_colloc_integrate<<<(unsigned)g.H, 128, sm, st>>>(cv, co, cp, gv, go, wd.nv, wd.no, wd.gp, g);
   return cudaGetLastError();
 }
 

@@ -27,11 +27,15 @@ cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const 
 // reference's pencil layout -> integrated right-hand sides of the banded
 // systems plus the wall polynomial (6 complex per pencil); and the solution
 // plus that polynomial back into pencils of pitch op (complex).
-size_t colloc_rhs_smem(int Ny);
-cudaError_t launch_colloc_rhs(const double2* bv, const double2* bo, long long bp, double2* gv,
-                              double2* go, double2* pbc, const WallDims& wd, const double* cosk,
-                              const double* Ut, const double* ddUt, const DnsGeom& g,
-                              const PhysParams& ph, cudaStream_t st);
+// prep: wall polynomial (pbc) and the point values (pitch sp) of the interior
+// right-hand side minus A p; integrate: the K-fold integrals of the
+// interpolant coefficients (pitch cp) into the banded systems' right-hand sides
+cudaError_t launch_colloc_prep(const double2* bv, const double2* bo, long long bp, double2* sv,
+                               double2* so, long long sp, double2* pbc, const double* cosk,
+                               const double* Ut, const double* ddUt, const DnsGeom& g,
+                               const PhysParams& ph, cudaStream_t st);
+cudaError_t launch_colloc_integrate(const double2* cv, const double2* co, long long cp, double2* gv,
+                                    double2* go, const WallDims& wd, const DnsGeom& g, cudaStream_t st);
 cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
                                  double2* ov, double2* oo, long long op, const DnsGeom& g,
                                  cudaStream_t st);

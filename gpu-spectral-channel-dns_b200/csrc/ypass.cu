@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   auto st = [&](int l, int k, C val) {
     if (k < Py) (l ? d1 : d0)[k] = val;
   };
-  wfft_io<C, M, 2, false>(wl, tab.wt[1], ld, st);
+  wfft_io<C, M, 2, false>(wl, wtw_of(tab, 1), ld, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 // also differentiate theirs), while warps 3 and 4 build the derivative
 // chains of v and omega_y; no block barrier inside the transforms.
 template <typename C, int M>
-__global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __restrict__ V,
+__global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
                                             double2* Nop, double2* gv, double2* go, RhsDims rd,
                                             RhsTabs tb, DnsGeom g, PhysParams ph,
@@ -831,7 +831,7 @@ __global__ void __launch_bounds__(160, 6) k_y1w(PencilArr lam, const double2* __
         lf[k] = c;
       }
     };
-    wfft_io<C, M, 1, false>(wline, tabP.wt[0], ld, st);
+    wfft_io<C, M, 1, false>(wline, wtw_of(tabP, 0), ld, st);
     if (warp < 2) ddz_warp(lf, lf + VS, Ny);
   } else if (!boot && warp == 3) {
     ddz_warp(Vc, DV, Ny);
@@ -1006,47 +1006,52 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
 
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
-                      PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st) {
+                      PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st, int variant, bool probe) {
+  const bool any = variant == VAR_AUTO;
   // the warp form stages its inputs by bulk copies (16-byte aligned
   // sources) and takes Ny = M/4 + 1, Py = M/2 + 1 as compile-time constants
-  const bool bulk_ok = aligned16(V) && aligned16(O) && tab.wt[1] &&
+  const bool bulk_ok = aligned16(V) && aligned16(O) && wtw_of(tab, 1) &&
                        g.Ny == tab.plan.L / 4 + 1 && g.Py == tab.plan.L / 2 + 1;
-  return with_len_m(tab.plan.L, [&](auto LL) {
+  return with_len_m(tab.plan.L, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    // warp-FFT form for FP32 (the FP64 form keeps the block FFT, whose
-    // register footprint is smaller)
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-     if (bulk_ok) {
+    if constexpr (L > 0 && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     if ((any || variant == DNS_Y3_FFT) && bulk_ok) {
+      if (probe) return cudaSuccess;
       const size_t sm = (size_t)6 * wlen<C>(L) * sizeof(C);
       cudaFuncSetAttribute(k_y3w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y3w<C, L><<<(unsigned)g.H, 96, sm, st>>>(V, O, out, g, ph, tab, status);
       return cudaGetLastError();
      }
     }
+    if (!any && variant != DNS_Y3_BLOCK) return cudaErrorNotSupported;
+    if (probe) return cudaSuccess;
     const size_t sm = y3_smem(g.Ny, FLine<C, L>::stride(tab.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y3<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_y3<C, L><<<(unsigned)g.H, 256, sm, st>>>(V, O, out, g, ph, tab);
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y3<double2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<double2>, int*, cudaStream_t);
-template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<float2>, int*, cudaStream_t);
+template cudaError_t launch_y3<double2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<double2>, int*, cudaStream_t, int, bool);
+template cudaError_t launch_y3<float2>(const double2*, const double2*, PencilArr, DnsGeom, PhysParams, FftTab<float2>, int*, cudaStream_t, int, bool);
 
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
                       double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
-                      PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st) {
+                      PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st, int variant,
+                      bool probe) {
+  const bool any = variant == VAR_AUTO;
   // the warp form stages its inputs by bulk copies (16-byte aligned pencils
   // with room for Py rounded up to even) and takes Ny = M/4 + 1,
   // Py = M/2 + 1 as compile-time constants
   const bool bulk_ok = aligned16(lam.base) && (lam.ps * sizeof(C)) % 16 == 0 &&
                        (lam.fs * sizeof(C)) % 16 == 0 && lam.ps >= ((g.Py + 1) & ~1) && aligned16(V) &&
-                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && tabP.wt[0] &&
+                       aligned16(O) && aligned16(Nvp) && aligned16(Nop) && wtw_of(tabP, 0) &&
                        g.Ny == tabP.plan.L / 4 + 1 && g.Py == tabP.plan.L / 2 + 1;
-  return with_len_m(tabP.plan.L, [&](auto LL) {
+  return with_len_m(tabP.plan.L, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
-     if (bulk_ok) {
+    if constexpr (L > 0 && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
+     if ((any || variant == DNS_Y1_WARP) && bulk_ok) {
+      if (probe) return cudaSuccess;
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
       const size_t bl = (size_t)3 * wlen<C>(L) * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
       const size_t sm = 9 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
@@ -1056,11 +1061,13 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
       return cudaGetLastError();
      }
     }
+    if (!any && variant != DNS_Y1_BLOCK) return cudaErrorNotSupported;
+    if (probe) return cudaSuccess;
     const size_t sm = y1_smem(g.Ny, FLine<C, L>::stride(tabP.plan.L), sizeof(C));
     cudaFuncSetAttribute(k_y1<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_y1<C, L><<<(unsigned)g.H, 256, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot);
     return cudaGetLastError();
   });
 }
-template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<double2>, int, int*, cudaStream_t);
-template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<float2>, int, int*, cudaStream_t);
+template cudaError_t launch_y1<double2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<double2>, int, int*, cudaStream_t, int, bool);
+template cudaError_t launch_y1<float2>(PencilArr, const double2*, const double2*, double2*, double2*, double2*, double2*, RhsDims, RhsTabs, DnsGeom, PhysParams, FftTab<float2>, int, int*, cudaStream_t, int, bool);

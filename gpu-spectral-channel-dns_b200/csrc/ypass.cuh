@@ -13,7 +13,8 @@ cudaError_t launch_solve_eq(const double2* inv, double2* rhs, long long ps, int 
                             long long npencils, cudaStream_t st);
 template <typename C>
 cudaError_t launch_y3(const double2* V, const double2* O, PencilArr out, DnsGeom g,
-                      PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st);
+                      PhysParams ph, FftTab<C> tab, int* status, cudaStream_t st, int variant = VAR_AUTO,
+                      bool probe = false);
 // rows of the integrated right-hand sides written by y1 for the wall solve
 struct RhsDims {
   int nv, no;       // rows per pencil (v / omega systems)
@@ -30,7 +31,8 @@ struct RhsTabs {
 template <typename C>
 cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2* Nvp,
                       double2* Nop, double2* gv, double2* go, RhsDims rd, RhsTabs tb, DnsGeom g,
-                      PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st);
+                      PhysParams ph, FftTab<C> tabP, int boot, int* status, cudaStream_t st,
+                      int variant = VAR_AUTO, bool probe = false);
 // tensor-core form of y3 (y3tc.cu): Ny = 129, FP32 output; cudaErrorNotSupported
 // for other sizes
 cudaError_t launch_y3tc(const double2* V, const double2* O, PencilArr out, DnsGeom g, PhysParams ph,

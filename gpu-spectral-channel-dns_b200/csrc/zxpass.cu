@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
-  wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, tab.wt[1], LS);
+  wfft<C, L, NLW, true>(lines + (size_t)NLW * warp * LS, wtw_of(tab, 1), LS);
   __syncthreads();
   // row side: this thread's kx, flat index i = yl * Pz + zp
   const int kxl = threadIdx.x % TX;
@@ -292,9 +292,8 @@ __global__ void __launch_bounds__(32 * NW, 4) k_zbt(const __grid_constant__ CUte
   }
 }
 
-template <typename C, int L, int NW>
+template <typename C, int L, int NW, int TX, int TY>
 __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGeom g, FftTab<C> tab) {
-  constexpr int TX = 4, TY = 4;
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
   constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -332,7 +331,7 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   constexpr int NLW = NL / NW;  // lines per warp
-  wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, tab.wt[1], LS);
+  wfft<C, L, NLW, false>(lines + (size_t)NLW * warp * LS, wtw_of(tab, 1), LS);
   __syncthreads();
   // pencil side: line li = (kxl, yl) of this thread, wavenumbers kz
   constexpr int hz = Nz / 2;
@@ -607,7 +606,7 @@ __global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, Ro
     const C* stg = zw;
     auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
     auto st = [&](int l, int k, C v) { zw[(size_t)l * LW + wsw<C>(k)] = v; };
-    wfft_io<C, L, 4, true>(zw, FftMaxRadix<C>::v == 8 ? tab.tw : tab.wt[2], ld, st);
+    wfft_io<C, L, 4, true>(zw, wtw_of(tab, 2), ld, st);
   }
   __syncthreads();
   const T ro = (T)Ro;
@@ -636,7 +635,7 @@ __global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, Ro
     z[(size_t)5 * LW + op] = B1;
   }
   __syncthreads();
-  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, FftMaxRadix<C>::v == 8 ? tab.tw : tab.wt[1]);
+  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, wtw_of(tab, 1));
   __syncthreads();
   // unpack: output row o = 3 rl + fl (field fl of row rl) by warp o mod 3,
   // lanes over the bins k; shared loads of a batch before its stores
@@ -811,38 +810,55 @@ bool row_tmap(const RowArr& in, int nf, const DnsGeom& g, size_t esz, CUtensorMa
 }
 }  // namespace
 
+// warp-FFT tiles gathered through L1: FP32 4 x 4 lines on 8 warps (whole
+// 32-byte sectors on both sides, three CTAs per SM); FP64 4 x 2 lines on 4
+// warps (64-byte runs on the row side, 32-byte runs of y pairs on the
+// pencil side, four CTAs per SM)
+template <typename C> struct ZWarpTile;
+template <> struct ZWarpTile<float2> { enum { NW = 8, TX = 4, TY = 4 }; };
+template <> struct ZWarpTile<double2> { enum { NW = 4, TX = 4, TY = 2 }; };
+
 template <typename C>
 cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
-                      int* status) {
+                      int* status, int variant, bool probe) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
-  return with_len_xz(g.Pz, [&](auto LL) {
+  const bool any = variant == VAR_AUTO;
+  return with_len_xz(g.Pz, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-     CUtensorMap tm;
+    if constexpr (L > 0 && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     const C* tw = wtw_of(tab, 1);
      constexpr int LS = wlen<C>(L) + 1;
-     if (status && g.Nz == L / 3 * 2 && tab.wt[1] && (size_t)g.Nz * 16 + 128 <= (size_t)2 * LS * sizeof(C) &&
-         pencil_tmap(in, nf, g, sizeof(C), &tm)) {
-      // pencils staged by tensor copies (a y pair per line pair), 8 x 2
-      // tile: 64-byte runs on the row side
-      const size_t sm = ((size_t)16 * LS) * sizeof(C);
-      cudaFuncSetAttribute(k_zbt<C, L, 8, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      dim3 grid((g.Kx + 7) / 8, (g.Py + 1) / 2, nf);
-      k_zbt<C, L, 8, 8, 2><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
-      return cudaGetLastError();
+     if constexpr (sizeof(C) == 8) {
+      CUtensorMap tm;
+      if ((any || variant == DNS_Z_TENSOR_COPY) && status && g.Nz == L / 3 * 2 && tw &&
+          (size_t)g.Nz * 16 + 128 <= (size_t)2 * LS * sizeof(C) && pencil_tmap(in, nf, g, sizeof(C), &tm)) {
+       if (probe) return cudaSuccess;
+       // pencils staged by tensor copies (a y pair per line pair), 8 x 2
+       // tile: 64-byte runs on the row side
+       const size_t sm = ((size_t)16 * LS) * sizeof(C);
+       cudaFuncSetAttribute(k_zbt<C, L, 8, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+       dim3 grid((g.Kx + 7) / 8, (g.Py + 1) / 2, nf);
+       k_zbt<C, L, 8, 8, 2><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
+       return cudaGetLastError();
+      }
      }
-     if (g.Nz == L / 3 * 2 && tab.wt[1]) {
-      const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
-      // 4 x 4 tile: whole 32-byte sectors on both sides.  Three CTAs per SM
-      // and the rest of the SM's memory as L1: the pencil-side gathers of
-      // neighbouring threads share sectors (measured: a quarter faster than
-      // four CTAs with a small L1)
-      cudaFuncSetAttribute(k_zbw<C, L, 8, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      cudaFuncSetAttribute(k_zbw<C, L, 8, 4, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
-      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
-      k_zbw<C, L, 8, 4, 4><<<grid, 256, sm, st>>>(in, out, g, tab);
+     if ((any || variant == DNS_Z_WARP) && g.Nz == L / 3 * 2 && tw) {
+      if (probe) return cudaSuccess;
+      typedef ZWarpTile<C> WT;
+      const size_t sm = ((size_t)WT::TX * WT::TY * LS) * sizeof(C);
+      // the rest of the SM's memory as L1: the pencil-side gathers of
+      // neighbouring threads share sectors (measured in FP32: a quarter
+      // faster than four CTAs with a small L1)
+      auto k = k_zbw<C, L, WT::NW, WT::TX, WT::TY>;
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
+      dim3 grid((g.Kx + WT::TX - 1) / WT::TX, (g.Py + WT::TY - 1) / WT::TY, nf);
+      k<<<grid, 32 * WT::NW, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
      }
     }
+    if (!any && variant != DNS_Z_BLOCK) return cudaErrorNotSupported;
+    if (probe) return cudaSuccess;
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zb<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
@@ -852,31 +868,41 @@ cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab
 }
 template <typename C>
 cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
-                      int* status) {
+                      int* status, int variant, bool probe) {
   const int TX = ZTile<C>::TX, TY = ZTile<C>::TY;
-  return with_len_xz(g.Pz, [&](auto LL) {
+  const bool any = variant == VAR_AUTO;
+  return with_len_xz(g.Pz, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && std::is_same<C, float2>::value && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
-     CUtensorMap tm;
+    if constexpr (L > 0 && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+     const C* tw = wtw_of(tab, 1);
      constexpr int LS = wlen<C>(L) + 1;
-     if (status && g.Nz == L / 3 * 2 && tab.wt[1] && (size_t)L * 16 + 128 <= (size_t)2 * LS * sizeof(C) &&
-         row_tmap(in, nf, g, sizeof(C), &tm)) {
-      // rows staged by tensor copies, 4 x 4 tile
-      const size_t sm = ((size_t)16 * LS) * sizeof(C);
-      cudaFuncSetAttribute(k_zft<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
-      k_zft<C, L, 8><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
-      return cudaGetLastError();
+     if constexpr (sizeof(C) == 8) {
+      CUtensorMap tm;
+      if ((any || variant == DNS_Z_TENSOR_COPY) && status && g.Nz == L / 3 * 2 && tw &&
+          (size_t)L * 16 + 128 <= (size_t)2 * LS * sizeof(C) && row_tmap(in, nf, g, sizeof(C), &tm)) {
+       if (probe) return cudaSuccess;
+       // rows staged by tensor copies, 4 x 4 tile
+       const size_t sm = ((size_t)16 * LS) * sizeof(C);
+       cudaFuncSetAttribute(k_zft<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+       dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
+       k_zft<C, L, 8><<<grid, 256, sm, st>>>(tm, out, g, tab, status);
+       return cudaGetLastError();
+      }
      }
-     if (g.Nz == L / 3 * 2 && tab.wt[1]) {
-      const size_t sm = ((size_t)16 * (wlen<C>(L) + 1)) * sizeof(C);
-      cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      cudaFuncSetAttribute(k_zfw<C, L, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
-      dim3 grid((g.Kx + 3) / 4, (g.Py + 3) / 4, nf);
-      k_zfw<C, L, 8><<<grid, 256, sm, st>>>(in, out, g, tab);
+     if ((any || variant == DNS_Z_WARP) && g.Nz == L / 3 * 2 && tw) {
+      if (probe) return cudaSuccess;
+      typedef ZWarpTile<C> WT;
+      const size_t sm = ((size_t)WT::TX * WT::TY * LS) * sizeof(C);
+      auto k = k_zfw<C, L, WT::NW, WT::TX, WT::TY>;
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 75);
+      dim3 grid((g.Kx + WT::TX - 1) / WT::TX, (g.Py + WT::TY - 1) / WT::TY, nf);
+      k<<<grid, 32 * WT::NW, sm, st>>>(in, out, g, tab);
       return cudaGetLastError();
      }
     }
+    if (!any && variant != DNS_Z_BLOCK) return cudaErrorNotSupported;
+    if (probe) return cudaSuccess;
     const size_t sm = (size_t)TX * TY * FLine<C, L>::stride(g.Pz) * sizeof(C);
     cudaFuncSetAttribute(k_zf<C, TX, TY, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     dim3 grid((g.Kx + TX - 1) / TX, (g.Py + TY - 1) / TY, nf);
@@ -894,7 +920,7 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
       // four rows per CTA within one wall-normal plane; a warp's 8 staged
       // rows of 128 bins fit in its 4 lines
       // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
-      const bool tw_ok = FftMaxRadix<C>::v == 8 ? tab.tw != nullptr : (tab.wt[1] && tab.wt[2]);
+      const bool tw_ok = wtw_of(tab, 1) && wtw_of(tab, 2);
       if (tw_ok && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) &&
           in.rs >= 128 && (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0) {
         const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
@@ -940,8 +966,8 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
 }
 
 #define INST_Z(C)                                                                                  \
-  template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*); \
-  template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*); \
+  template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
+  template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
                                          double, int*, cudaStream_t);                             \
   template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \

@@ -4,10 +4,10 @@
 
 template <typename C>
 cudaError_t launch_zb(PencilArr in, RowArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
-                      int* status = nullptr);
+                      int* status = nullptr, int variant = VAR_AUTO, bool probe = false);
 template <typename C>
 cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab, cudaStream_t st,
-                      int* status = nullptr);
+                      int* status = nullptr, int variant = VAR_AUTO, bool probe = false);
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
                            double Ro, int* status, cudaStream_t st);

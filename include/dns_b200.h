@@ -178,19 +178,41 @@ dns_status dns_set_wait_limit(dns_ctx* ctx, long long cycles);
 
 /* Kernel variants and the autotuner (no counterpart in the reference).  A
  * tunable pass has several compiled kernels for the same arithmetic; the
- * context starts with variant 0 of each.
+ * context starts with the first variant, in the order listed below, that it
+ * can run (the tensor-core y3 only by choice or by the autotuner).
  *   DNS_PASS_Y3: the backward wall-normal pass (getUVW + padded s2p)
- *     DNS_Y3_FFT     shared-memory FFT of the even extension (every grid);
+ *     DNS_Y3_FFT     warp-synchronous FFTs of the even extensions, two lines
+ *                    per warp (lengths with a warp plan);
  *     DNS_Y3_TENSOR  batched 3xTF32 Chebyshev products on the tensor cores
- *                    (tcgen05, FP32 accumulation): mixed form, Ny = 129.
+ *                    (tcgen05, FP32 accumulation): mixed form, Ny = 129;
+ *     DNS_Y3_BLOCK   block-wide FFT (every grid).
+ *   DNS_PASS_Y1: the forward wall-normal pass (p2s, nonlinear terms,
+ *     right-hand sides): DNS_Y1_WARP (one warp per Lamb line, lengths with a
+ *     warp plan) or DNS_Y1_BLOCK (every grid).
+ *   DNS_PASS_ZB, DNS_PASS_ZF: the spanwise inverse / forward passes:
+ *     DNS_Z_TENSOR_COPY  warp FFTs on tiles staged by tensor copies (mixed
+ *                        form, Nz <= 256);
+ *     DNS_Z_WARP         warp FFTs on tiles gathered through L1;
+ *     DNS_Z_BLOCK        block-wide FFT (every grid).
  * dns_set_variant fails with DNS_ERR_ARG for a variant this context cannot
- * run.  dns_autotune times every available variant of every tunable pass on
- * this context's buffers and grid (the state is not modified), keeps the
- * fastest and, if ms is not NULL, writes the mean times in ms to
- * ms[pass * DNS_MAX_VARIANTS + variant] (-1 where unavailable).  Synchronous;
- * the next dns_step captures the step graph again. */
-enum { DNS_PASS_Y3 = 0, DNS_NUM_PASSES = 1, DNS_MAX_VARIANTS = 4 };
-enum { DNS_Y3_FFT = 0, DNS_Y3_TENSOR = 1 };
+ * run.  dns_autotune times every available variant of every tunable pass
+ * inside whole steps on this context's buffers and grid (state and AB2
+ * history are saved and put back: the state is not modified), keeps the
+ * fastest of each pass and, if ms is not NULL, writes the mean times in ms
+ * to ms[pass * DNS_MAX_VARIANTS + variant] (-1 where unavailable).  It needs
+ * a state (dns_set_state or dns_init_flow).  Synchronous; the next dns_step
+ * captures the step graph again. */
+enum {
+  DNS_PASS_Y3 = 0,
+  DNS_PASS_Y1 = 1,
+  DNS_PASS_ZB = 2,
+  DNS_PASS_ZF = 3,
+  DNS_NUM_PASSES = 4,
+  DNS_MAX_VARIANTS = 4
+};
+enum { DNS_Y3_FFT = 0, DNS_Y3_TENSOR = 1, DNS_Y3_BLOCK = 2 };
+enum { DNS_Y1_WARP = 0, DNS_Y1_BLOCK = 1 };
+enum { DNS_Z_TENSOR_COPY = 0, DNS_Z_WARP = 1, DNS_Z_BLOCK = 2 };
 dns_status dns_set_variant(dns_ctx* ctx, int pass, int variant);
 dns_status dns_get_variant(const dns_ctx* ctx, int pass, int* variant);
 dns_status dns_autotune(dns_ctx* ctx, double* ms);
@@ -265,8 +287,21 @@ dns_status dns_solve_eq(dns_ctx* ctx, const void* inv, void* rhs, int N, size_t 
  * Either pointer may be NULL: that system is not touched (the reference
  * solves v before it forms the omega_y right-hand side).  where = DNS_HOST
  * or DNS_DEVICE.  Synchronous; allocates its vectors (2 H Ny + 6 H complex)
- * on first use. */
+ * on first use.  On device pencils with both systems the whole sequence
+ * (right-hand-side preparation, DCT-I, integration, the banded solve of all
+ * pencils in one launch, the wall polynomial added back) is one CUDA graph,
+ * captured on the first call with those buffers and launched on each. */
 dns_status dns_solve_wall(dns_ctx* ctx, void* v, void* omega, size_t tpitch, int where);
+/* No counterpart in the reference.  Residual of solved systems: b the
+ * collocation right-hand sides as dns_solve_wall takes them, x the
+ * solutions it returned, A the reference's operators
+ * (source/coefficient.cu:7-86).  out[0], out[1]: largest per-pencil
+ * ||A x - b||_2 / ||b||_2 of the v and the omega systems; out[2], out[3]:
+ * the same over all pencils together; out[4], out[5]: largest normwise
+ * backward error ||A x - b||_inf / (||A||_inf ||x||_inf + ||b||_inf).
+ * Synchronous; O(H Ny^2) on the device. */
+dns_status dns_solve_residual(dns_ctx* ctx, const void* b_v, const void* b_omega, const void* x_v,
+                              const void* x_omega, size_t tpitch, int where, double out[6]);
 /* initAuxMatrix (source/solver.cpp:260-320): explicit inverses of the v and
  * omega operators of every pencil, row-major [ky][kx][nz][nz] complex. */
 dns_status dns_init_aux_matrix(dns_ctx* ctx, void* inv_v, void* inv_omega, int where);

@@ -157,6 +157,7 @@ def test_solve_wall_384x193x384(pkg):
         t0 = time.perf_counter()
         ctx.solve_wall(wv.data_ptr(), wo.data_ptr(), L * 16)
         ms.append((time.perf_counter() - t0) * 1e3)
+    res = ctx.solve_residual(tv.data_ptr(), to.data_ptr(), wv.data_ptr(), wo.data_ptr(), L * 16)
     xv = wv.cpu().numpy()
     xo = wo.cpu().numpy()
     # host buffers give the same result
@@ -170,7 +171,49 @@ def test_solve_wall_384x193x384(pkg):
     picks += [(int(r.integers(sz.hnx)), int(r.integers(sz.ny))) for _ in range(25)]
     worst = _check_all(p, sz, picks, bv, bo, xv, xo)
     print(f"\n384x193x384 solve: {min(ms):.2f} ms per call (both systems, 74 112 pencils, "
-          f"synchronous); {_report(worst)}")
+          f"synchronous); {_report(worst)}; device residual over all pencils {res}")
+    assert max(res[4], res[5]) < 1e-13, res  # normwise backward error, every pencil
+
+
+@pytest.mark.parametrize("case", CASES[:2])
+def test_solve_residual_planted(pkg, case):
+    """dns_solve_residual on x and b = A x + delta with a planted delta
+    (1e-6 |A x| per pencil, far above the rounding of A x): the reported
+    relative residuals and backward errors equal numpy's figures for delta."""
+    case = dict(case)
+    U = case.pop("U", (0.5, 0.5, 0.0))
+    p = O.Params(case["mx"], case["my"], case["mz"], Re=case["Re"], Ro=case["Ro"], dt=case["dt"], prof=U)
+    sz = O.Sizes(p.mx, p.my, p.mz)
+    rng = np.random.default_rng(11)
+    shape = (sz.ny, sz.hnx, sz.nz)
+    xv = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    xo = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    bv, bo = np.empty_like(xv), np.empty_like(xo)
+    rel = np.zeros((2, sz.ny, sz.hnx))
+    sums = np.zeros(4)
+    bw = np.zeros(2)
+    for ky in range(sz.ny):
+        for kx in range(sz.hnx):
+            As = _dense(p, sz, kx, ky)
+            for k, (A, x, b) in enumerate(zip(As, (xv, xo), (bv, bo))):
+                ax = A @ x[ky, kx]
+                d = rng.standard_normal(sz.nz) + 1j * rng.standard_normal(sz.nz)
+                d *= 1e-6 * np.linalg.norm(ax) / np.linalg.norm(d)
+                b[ky, kx] = ax + d
+                rel[k, ky, kx] = np.linalg.norm(d) / np.linalg.norm(b[ky, kx])
+                sums[2 * k] += np.linalg.norm(d) ** 2
+                sums[2 * k + 1] += np.linalg.norm(b[ky, kx]) ** 2
+                an = np.abs(A).sum(axis=1).max()
+                bw[k] = max(bw[k], np.abs(d).max() / (an * np.abs(x[ky, kx]).max() + np.abs(b[ky, kx]).max()))
+    want = [rel[0].max(), rel[1].max(), np.sqrt(sums[0] / sums[1]), np.sqrt(sums[2] / sums[3]), bw[0], bw[1]]
+    ctx = pkg.Context(pkg.make_params(p.mx, p.my, p.mz, Re=p.Re, Ro=p.Ro, dt=p.dt, U=U))
+    got_h = ctx.solve_residual(bv, bo, xv, xo, sz.nz * 16, where=pkg.HOST)
+    t = [torch.from_numpy(a).cuda() for a in (bv, bo, xv, xo)]
+    torch.cuda.synchronize()
+    got_d = ctx.solve_residual(*(a.data_ptr() for a in t), sz.nz * 16)
+    ctx.close()
+    assert got_h == got_d
+    np.testing.assert_allclose(got_d, want, rtol=1e-6)
 
 
 def test_solve_wall_one_system(pkg):

@@ -111,13 +111,14 @@ def test_variants_and_autotune(pkg):
     V0, O0 = pkg.seeded_state(32, 129, 32, amplitude=0.1, seed=0)
     c.set_state(V0, O0)
     times = c.autotune()[pkg.PASS_Y3]
-    assert set(times) == {pkg.Y3_FFT, pkg.Y3_TENSOR} and all(t > 0 for t in times.values())
+    assert set(times) == {pkg.Y3_FFT, pkg.Y3_TENSOR, pkg.Y3_BLOCK} and all(t > 0 for t in times.values())
     assert c.get_variant(pkg.PASS_Y3) == min(times, key=times.get)
     c.close()
     d = ctx_for(pkg, 48, 48, 256, pkg.PREC_MIXED)  # Ny = 65: no tensor variant
     with pytest.raises(pkg.DnsError):
         d.set_variant(pkg.PASS_Y3, pkg.Y3_TENSOR)
-    assert set(d.autotune()[pkg.PASS_Y3]) == {pkg.Y3_FFT}
+    d.set_state(*pkg.seeded_state(32, 65, 32, amplitude=0.1, seed=0))
+    assert set(d.autotune()[pkg.PASS_Y3]) == {pkg.Y3_FFT, pkg.Y3_BLOCK}
     d.close()
     e = ctx_for(pkg, 48, 48, 512, pkg.PREC_FP64)
     with pytest.raises(pkg.DnsError):

@@ -1,0 +1,80 @@
+"""GPU: every compiled variant of every tunable pass (wall-normal backward and
+forward passes, spanwise inverse and forward passes) gives the step of the
+default variants: in FP64 to 1e-12 relative (the parity bar; measured
+differences are rounding, ~1e-15), in the mixed form to 1e-6 against the
+FP64 step.  192x192x128 (128x33x128 modes): lengths with warp plans in both
+precisions (Pz = 192, M = 128), so every variant is available; 3 steps after
+the bootstrap from the seeded state, Re 1300, Ro 0.1, dt 0.005."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _run(pkg, prec, variants=None, steps=3):
+    c = pkg.Context(pkg.make_params(192, 192, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+    for p, v in (variants or {}).items():
+        c.set_variant(p, v)
+    c.set_state(*pkg.seeded_state(128, 33, 128, amplitude=0.1, seed=0))
+    c.bootstrap()
+    c.step(steps)
+    V, O = c.get_state()
+    got = {p: c.get_variant(p) for p in range(pkg.NUM_PASSES)}
+    c.close()
+    return V, O, got
+
+
+def _available(pkg, prec):
+    c = pkg.Context(pkg.make_params(192, 192, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+    out = {}
+    for p in range(pkg.NUM_PASSES):
+        out[p] = []
+        for v in range(pkg.MAX_VARIANTS):
+            try:
+                c.set_variant(p, v)
+                out[p].append(v)
+            except pkg.DnsError:
+                pass
+    c.close()
+    return out
+
+
+def test_available_variants(pkg):
+    a64 = _available(pkg, pkg.PREC_FP64)
+    amx = _available(pkg, pkg.PREC_MIXED)
+    assert a64 == {pkg.PASS_Y3: [pkg.Y3_FFT, pkg.Y3_BLOCK], pkg.PASS_Y1: [pkg.Y1_WARP, pkg.Y1_BLOCK],
+                   pkg.PASS_ZB: [pkg.Z_WARP, pkg.Z_BLOCK], pkg.PASS_ZF: [pkg.Z_WARP, pkg.Z_BLOCK]}
+    assert amx[pkg.PASS_ZB] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
+    assert amx[pkg.PASS_ZF] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
+    assert amx[pkg.PASS_Y1] == [pkg.Y1_WARP, pkg.Y1_BLOCK]
+    assert amx[pkg.PASS_Y3] == [pkg.Y3_FFT, pkg.Y3_BLOCK]  # the tensor form needs Ny = 129
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_every_variant_same_step(pkg, prec, parity_log):
+    P = pkg.PREC_FP64 if prec == "fp64" else pkg.PREC_MIXED
+    V64, O64, _ = _run(pkg, pkg.PREC_FP64)
+    base = (V64, O64)
+    tol = 1e-12 if prec == "fp64" else 1e-6
+    avail = _available(pkg, P)
+    worst = {}
+    for p, vs in avail.items():
+        for v in vs:
+            V, O, got = _run(pkg, P, {p: v})
+            assert got[p] == v
+            e = max(_rel(V, base[0]), _rel(O, base[1]))
+            worst[f"{pkg.PASS_NAMES[p]}:{pkg.VARIANT_NAMES[p][v]}"] = e
+            assert e < tol, (prec, pkg.PASS_NAMES[p], pkg.VARIANT_NAMES[p][v], e)
+    parity_log.append(f"variants, {prec}, 3 steps at 192x192x128 vs the FP64 default step: " +
+                      ", ".join(f"{k} {e:.1e}" for k, e in worst.items()))
