@@ -134,7 +134,7 @@ dns_status build_wall_solver(dns_ctx* c) {
   wd.group_complex = pk.group_complex;
   wd.nslots = (long long)g.Kx * g.Kh;
   wd.ngroups = (wd.nslots + 15) / 16;
-  if (wall_smem_bytes(wd) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
+  if (wall_smem_bytes(wd, DNS_Y2_RING2_8K_EF) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
   if (wall_scratch_complex(wd) * 16 > c->F6_bytes)
     return fail(DNS_ERR_ARG, "wall solve scratch does not fit the transform buffer");
   CK(c->alloc(&c->wfac, fac.size()));
@@ -199,8 +199,10 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
     return e;
   mark();
   if (!boot)
-    if ((e = launch_wall_solve(c->wfac, b.V, b.O, c->rv, c->ro, c->wQ, (double2*)c->F6, c->wd, g,
-                               c->ph, c->status, c->st)))
+    if ((e = var(DNS_PASS_Y2, [&](int v) {
+           return launch_wall_solve(c->wfac, b.V, b.O, c->rv, c->ro, c->wQ, (double2*)c->F6, c->wd, g, c->ph,
+                                    c->status, c->st, v == VAR_AUTO ? DNS_Y2_RING2_8K_EF : v);
+         })))
       return e;
   mark();
   return cudaSuccess;
@@ -238,6 +240,8 @@ bool probe_pass(const dns_ctx* c, int pass, int v, const DevFft<C>& fz, const De
       return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
     case DNS_PASS_ZF:
       return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
+    case DNS_PASS_Y2:
+      return v < DNS_WALL_VARIANTS && wall_smem_bytes(c->wd, v) <= 227 * 1024;
   }
   return false;
 }
@@ -251,10 +255,12 @@ void default_variants(dns_ctx* c) {
   const bool mixed = c->P.precision == DNS_PREC_MIXED;
   static const int order_mixed[DNS_NUM_PASSES][3] = {
       {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
-      {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}, {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}};
+      {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}, {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK},
+      {DNS_Y2_RING3_12K, DNS_Y2_RING2_8K_EF, -1}};
   static const int order_fp64[DNS_NUM_PASSES][3] = {
       {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
-      {DNS_Z_WARP, DNS_Z_BLOCK, -1}, {DNS_Z_WARP, DNS_Z_BLOCK, -1}};
+      {DNS_Z_WARP, DNS_Z_BLOCK, -1}, {DNS_Z_WARP, DNS_Z_BLOCK, -1},
+      {DNS_Y2_RING3_12K, DNS_Y2_RING2_8K_EF, -1}};
   for (int p = 0; p < DNS_NUM_PASSES; ++p) {
     const int* ord = mixed ? order_mixed[p] : order_fp64[p];
     c->variant[p] = ord[0];
@@ -709,7 +715,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   int keep[DNS_NUM_PASSES];
   for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = c->variant[p];
   // kernel slot of each pass in a step's events
-  static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3};
+  static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3, 5};
   const int ne = DNS_NUM_KERNELS + 1, nt = 3;
   std::vector<cudaEvent_t> ev((size_t)ne * (nt + 1));
   for (auto& x : ev)
@@ -1029,7 +1035,10 @@ cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo,
   WallDims wd = c->wd;
   wd.tilt = 0;
   if (!e) e = launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph,
-                                c->status, c->st);
+                                c->status, c->st, c->variant[DNS_PASS_Y2]);
+  if (e == cudaErrorNotSupported)
+    e = launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph, c->status, c->st,
+                          DNS_Y2_RING2_8K_EF);
   if (!e) e = launch_colloc_finish(Xv, Xo, pbc, ov, oo, op, g, c->st);
   return e;
 }

@@ -27,22 +27,33 @@
 
 namespace {
 
-constexpr int WALL_NST = 3;          // ring stages
-constexpr int WALL_STG = 12288;      // bytes per stage
 constexpr int WALL_HDR = 128;        // mbarriers
 
-__host__ __device__ constexpr int rows_per_chunk(int entries, int cap) {
-  return (WALL_STG / (entries * 256)) < cap ? (WALL_STG / (entries * 256)) : cap;
+// Variants (the solve's tunable block shape): ring stages, bytes per stage,
+// whether the tilting table sits in shared memory (else read through L1),
+// and whether the factor stream is read with the L2 evict-first policy (the
+// scratch vectors then stay in L2).  Smaller rings leave room for more CTAs
+// per SM.
+struct WallVar {
+  int nst, stg;
+  bool qsm, ef;
+};
+constexpr WallVar kWallVar[DNS_WALL_VARIANTS] = {
+    {3, 12288, true, false}, {3, 12288, true, true}, {2, 8192, false, true}, {3, 8192, false, true}};
+
+__host__ __device__ constexpr int rows_per_chunk(int stg, int entries, int cap) {
+  return (stg / (entries * 256)) < cap ? (stg / (entries * 256)) : cap;
 }
 
 __device__ __forceinline__ double2 sel(bool p, double2 a) { return p ? a : make_double2(0.0, 0.0); }
 
-template <int KLV, int KUV, int KLO, int KUO>
+template <int KLV, int KUV, int KLO, int KUO, int STG>
 struct WallCfg {
   static constexpr int E0 = KLV, E1 = 1 + KUV + 2, E2 = KLO, E3 = 1 + KUO;
   // rows per ring chunk; the solve keeps two chunks of vector rows in registers
-  static constexpr int R0 = rows_per_chunk(E0, 12), R1 = rows_per_chunk(E1, 12);
-  static constexpr int R2 = rows_per_chunk(E2, 8), R3 = rows_per_chunk(E3, 12);
+  static constexpr int R0 = rows_per_chunk(STG, E0, 12), R1 = rows_per_chunk(STG, E1, 12);
+  static constexpr int R2 = rows_per_chunk(STG, E2, 8), R3 = rows_per_chunk(STG, E3, 12);
+  static_assert(R0 > 0 && R1 > 0 && R2 > 0 && R3 > 0, "stage too small for a row");
 };
 
 // chunk c of a group's stream: byte count and offset (complex values)
@@ -69,19 +80,20 @@ __device__ __forceinline__ void chunk_of(int c, const WallDims& wd, uint32_t& by
 
 }  // namespace
 
-template <int KLV, int KUV, int KLO, int KUO>
+template <int KLV, int KUV, int KLO, int KUO, int WALL_NST, int WALL_STG, bool QSM, bool EF>
 __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ fac, double2* V,
                                                    double2* O, const double2* __restrict__ gv,
                                                    const double2* __restrict__ go,
                                                    const double* __restrict__ Qg, double2* Sw,
                                                    WallDims wd, DnsGeom g, PhysParams ph, int* status) {
-  typedef WallCfg<KLV, KUV, KLO, KUO> CF;
+  typedef WallCfg<KLV, KUV, KLO, KUO, WALL_STG> CF;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* full = (uint64_t*)smem_raw;
   double2* ring = (double2*)(smem_raw + WALL_HDR);
-  double* Qs = (double*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG);
+  double* Qsm = (double*)(smem_raw + WALL_HDR + WALL_NST * WALL_STG);
+  const double* Qs = QSM ? Qsm : Qg;  // tilting table: shared memory or through L1
   // recombination weights 2k/(k+1), (k-3)/(k-1) of the clamped basis, k <= N
-  double* rc2 = Qs + wd.qbytes / 8;
+  double* rc2 = Qsm + (QSM ? wd.qbytes / 8 : 0);
   double* rc4 = rc2 + g.Ny;
 
   const int lane = threadIdx.x;
@@ -109,13 +121,15 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   const int nch2 = (wd.no + CF::R2 - 1) / CF::R2, nch3 = (wd.no + CF::R3 - 1) / CF::R3;
   const int total = nch0 + nch1 + nch2 + nch3;
 
+  const uint64_t pol = EF ? l2_evict_first() : 0;
   auto issue = [&](int c) {
     uint32_t bytes;
     long long off;
     chunk_of<CF>(c, wd, bytes, off);
     uint64_t* bar = &full[c % WALL_NST];
     mbar_expect_tx(bar, bytes);
-    bulk_g2s(ring + (size_t)(c % WALL_NST) * (WALL_STG / 16), gfac + off, bytes, bar);
+    if (EF) bulk_g2s_hint(ring + (size_t)(c % WALL_NST) * (WALL_STG / 16), gfac + off, bytes, bar, pol);
+    else bulk_g2s(ring + (size_t)(c % WALL_NST) * (WALL_STG / 16), gfac + off, bytes, bar);
   };
   // on a timed-out wait: report, let the copies in flight land, leave
   auto abort_at = [&](int c) {
@@ -148,7 +162,8 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
     fence_mbar_init();
   }
   __syncwarp();
-  for (int k = lane; k < 7 * wd.no; k += 32) Qs[k] = Qg[k];
+  if (QSM)
+    for (int k = lane; k < 7 * wd.no; k += 32) Qsm[k] = Qg[k];
   for (int k = lane; k < g.Ny; k += 32) {
     rc2[k] = 2.0 * k / (k + 1);
     rc4[k] = (k >= 4) ? (double)(k - 3) / (double)(k - 1) : 0.0;
@@ -224,7 +239,7 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
       for (int j = 0; j < 7; ++j) {
         if (DEG == 0 || (DEG == 1 && (j & 1) == 0)) continue;
         const int r = k + 1 - j;
-        if (r >= 0 && r < wd.no) P[j] = P[j] + a * Qs[7 * r + j];
+        if (r >= 0 && r < wd.no) P[j] = P[j] + a * (QSM ? Qs[7 * r + j] : __ldg(Qs + 7 * r + j));
       }
       if (k + 1 < wd.no) S[32 * (k + 1)] = muli(P[0] * kap);
 #pragma unroll
@@ -383,8 +398,9 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
   }
 }
 
-size_t wall_smem_bytes(const WallDims& wd) {
-  return (size_t)WALL_HDR + (size_t)WALL_NST * WALL_STG + wd.qbytes + (size_t)2 * (wd.nv + 2) * 8;
+size_t wall_smem_bytes(const WallDims& wd, int variant) {
+  const WallVar& v = kWallVar[variant];
+  return (size_t)WALL_HDR + (size_t)v.nst * v.stg + (v.qsm ? wd.qbytes : 0) + (size_t)2 * (wd.nv + 2) * 8;
 }
 size_t wall_scratch_complex(const WallDims& wd) { return (size_t)wd.ngroups * 32 * wd.nv; }
 
@@ -396,26 +412,42 @@ bool wall_band_of(int delta, int* klv, int* kuv, int* klo, int* kuo) {
   return true;
 }
 
-template <int A, int B, int C, int D>
+template <int A, int B, int C, int D, int VAR>
 static cudaError_t launch_inst(const double2* fac, double2* V, double2* O, const double2* gv,
                                const double2* go, const double* Q, double2* Sw, const WallDims& wd,
                                const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
-  const size_t sm = wall_smem_bytes(wd);
-  cudaError_t e = cudaFuncSetAttribute(k_wall_solve<A, B, C, D>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  constexpr WallVar v = kWallVar[VAR];
+  auto k = k_wall_solve<A, B, C, D, v.nst, v.stg, v.qsm, v.ef>;
+  const size_t sm = wall_smem_bytes(wd, VAR);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e) return e;
-  k_wall_solve<A, B, C, D><<<(unsigned)wd.ngroups, 32, sm, st>>>(fac, V, O, gv, go, Q, Sw, wd, g, ph,
-                                                                  status);
+  k<<<(unsigned)wd.ngroups, 32, sm, st>>>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status);
   return cudaGetLastError();
+}
+
+template <int A, int B, int C, int D>
+static cudaError_t launch_var(int variant, const double2* fac, double2* V, double2* O, const double2* gv,
+                              const double2* go, const double* Q, double2* Sw, const WallDims& wd,
+                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
+  switch (variant) {
+    case 0: return launch_inst<A, B, C, D, 0>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 1: return launch_inst<A, B, C, D, 1>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 2: return launch_inst<A, B, C, D, 2>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 3: return launch_inst<A, B, C, D, 3>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+  }
+  return cudaErrorNotSupported;
 }
 
 cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const double2* gv,
                               const double2* go, const double* Q, double2* Sw, const WallDims& wd,
-                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st) {
+                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st,
+                              int variant) {
+  if (variant < 0 || variant >= DNS_WALL_VARIANTS) return cudaErrorNotSupported;
+  if (wall_smem_bytes(wd, variant) > 227 * 1024) return cudaErrorNotSupported;
   switch (wd.delta) {
-    case 0: return launch_inst<4, 8, 2, 4>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
-    case 1: return launch_inst<5, 9, 3, 6>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
-    case 2: return launch_inst<6, 10, 4, 8>(fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 0: return launch_var<4, 8, 2, 4>(variant, fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 1: return launch_var<5, 9, 3, 6>(variant, fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
+    case 2: return launch_var<6, 10, 4, 8>(variant, fac, V, O, gv, go, Q, Sw, wd, g, ph, status, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -16,12 +16,16 @@ struct WallDims {
 
 // band instance (v lower/upper, omega lower/upper) for base-flow degree delta
 bool wall_band_of(int delta, int* klv, int* kuv, int* klo, int* kuo);
-size_t wall_smem_bytes(const WallDims& wd);
+#define DNS_WALL_VARIANTS 4
+// block shapes of the solve (ring stages x stage bytes, tilting table
+// placement): variant 0 .. DNS_WALL_VARIANTS - 1
+size_t wall_smem_bytes(const WallDims& wd, int variant);
 // complex values of the solve's global scratch (Sw of the launcher)
 size_t wall_scratch_complex(const WallDims& wd);
 cudaError_t launch_wall_solve(const double2* fac, double2* V, double2* O, const double2* gv,
                               const double2* go, const double* Q, double2* Sw, const WallDims& wd,
-                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st);
+                              const DnsGeom& g, const PhysParams& ph, int* status, cudaStream_t st,
+                              int variant = 0);
 
 // Solve-only entry (wallentry.cu): collocation right-hand sides in the
 // reference's pencil layout -> integrated right-hand sides of the banded

@@ -1,5 +1,6 @@
 """GPU: every compiled variant of every tunable pass (wall-normal backward and
-forward passes, spanwise inverse and forward passes) gives the step of the
+forward passes, spanwise inverse and forward passes, the block shapes of the
+banded solve) gives the step of the
 default variants: in FP64 to 1e-12 relative (the parity bar; measured
 differences are rounding, ~1e-15), in the mixed form to 1e-6 against the
 FP64 step.  192x192x128 (128x33x128 modes): lengths with warp plans in both
@@ -53,8 +54,11 @@ def _available(pkg, prec):
 def test_available_variants(pkg):
     a64 = _available(pkg, pkg.PREC_FP64)
     amx = _available(pkg, pkg.PREC_MIXED)
+    rings = [pkg.Y2_RING3_12K, pkg.Y2_RING3_12K_EF, pkg.Y2_RING2_8K_EF, pkg.Y2_RING3_8K_EF]
     assert a64 == {pkg.PASS_Y3: [pkg.Y3_FFT, pkg.Y3_BLOCK], pkg.PASS_Y1: [pkg.Y1_WARP, pkg.Y1_BLOCK],
-                   pkg.PASS_ZB: [pkg.Z_WARP, pkg.Z_BLOCK], pkg.PASS_ZF: [pkg.Z_WARP, pkg.Z_BLOCK]}
+                   pkg.PASS_ZB: [pkg.Z_WARP, pkg.Z_BLOCK], pkg.PASS_ZF: [pkg.Z_WARP, pkg.Z_BLOCK],
+                   pkg.PASS_Y2: rings}
+    assert amx[pkg.PASS_Y2] == rings
     assert amx[pkg.PASS_ZB] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
     assert amx[pkg.PASS_ZF] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
     assert amx[pkg.PASS_Y1] == [pkg.Y1_WARP, pkg.Y1_BLOCK]
