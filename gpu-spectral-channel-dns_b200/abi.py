@@ -30,6 +30,7 @@ EXPORTS = [
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
     "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
+    "dns_slab_create", "dns_slab_exchange_bytes", "dns_slab_local", "dns_slab_part",
     "dns_nonlinear", "dns_rhs_v", "dns_rhs_omega", "dns_rhs_mean", "dns_operator_matrices",
     "dns_operator_tables", "dns_set_wait_limit", "dns_set_variant", "dns_get_variant",
     "dns_autotune", "dns_solve_residual",
@@ -53,6 +54,8 @@ VARIANT_NAMES = {
 }
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1
+SLAB_Y3, SLAB_XZ, SLAB_Y1 = 0, 1, 2
+SLAB_V, SLAB_OMEGA, SLAB_NV, SLAB_NOMEGA = 0, 1, 2, 3
 
 
 class SlabSegment(C.Structure):
@@ -153,6 +156,10 @@ def load_library(path: str | None = None):
         "dns_check_state": [vp],
         "dns_slab_ranges": [i, i, i, i, i, C.POINTER(C.c_int)],
         "dns_slab_segments": [i, i, i, i, i, i, C.POINTER(SlabSegment), i, C.POINTER(C.c_int)],
+        "dns_slab_create": [C.POINTER(DnsParams), i, i, C.POINTER(vp)],
+        "dns_slab_exchange_bytes": [vp, i, C.POINTER(sz), C.POINTER(sz)],
+        "dns_slab_local": [vp, i, vp, i, i],
+        "dns_slab_part": [vp, i, i, vp, vp],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -458,3 +465,61 @@ class Context:
             self._call("dns_init_aux_matrix", inv_v.ctypes.data, inv_o.ctypes.data, HOST)
         else:
             self._call("dns_init_aux_matrix", C.c_void_p(inv_v), C.c_void_p(inv_o), DEVICE)
+
+
+class SlabContext(Context):
+    """One rank of a slab-decomposed step (``dns_slab_create``): the pencils
+    of its operator slots and the wall-normal planes of its range.  A step
+    is ``part(SLAB_Y3)``, exchange 0, ``part(SLAB_XZ)``, exchange 1,
+    ``part(SLAB_Y1)``; the exchanges are the caller's (``slab.py``)."""
+
+    def __init__(self, params: DnsParams, nranks: int, rank: int):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib, self.lib.dns_slab_create(C.byref(params), int(nranks), int(rank), C.byref(h)))
+        self.h = h
+        self.params = params
+        g = (C.c_int * 8)()
+        _check(self.lib, self.lib.dns_geometry(self.h, g))
+        self.Nx, self.Ny, self.Nz, self.Kx, self.Px, self.Py, self.Pz, self.H = list(g)
+        self.nranks, self.rank = int(nranks), int(rank)
+        self.ranges = slab_ranges(params.mx, params.my, params.mz, nranks, rank)
+        self.np = self.ranges[4]
+        segs = slab_segments(params.mx, params.my, params.mz, nranks, rank, SLAB_PENCILS)
+        self.runs = sorted({(sg["kz0"], sg["nkz"], sg["local_row0"]) for sg in segs}, key=lambda t: t[2])
+        # global pencil index p = kz Kx + kx of each local row
+        self.pencils = np.concatenate([np.arange(kz0 * self.Kx, (kz0 + nkz) * self.Kx)
+                                       for kz0, nkz, _ in self.runs]).astype(np.int64)
+
+    def exchange_bytes(self, exchange):
+        """(send bytes per peer, recv bytes per peer) of exchange 0 or 1."""
+        snd = (C.c_size_t * self.nranks)()
+        rcv = (C.c_size_t * self.nranks)()
+        self._call("dns_slab_exchange_bytes", int(exchange), snd, rcv)
+        return list(snd), list(rcv)
+
+    def set_local(self, which, a):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.shape != (self.np, self.Ny):
+            raise ValueError(f"expected shape {(self.np, self.Ny)}, got {a.shape}")
+        self._call("dns_slab_local", int(which), C.c_void_p(a.ctypes.data), HOST, 1)
+
+    def get_local(self, which):
+        a = np.empty((self.np, self.Ny), dtype=np.complex128)
+        self._call("dns_slab_local", int(which), C.c_void_p(a.ctypes.data), HOST, 0)
+        return a
+
+    def scatter_state(self, V, O):
+        """This rank's pencils of whole-grid (Nz, Kx, Ny) arrays."""
+        self.set_local(SLAB_V, np.asarray(V).reshape(self.H, self.Ny)[self.pencils])
+        self.set_local(SLAB_OMEGA, np.asarray(O).reshape(self.H, self.Ny)[self.pencils])
+
+    def gather_state(self, V, O):
+        """Write this rank's pencils into whole-grid (Nz, Kx, Ny) arrays."""
+        V.reshape(self.H, self.Ny)[self.pencils] = self.get_local(SLAB_V)
+        O.reshape(self.H, self.Ny)[self.pencils] = self.get_local(SLAB_OMEGA)
+
+    def part(self, part, send_ptr, recv_ptr, boot=False):
+        """Enqueue one part on the context's stream (asynchronous)."""
+        self._call("dns_slab_part", int(part), int(bool(boot)), C.c_void_p(send_ptr or None),
+                   C.c_void_p(recv_ptr or None))

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -95,8 +96,14 @@ bool fft_len_ok(int L) {
 long long roundup(long long a, long long b) { return (a + b - 1) / b * b; }
 }  // namespace
 
+dns_status ctx_check_status(dns_ctx* c);
+dns_status ctx_build_wall_solver(dns_ctx* c);
 namespace {
-dns_status check_status(dns_ctx* c) {
+dns_status check_status(dns_ctx* c) { return ctx_check_status(c); }
+dns_status build_wall_solver(dns_ctx* c) { return ctx_build_wall_solver(c); }
+}  // namespace
+
+dns_status ctx_check_status(dns_ctx* c) {
   int s = 0;
   CK(cudaMemcpyAsync(&s, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -110,9 +117,10 @@ dns_status check_status(dns_ctx* c) {
   return DNS_OK;
 }
 
-// Factor the banded wall-normal systems of every operator slot on the host
-// threads and upload them (once per context, before the first step).
-dns_status build_wall_solver(dns_ctx* c) {
+// Factor the banded wall-normal systems of every operator slot (a slab
+// rank: of its slots) on the host threads and upload them (once per
+// context, before the first step).
+dns_status ctx_build_wall_solver(dns_ctx* c) {
   if (c->wall_ready) return DNS_OK;
   const DnsGeom& g = c->g;
   const int N = g.Ny - 1;
@@ -124,6 +132,18 @@ dns_status build_wall_solver(dns_ctx* c) {
   const wall::Packing pk = wall::make_packing(sv, so);
   wall::Grid gr{N, g.Kx, g.Nz, g.Kh, c->ph.aphi, c->ph.beta, c->ph.Re, c->ph.dt,
                 c->ph.U0, c->ph.U1, c->ph.U2};
+  const SlabState* sl = c->slab;
+  if (sl) {
+    gr.kz0 = sl->s0;
+    gr.nkz = sl->s1 - sl->s0;
+    // run 0 holds kz = kz' in [s0, s1) in slot order; run 1 the mirrored
+    // pencils kz = Nz - kz'
+    wd.kzs0 = sl->s0;
+    wd.kza = sl->run[0].kz0;
+    wd.rowa = sl->run[0].row0;
+    wd.kzb = sl->nruns > 1 ? sl->run[1].kz0 : 0;
+    wd.rowb = sl->nruns > 1 ? sl->run[1].row0 : 0;
+  }
   std::vector<wall::cx> fac;
   unsigned nt = std::thread::hardware_concurrency();
   const std::string err = wall::pack_grid(gr, sv, so, fac, (int)std::min(32u, std::max(1u, nt)));
@@ -132,7 +152,7 @@ dns_status build_wall_solver(dns_ctx* c) {
   if (!wall::tilting_table(N, wd.no, c->ph.U1, c->ph.U2, Q.data()))
     return fail(DNS_ERR_ARG, "tilting table outside its band");
   wd.group_complex = pk.group_complex;
-  wd.nslots = (long long)g.Kx * g.Kh;
+  wd.nslots = (long long)g.Kx * (sl ? sl->s1 - sl->s0 : g.Kh);
   wd.ngroups = (wd.nslots + 15) / 16;
   if (wall_smem_bytes(wd, DNS_Y2_RING2_8K_EF) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
   if (wall_scratch_complex(wd) * 16 > c->F6_bytes)
@@ -145,6 +165,7 @@ dns_status build_wall_solver(dns_ctx* c) {
   return DNS_OK;
 }
 
+namespace {
 // the state and AB2 history a pass sequence reads and writes
 struct StepBufs {
   double2 *V, *O, *Nvp, *Nop;
@@ -342,7 +363,14 @@ dns_status dns_read_parameter_file(const char* path, dns_params* p, dns_run_para
   return DNS_OK;
 }
 
-dns_status dns_create(const dns_params* p, dns_ctx** out) {
+dns_status dns_create(const dns_params* p, dns_ctx** out) { return ctx_create(p, nullptr, out); }
+
+// A context of the whole grid (slab == NULL) or of one slab rank: then the
+// pencil arrays hold the rank's pencils only and the transform buffers its
+// pencils (all planes) and its planes (all pencils); the context takes
+// ownership of slab.
+dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out) {
+  std::unique_ptr<SlabState> own(slab);
   if (!p || !out) return fail(DNS_ERR_ARG, "null argument");
   *out = nullptr;
   if (p->mx <= 0 || p->my <= 0 || p->mz <= 0 || p->mz % 4 != 0)
@@ -364,6 +392,7 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   CK(cudaSetDevice(p->device));
 
   dns_ctx* c = new dns_ctx();
+  c->slab = own.release();
   c->P = *p;
   c->g = g;
   c->ph.aphi = p->n_pi_x / 2;
@@ -397,15 +426,24 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
   host_base_flow(g.Py, p->U0, p->U1, p->U2, Uy.data(), nullptr, nullptr);
   const size_t NN = (size_t)Ny * Ny;
   const size_t csz = p->precision == DNS_PREC_MIXED ? 8 : 16;
-  const size_t f6 = std::max((size_t)6 * g.H * c->PyS, (size_t)3 * g.Py * g.Pz * c->KxS);
-  const size_t g6 = std::max((size_t)6 * g.Py * g.Pz * c->KxS, (size_t)3 * g.H * c->PyS);
-  const size_t hn = (size_t)g.H * Ny;
+  SlabState* sl = c->slab;
+  // whole grid: F6 = the six pencil fields, then the three Lamb rows; G6 =
+  // the six rows, then the three pencil fields.  Slab rank: F6 = its
+  // pencils' fields (all planes), G6 and sl->A = its planes' rows and
+  // pencils (all pencils)
+  size_t f6 = std::max((size_t)6 * g.H * c->PyS, (size_t)3 * g.Py * g.Pz * c->KxS);
+  size_t g6 = std::max((size_t)6 * g.Py * g.Pz * c->KxS, (size_t)3 * g.H * c->PyS);
+  if (sl) {
+    f6 = (size_t)6 * sl->np * c->PyS;
+    g6 = std::max((size_t)6 * sl->ny * g.Pz * c->KxS, (size_t)3 * g.H * sl->nyS);
+  }
+  const size_t hn = (size_t)(sl ? sl->np : g.H) * Ny;
   // integrated right-hand sides: N + deg(U) + 1 rows per pencil
   c->wd.delta = wall::base_degree(p->U1, p->U2);
   c->wd.nv = c->wd.no = Ny + c->wd.delta;
   c->wd.gp = c->wd.nv;
   c->wd.qbytes = (int)((7 * (size_t)c->wd.no * 8 + 15) & ~(size_t)15);
-  const size_t gn = (size_t)g.H * c->wd.gp;
+  const size_t gn = (size_t)(sl ? sl->np : g.H) * c->wd.gp;
   if ((e = c->alloc(&c->T0, NN)) || (e = c->alloc(&c->T2, NN)) || (e = c->alloc(&c->T4, NN)) ||
       (e = c->alloc(&c->Ut, Ny)) || (e = c->alloc(&c->dUt, Ny)) || (e = c->alloc(&c->ddUt, Ny)) ||
       (e = c->alloc(&c->Uy, g.Py)) || (e = c->alloc(&c->V, hn)) || (e = c->alloc(&c->O, hn)) ||
@@ -413,7 +451,9 @@ dns_status dns_create(const dns_params* p, dns_ctx** out) {
       (e = c->alloc(&c->ro, gn)) || (e = c->alloc(&c->status, 1)) ||
       (e = c->alloc((unsigned char**)&c->F6, c->F6_bytes = f6 * csz)) ||
       (e = c->alloc((unsigned char**)&c->G6, g6 * csz)) ||
-      (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny + 8 * (size_t)c->wd.nv)))
+      (e = c->alloc(&c->rtab, 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no + Ny + 8 * (size_t)c->wd.nv)) ||
+      (sl && (e = c->alloc((unsigned char**)&sl->A,
+                           std::max((size_t)6 * g.H * sl->nyS, (size_t)3 * sl->ny * g.Pz * c->KxS) * csz))))
     return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
   cudaMemcpy(c->T0, T0.data(), NN * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->T2, T2.data(), NN * 8, cudaMemcpyHostToDevice);
@@ -465,6 +505,8 @@ dns_status dns_destroy(dns_ctx* c) {
                   c->Nop, c->rv, c->ro, c->wfac, c->wQ, c->rtab, c->F6, c->G6, c->scratch, c->solve_io, c->rhs_io, c->nl_io, c->eq_io, c->probe, c->status,
                   c->y3tc_tab};
   for (void* q : ptrs) cudaFree(q);
+  if (c->slab) cudaFree(c->slab->A);
+  delete c->slab;
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return DNS_OK;
@@ -516,6 +558,7 @@ static dns_status copy_pencils(dns_ctx* c, double2* dev, const void* src, void* 
 }
 
 dns_status dns_set_state(dns_ctx* c, const void* v, const void* o, size_t pitch, int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !v || !o) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
   dns_status s = copy_pencils(c, c->V, v, nullptr, pitch, where, true);
@@ -526,6 +569,7 @@ dns_status dns_set_state(dns_ctx* c, const void* v, const void* o, size_t pitch,
 }
 
 dns_status dns_get_state(dns_ctx* c, void* v, void* o, size_t pitch, int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !v || !o) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
   dns_status s = copy_pencils(c, c->V, nullptr, v, pitch, where, false);
@@ -567,6 +611,7 @@ static dns_status history_in(dns_ctx* c, double2* dst, const void* src, size_t p
 }
 
 dns_status dns_get_history(dns_ctx* c, void* nv, void* no, size_t pitch, int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
   dns_status s = history_out(c, c->Nvp, nv, pitch, where);
@@ -575,6 +620,7 @@ dns_status dns_get_history(dns_ctx* c, void* nv, void* no, size_t pitch, int whe
 }
 
 dns_status dns_set_history(dns_ctx* c, const void* nv, const void* no, size_t pitch, int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
   dns_status s = history_in(c, c->Nvp, nv, pitch, where);
@@ -584,6 +630,7 @@ dns_status dns_set_history(dns_ctx* c, const void* nv, const void* no, size_t pi
 }
 
 dns_status dns_bootstrap(dns_ctx* c) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (!c->have_state) return fail(DNS_ERR_STATE, "dns_set_state must precede dns_bootstrap");
   CK(cudaSetDevice(c->P.device));
@@ -595,6 +642,7 @@ dns_status dns_bootstrap(dns_ctx* c) {
 
 dns_status dns_nonlinear(dns_ctx* c, const void* v, const void* o, void* nv, void* no, size_t tpitch,
                          int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !v || !o || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
   const size_t hn = (size_t)c->g.H * c->g.Ny;
@@ -615,6 +663,7 @@ dns_status dns_nonlinear(dns_ctx* c, const void* v, const void* o, void* nv, voi
 namespace {
 // checks, factors and the captured step graph of one context
 dns_status step_ready(dns_ctx* c) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (!c->have_state || !c->booted)
     return fail(DNS_ERR_STATE, "dns_set_state and dns_bootstrap must precede dns_step");
@@ -683,6 +732,7 @@ dns_status dns_get_variant(const dns_ctx* c, int pass, int* v) {
 }
 
 dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (!c->have_state) return fail(DNS_ERR_STATE, "dns_autotune needs a state");
   CK(cudaSetDevice(c->P.device));
@@ -787,6 +837,7 @@ dns_status dns_step_many(dns_ctx* const* ctxs, int n, int nsteps) {
 }
 
 dns_status dns_step_profiled(dns_ctx* c, int nsteps, double kernel_ms[DNS_NUM_KERNELS]) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !kernel_ms) return fail(DNS_ERR_ARG, "null argument");
   if (nsteps < 1) return fail(DNS_ERR_ARG, "nsteps < 1");
   if (!c->have_state || !c->booted)
@@ -1000,6 +1051,7 @@ dns_status dns_operator_matrices(dns_ctx* c, void* a_v, void* a_o, int where) {
 }
 
 dns_status dns_check_state(dns_ctx* c) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c) return fail(DNS_ERR_ARG, "null context");
   if (!c->have_state) return fail(DNS_ERR_STATE, "no state to check");
   CK(cudaSetDevice(c->P.device));
@@ -1045,6 +1097,7 @@ cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo,
 }  // namespace
 
 dns_status dns_solve_wall(dns_ctx* c, void* v, void* omega, size_t tpitch, int where) {
+  if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || (!v && !omega)) return fail(DNS_ERR_ARG, "null argument");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");
   const DnsGeom& g = c->g;

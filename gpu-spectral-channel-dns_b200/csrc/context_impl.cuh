@@ -1,6 +1,9 @@
 // Internal layout of dns_ctx, shared by the translation units that implement
 // the C ABI (context.cu, noalloc.cu).  Not part of the public interface.
 #pragma once
+#include <string>
+#include <vector>
+
 #include "../../include/dns_b200.h"
 #include "kernels.cuh"
 #include "wallsolve_dev.cuh"
@@ -18,6 +21,25 @@ template <typename C> struct DevFft {
     for (int i = 0; i < 3; ++i) t.wt[i] = wt[i];
     return t;
   }
+};
+
+// One rank of a slab-decomposed step (dns_slab_create): the runs of its
+// pencils (in local row order), its planes and the segments of the two
+// exchanges in both roles, with the bytes per peer.
+struct SlabRun {
+  int kz0, nkz;
+  long long row0;  // first local pencil row of the run
+};
+struct SlabState {
+  int R = 1, r = 0;
+  int s0 = 0, s1 = 0;          // operator slots kz' in [s0, s1)
+  int y0 = 0, ny = 0, nyS = 0;  // planes [y0, y0 + ny), their pencil pitch nyS
+  long long np = 0;            // pencils owned
+  int nruns = 0;
+  SlabRun run[2];
+  std::vector<dns_slab_segment> segP, segY;  // as pencil owner / as plane owner
+  std::vector<size_t> sendB[2], recvB[2];     // bytes per peer: [0] backward (6 fields), [1] forward (3)
+  void* A = nullptr;                          // plane-local pencils (6 fields), then rows (3 fields)
 };
 
 struct dns_ctx {
@@ -57,6 +79,7 @@ struct dns_ctx {
   cudaGraphExec_t solve_graph = nullptr;  // dns_solve_wall on device pencils
   const void* solve_key[2] = {nullptr, nullptr};
   size_t solve_pitch = 0;
+  SlabState* slab = nullptr;  // set on the contexts of dns_slab_create
 
   template <typename T> cudaError_t alloc(T** p, size_t n) {
     bytes += n * sizeof(T);
@@ -67,3 +90,10 @@ struct dns_ctx {
 
 // record an error message for dns_last_error() and return the status
 dns_status dns_internal_fail(dns_status s, const char* msg);
+
+// context.cu internals used by the slab-decomposed step (slabstep.cu)
+extern "C" dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out);
+dns_status ctx_check_status(dns_ctx* c);
+dns_status ctx_build_wall_solver(dns_ctx* c);
+// slab.cpp: the runs of pencils of a rank (their count, or -1)
+int slab_runs(int mx, int my, int mz, int nranks, int rank, int kz0[2], int nkz[2], long long row0[2]);

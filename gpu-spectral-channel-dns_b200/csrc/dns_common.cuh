@@ -58,8 +58,10 @@ struct DnsGeom {
   int Nx, Nz, Ny;   // Fourier modes (x, span) and Chebyshev modes
   int Kx;           // streamwise modes kept: Nx/2 + 1 (reference hnx)
   int Px, Pz, Py;   // physical points: mx, my, 2*Ny - 1 (reference pz)
-  long long H;      // number of pencils Kx * Nz
+  long long H;      // number of pencils Kx * Nz (of a launch: the pencils it covers)
   int Kh;           // spanwise pencils that own an operator: Nz/2 + 1
+  int kz0;          // spanwise index of a launch's first pencil (wall-normal passes
+                    // on a run of pencils kz0 .. kz0 + H/Kx - 1; 0 for the whole grid)
 };
 
 static inline DnsGeom dns_make_geom(int mx, int my, int mz) {
@@ -70,6 +72,7 @@ static inline DnsGeom dns_make_geom(int mx, int my, int mz) {
   g.Px = mx; g.Pz = my; g.Py = mz / 2 + 1;
   g.H = (long long)g.Kx * g.Nz;
   g.Kh = g.Nz / 2 + 1;
+  g.kz0 = 0;
   return g;
 }
 

@@ -85,6 +85,19 @@ std::vector<std::array<int, 3>> runs_of(const Part& P, int r) {
 
 }  // namespace
 
+// the runs of rank r (kz0, nkz, first local row) for the slab step
+int slab_runs(int mx, int my, int mz, int nranks, int rank, int kz0[2], int nkz[2], long long row0[2]) {
+  Part P;
+  if (rank < 0 || rank >= nranks || !make_part(mx, my, mz, nranks, P)) return -1;
+  const auto runs = runs_of(P, rank);
+  for (size_t i = 0; i < runs.size() && i < 2; ++i) {
+    kz0[i] = runs[i][0];
+    nkz[i] = runs[i][1];
+    row0[i] = (long long)runs[i][2];
+  }
+  return (int)runs.size();
+}
+
 extern "C" {
 
 dns_status dns_slab_ranges(int mx, int my, int mz, int nranks, int rank, int out[5]) {

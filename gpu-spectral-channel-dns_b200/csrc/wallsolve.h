@@ -127,6 +127,7 @@ void pack_slot(const Packing& pk, int q, const cx* Lv, const cx* Uv, const cx* L
 struct Grid {
   int N, Kx, Nz, Kh;
   double aphi, beta, Re, dt, U0, U1, U2;
+  int kz0 = 0, nkz = -1;  // the slots kz' in [kz0, kz0 + nkz) only (nkz < 0: all Kh)
 };
 // Factor every slot for the packed shapes v and o and write the groups of 16
 // slots (slot 0, the mean modes, holds the mean-mode system in both shapes;

@@ -12,6 +12,12 @@ struct WallDims {
   long long ngroups;       // groups of 16 slots = CTAs
   long long group_complex; // packed factor values per group
   int tilt = 1;            // 0: no tilting term (the solve-only entry)
+  // a slab's slots: operator slots kz' = kzs0 + s / Kx (local slot s); the
+  // pencil of (kx, kz) with kz = kz' sits at row rowa + (kz - kza) Kx + kx of
+  // the data arrays, with kz = Nz - kz' at rowb + (kz - kzb) Kx + kx (the
+  // whole grid: all zero, row kz Kx + kx)
+  int kzs0 = 0, kza = 0, kzb = 0;
+  long long rowa = 0, rowb = 0;
 };
 
 // band instance (v lower/upper, omega lower/upper) for base-flow degree delta

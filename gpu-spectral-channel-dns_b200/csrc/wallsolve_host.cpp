@@ -429,7 +429,8 @@ std::string pack_grid(const Grid& gr, const Shape& v, const Shape& o, std::vecto
   if (!prepare(fv, v, pv) || !prepare(fo, o, po) || !prepare(fm, v, pmv) || !prepare(fm, o, pmo))
     return "wall-normal operator outside its packed band";
   const Packing pk = make_packing(v, o);
-  const long long nslots = (long long)gr.Kx * gr.Kh;
+  const long long nslots = (long long)gr.Kx * (gr.nkz < 0 ? gr.Kh : gr.nkz);
+  const long long s0 = (long long)gr.Kx * gr.kz0;  // global slot of local slot 0
   const long long ngroups = (nslots + 15) / 16;
   out.assign((size_t)(ngroups * pk.group_complex), cx{0, 0});
   if (threads < 1) threads = 1;
@@ -440,8 +441,8 @@ std::string pack_grid(const Grid& gr, const Shape& v, const Shape& o, std::vecto
     for (long long grp = t; grp < ngroups; grp += threads) {
       cx* group = out.data() + grp * pk.group_complex;
       for (int q = 0; q < 16; ++q) {
-        const long long s = grp * 16 + q;
-        if (s >= nslots) {  // identity factors
+        const long long sl = grp * 16 + q, s = s0 + sl;
+        if (sl >= nslots) {  // identity factors
           std::fill(Lv.begin(), Lv.end(), cx{0, 0});
           std::fill(Uv.begin(), Uv.end(), cx{0, 0});
           std::fill(Lo.begin(), Lo.end(), cx{0, 0});

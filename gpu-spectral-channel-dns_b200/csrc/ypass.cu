@@ -165,7 +165,7 @@ __global__ void k_get_uvw(SixPtr a, DnsGeom g, PhysParams ph) {
   double2* Dv = cv.take<double2>(Ny);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -223,7 +223,7 @@ __global__ void k_rhs_nonlinear(double2* lx, double2* ly, const double2* lz, lon
   double2* Dy = cv.take<double2>(Ny);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   if (kx == 0 && kz == 0) return;  // source/nonlinear.cu:157
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
   C* lines = cv.take<C>((size_t)6 * ls);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   C* foz = (C*)(rb2 + 2 * VS * 16 + FS);
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -782,7 +782,7 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
 
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx);
-  const int kz = (int)(p / g.Kx);
+  const int kz = g.kz0 + (int)(p / g.Kx);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);

@@ -385,6 +385,46 @@ typedef struct {
 dns_status dns_slab_segments(int mx, int my, int mz, int nranks, int rank, int role,
                              dns_slab_segment* seg, int cap, int* count);
 
+/* ---- slab-decomposed step (one context per rank) ------------------------
+ * No counterpart in the reference.  dns_slab_create makes rank `rank`'s
+ * context of an R-rank decomposition (dns_slab_ranges): its pencil arrays
+ * hold only its pencils, in local row order (the runs of
+ * dns_slab_segments in increasing kz, Kx pencils per kz, Ny complex FP64
+ * coefficients each), and the step runs in three parts with two exchanges
+ * between them, which the caller performs (an all-to-all over NCCL, or
+ * copies between the ranks' buffers on one device):
+ *   DNS_SLAB_Y3: wall-normal backward pass on the rank's pencils; packs the
+ *                six fields for every plane owner into `send`;
+ *   exchange 0:  send -> the peers' recv, dns_slab_exchange_bytes(.., 0, ..)
+ *                bytes per peer, buffers ordered by peer;
+ *   DNS_SLAB_XZ: unpacks `recv`; spanwise inverse, streamwise (Lamb vector
+ *                and rotation term) and spanwise forward passes on the
+ *                rank's planes; packs the three fields for every pencil
+ *                owner into `send`;
+ *   exchange 1:  as exchange 0 with dns_slab_exchange_bytes(.., 1, ..);
+ *   DNS_SLAB_Y1: unpacks `recv`; wall-normal forward pass and right-hand
+ *                sides on the rank's pencils; with boot = 0 the banded
+ *                solves of its slots (the new state).  boot = 1 runs the
+ *                three parts as the bootstrap (the AB2 history only).
+ * Per peer and field the packed buffers hold the segments in plan order,
+ * each block [pencil][plane], in the transform precision (8 bytes per
+ * complex value in the mixed form, 16 in FP64).  The parts are enqueued on
+ * the context's stream (dns_get_stream) and return at once; `send` and
+ * `recv` are device buffers the caller keeps until the work is done.
+ * dns_synchronize reports device-side failures.  The whole-grid entry points
+ * (dns_set_state, dns_step, ...) refuse a slab context. */
+enum { DNS_SLAB_Y3 = 0, DNS_SLAB_XZ = 1, DNS_SLAB_Y1 = 2 };
+enum { DNS_SLAB_V = 0, DNS_SLAB_OMEGA = 1, DNS_SLAB_NV = 2, DNS_SLAB_NOMEGA = 3 };
+dns_status dns_slab_create(const dns_params* p, int nranks, int rank, dns_ctx** ctx);
+/* send[peer], recv[peer]: bytes of exchange 0 or 1 (nranks entries each) */
+dns_status dns_slab_exchange_bytes(const dns_ctx* ctx, int exchange, size_t* send, size_t* recv);
+/* the rank's v, omega_y (DNS_SLAB_V, DNS_SLAB_OMEGA) or AB2 history
+ * (DNS_SLAB_NV, DNS_SLAB_NOMEGA: Chebyshev coefficients of the nonlinear
+ * terms) in local row order, np x Ny complex FP64, unpitched: into the
+ * context (to_ctx = 1) or out of it.  Synchronous. */
+dns_status dns_slab_local(dns_ctx* ctx, int which, void* buf, int where, int to_ctx);
+dns_status dns_slab_part(dns_ctx* ctx, int part, int boot, void* send, const void* recv);
+
 #ifdef __cplusplus
 }
 #endif
