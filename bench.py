@@ -14,8 +14,10 @@ memory and back out every step.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 With --gpus N > 1 (launched by torchrun) every rank runs an independent
-replica of the problem (the step does not shard at this size); the time is
-the maximum over ranks and `value` sums the replicas' steps/s.
+replica of the problem; the time is the maximum over ranks and `value` sums
+the replicas' steps/s.  --decomposed runs one problem split over the ranks
+instead (the slab decomposition, NCCL all-to-all exchanges, strong scaling),
+or over --slab-ranks R ranks on one device.
 """
 from __future__ import annotations
 
@@ -590,6 +592,86 @@ def roofline(kms, geo, c, peak, config="256x129x256", prec="mixed"):
                  "bytes_per_launch": kb[top], "ms_per_launch": round(kms[top], 4)}
 
 
+def run_decomposed(args, rank, world):
+    """The slab-decomposed mixed step (dns_slab_part) of the headline
+    workload: with N ranks one per GPU and the two exchanges as NCCL
+    all-to-all collectives (strong scaling: one problem over N GPUs); in one
+    process with --slab-ranks R > 1, R ranks on one device with the
+    exchanges as device copies (the decomposition's own cost, no scaling).
+    CUDA events around the timed steps, maximum over ranks."""
+    import importlib
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    slab = importlib.import_module(pkg.__name__ + ".slab")
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    params = pkg.make_params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"], dt=CFG["dt"],
+                             precision=pkg.PREC_MIXED, device=dev)
+    V0, O0 = pkg.seeded_state(CFG["Nx"], CFG["Ny"], CFG["Nz"], 4.0, 2.0, CFG["amplitude"], CFG["seed"])
+    R = world if world > 1 else max(1, args.slab_ranks)
+    ctxs = [pkg.SlabContext(params, R, r) for r in ([rank] if world > 1 else range(R))]
+    for c in ctxs:
+        c.scatter_state(V0, O0)
+        try:  # the tensor-core wall-normal pass where the grid has it
+            c.set_variant(pkg.PASS_Y3, pkg.Y3_TENSOR)
+        except pkg.DnsError:
+            pass
+    K, W = args.steps, args.warmup
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        bufs = slab.step_dist(ctxs[0], boot=True)
+        slab.step_dist(ctxs[0], W, bufs=bufs)
+        ctxs[0].synchronize()
+        torch.distributed.barrier()
+        torch.cuda.synchronize()
+        s = torch.cuda.ExternalStream(ctxs[0].stream)
+        with ClockSampler(dev) as clk:
+            e0.record(s)
+            slab.step_dist(ctxs[0], K, bufs=bufs)
+            e1.record(s)
+            ctxs[0].synchronize()
+            torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1)) / K
+        xbytes = sum(sum(bufs.split[x][0]) for x in (0, 1))
+        xbytes = int(dist_max(xbytes))  # the busiest rank's bytes sent per step
+    else:
+        bufs = slab.step_local(ctxs, boot=True)
+        slab.step_local(ctxs, W, bufs=bufs)
+        torch.cuda.synchronize()
+        with ClockSampler(dev) as clk:
+            e0.record()
+            slab.step_local(ctxs, K, bufs=bufs)
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        xbytes = max(sum(sum(b.split[x][0]) for x in (0, 1)) for b in bufs)
+    finite = all(np.isfinite(c.get_local(pkg.SLAB_V)).all() for c in ctxs)
+    # kernels per step and rank: y3 and y1 per run, one copy per segment and
+    # exchange direction at both ends, zb, x, zf and the solve
+    launches = 0
+    for c in ctxs:
+        nseg = sum(len(pkg.slab_segments(CFG["mx"], CFG["my"], CFG["mz"], R, c.rank, role))
+                   for role in (pkg.SLAB_PENCILS, pkg.SLAB_PLANES))
+        launches += 2 * len(c.runs) + 2 * nseg + 4
+    if world > 1:
+        launches = int(dist_max(launches))
+    for c in ctxs:
+        c.close()
+    return {"metric": METRIC, "value": round(1000.0 / ms, 2), "unit": "steps/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 transforms/Lamb + f64 solves/state (mixed)",
+            "data": "synthetic seeded divergence-free field (seed 0, amplitude 0.1)",
+            "config": {"workload": f"rotating plane Couette {args.config} modes, slab-decomposed step",
+                       "parallelism": (f"slab x{world} (NCCL all-to-all)" if world > 1 else
+                                       f"slab x{R} ranks on one device (exchanges as device copies)"),
+                       "l2": "inputs larger than L2 (no flush)"},
+            "exchange_bytes_per_step_max_rank": xbytes, "state_finite": bool(finite),
+            "clocks": clk.summary(), "gpu_launches": launches * K}
+
+
 def launch_ranks(n):
     """Run this command as n local ranks under torch.distributed.run (one
     process per GPU, rendezvous on 127.0.0.1) and return its exit status."""
@@ -640,6 +722,11 @@ def main():
                     help="the 48-run ensemble (concurrent runs, one GPU): prints its own line")
     ap.add_argument("--check-launch", action="store_true",
                     help="start the ranks and print their count only (no device work)")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="the slab-decomposed step: one problem over the N ranks (NCCL all-to-all "
+                         "exchanges), or over --slab-ranks ranks on one device")
+    ap.add_argument("--slab-ranks", type=int, default=2,
+                    help="with --decomposed on one process: ranks emulated on the device")
     args = ap.parse_args()
     global CFG
     CFG = CONFIGS[args.config]
@@ -677,6 +764,15 @@ def main():
     if args.ensemble:
         if rank == 0:
             print(json.dumps(run_ensemble(args)))
+        return
+    if args.decomposed:
+        r = run_decomposed(args, rank, world)
+        if rank == 0:
+            print(json.dumps(r))
+        if world > 1:
+            import torch
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
         return
     r = run_ours(args, rank, world)
     peak, peak_kind = measured_peaks()

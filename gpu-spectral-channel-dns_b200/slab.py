@@ -6,14 +6,14 @@ GPU).  The packed buffers are byte tensors on the device; their layout is
 the library's (per peer, per field, the segments in plan order)."""
 import torch
 
-from .abi import SLAB_XZ, SLAB_Y1, SLAB_Y3, SlabContext
+from .abi import SLAB_XZ, SLAB_Y1, SLAB_Y3
 
 
 class SlabBuffers:
     """Send and receive buffers of one rank and the bytes per peer of both
     exchanges."""
 
-    def __init__(self, ctx: SlabContext, device=None):
+    def __init__(self, ctx, device=None):
         self.split = {x: ctx.exchange_bytes(x) for x in (0, 1)}
         ns = max(sum(self.split[0][0]), sum(self.split[1][0]), 16)
         nr = max(sum(self.split[0][1]), sum(self.split[1][1]), 16)
@@ -62,15 +62,17 @@ def step_local(ctxs, nsteps=1, boot=False, bufs=None):
     return bufs
 
 
-def step_dist(ctx: SlabContext, nsteps=1, boot=False, bufs=None, group=None):
+def step_dist(ctx, nsteps=1, boot=False, bufs=None, group=None):
     """This process's rank of a decomposition across processes: the parts on
     the context's stream, the exchanges as all-to-all collectives of
     torch.distributed (NCCL) ordered on the same stream.  Asynchronous on
     that stream; returns the buffers for reuse."""
+    import contextlib
+
     import torch.distributed as dist
     bufs = bufs or SlabBuffers(ctx)
-    stream = torch.cuda.ExternalStream(ctx.stream)
-    with torch.cuda.stream(stream):
+    on_gpu = bufs.send.is_cuda
+    with (torch.cuda.stream(torch.cuda.ExternalStream(ctx.stream)) if on_gpu else contextlib.nullcontext()):
         for _ in range(1 if boot else nsteps):
             for part, x in ((SLAB_Y3, 0), (SLAB_XZ, 1), (SLAB_Y1, None)):
                 ctx.part(part, bufs.send.data_ptr(), bufs.recv.data_ptr(), boot)

@@ -204,6 +204,51 @@ def decomposed_nonlinear(pkg, pb, R, r, dist, torch):
     return rows, res[0], res[1]
 
 
+class _FakeRank:
+    """Stand-in for a SlabContext in the driver test: exchange sizes from the
+    plan (as dns_slab_exchange_bytes computes them: 6 fields back, 3 fields
+    forward, 8 bytes per value), parts that write peer-tagged bytes into the
+    send buffer and check what the all-to-all delivered."""
+
+    def __init__(self, pkg, grid, R, r, torch):
+        Kx = _geom(*grid)[0]
+        self.torch, self.R, self.r, self.checked, self.bufs = torch, R, r, 0, None
+        self.sizes = {x: ([0] * R, [0] * R) for x in (0, 1)}
+        for sg in pkg.slab_segments(*grid, R, r, pkg.SLAB_PENCILS):
+            b = sg["nkz"] * Kx * sg["ny"] * 8
+            self.sizes[0][0][sg["peer"]] += 6 * b
+            self.sizes[1][1][sg["peer"]] += 3 * b
+        for sg in pkg.slab_segments(*grid, R, r, pkg.SLAB_PLANES):
+            b = sg["nkz"] * Kx * sg["ny"] * 8
+            self.sizes[0][1][sg["peer"]] += 6 * b
+            self.sizes[1][0][sg["peer"]] += 3 * b
+
+    def exchange_bytes(self, x):
+        return self.sizes[x]
+
+    def _fill(self, x):
+        off = 0
+        for s, n in enumerate(self.sizes[x][0]):
+            self.bufs.send[off:off + n] = (self.r * 16 + s + 64 * x) & 0xFF
+            off += n
+
+    def _check(self, x):
+        off = 0
+        for p, n in enumerate(self.sizes[x][1]):
+            assert bool(self.torch.all(self.bufs.recv[off:off + n] == ((p * 16 + self.r + 64 * x) & 0xFF)))
+            off += n
+        self.checked += 1
+
+    def part(self, part, send_ptr, recv_ptr, boot=False):
+        if part == 0:
+            self._fill(0)
+        elif part == 1:
+            self._check(0)
+            self._fill(1)
+        else:
+            self._check(1)
+
+
 def _worker(rank, world, port, grid, q, mode="exchange"):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import torch
@@ -211,7 +256,15 @@ def _worker(rank, world, port, grid, q, mode="exchange"):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         pkg = load_package()
-        if mode == "exchange":
+        if mode == "driver":
+            import importlib
+            slab = importlib.import_module(pkg.__name__ + ".slab")
+            fake = _FakeRank(pkg, grid, world, rank, torch)
+            fake.bufs = slab.SlabBuffers(fake, device="cpu")
+            slab.step_dist(fake, boot=True, bufs=fake.bufs)
+            slab.step_dist(fake, 2, bufs=fake.bufs)
+            assert fake.checked == 6, fake.checked
+        elif mode == "exchange":
             Kx, Nz, Py = _geom(*grid)
             G = np.random.default_rng(5).standard_normal((6, Kx * Nz, Py))
             _exchange(pkg, grid, world, rank, G, dist, torch)
@@ -265,3 +318,12 @@ def test_decomposed_nonlinear_matches_oracle_gloo(world):
     rank's pencils, plane passes on its planes, the two exchanges between)
     equals the undecomposed oracle on every rank's pencils."""
     _spawn(world, (48, 48, 128), "nonlinear")
+
+
+@pytest.mark.parametrize("world,grid", [(2, (48, 48, 128)), (3, (24, 36, 64))])
+def test_step_dist_driver_gloo(world, grid):
+    """slab.step_dist, the NCCL driver of the decomposed step, on gloo ranks:
+    the all-to-all byte splits of both exchanges agree at both ends and every
+    peer's bytes arrive where the receiving part reads them, for a bootstrap
+    and two steps."""
+    _spawn(world, grid, "driver")
