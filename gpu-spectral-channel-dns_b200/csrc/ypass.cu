@@ -71,6 +71,105 @@ __device__ __noinline__ void ddz_warp(const double2* a, double2* b, int N) {
   }
 }
 
+// The same derivative with CH (even) coefficients per lane: every lane's
+// run starts at an even index, so the parity of each of its elements is
+// known at compile time (the sums split by parity without divergent
+// branches), and the run stays in registers between the two sweeps.
+template <int CH>
+__device__ __noinline__ void ddz_fast(const double2* __restrict__ a, double2* __restrict__ b, int N) {
+  static_assert(CH % 2 == 0, "runs of even length");
+  const int lane = threadIdx.x & 31;
+  const int j0 = lane * CH;
+  double2 v[CH];
+#pragma unroll
+  for (int i = 0; i < CH; ++i) v[i] = (j0 + i < N) ? a[j0 + i] : make_double2(0.0, 0.0);
+  double2 te = make_double2(0.0, 0.0), to = te;  // this run's sums of 2 j a_j, even / odd j
+#pragma unroll
+  for (int i = 0; i < CH; ++i) {
+    const double f = 2.0 * (j0 + i);
+    if (i & 1) to = to + v[i] * f;
+    else te = te + v[i] * f;
+  }
+  double s0 = te.x, s1 = te.y, s2 = to.x, s3 = to.y;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double t0 = __shfl_down_sync(0xffffffffu, s0, d);
+    const double t1 = __shfl_down_sync(0xffffffffu, s1, d);
+    const double t2 = __shfl_down_sync(0xffffffffu, s2, d);
+    const double t3 = __shfl_down_sync(0xffffffffu, s3, d);
+    if (lane + d < 32) { s0 += t0; s1 += t1; s2 += t2; s3 += t3; }
+  }
+  // sums over the runs of the lanes above, then down this run
+  double2 re = make_double2(s0 - te.x, s1 - te.y), ro = make_double2(s2 - to.x, s3 - to.y);
+#pragma unroll
+  for (int i = CH - 1; i >= 0; --i) {
+    const int j = j0 + i;
+    double2 out = (i & 1) ? re : ro;  // j' > j of the other parity
+    if (j == 0) out = out * 0.5;
+    if (j < N) b[j] = out;
+    const double f = 2.0 * j;
+    if (i & 1) ro = ro + v[i] * f;
+    else re = re + v[i] * f;
+  }
+}
+
+// Second derivative of a Chebyshev series by one warp in one sweep, CH
+// (even) coefficients per lane: b_i = (1 / c_i) sum_{j >= i+2, j - i even}
+// j (j^2 - i^2) a_j (c_0 = 2, else 1), the composition of two ddz_warp
+// steps, as parity-split suffix sums of j a_j and j^3 a_j.  The lane's run
+// is read twice from shared memory rather than held in registers.
+template <int CH>
+__device__ __noinline__ void d2z_fast(const double2* __restrict__ a, double2* __restrict__ b, int N) {
+  static_assert(CH % 2 == 0, "runs of even length");
+  const int lane = threadIdx.x & 31;
+  const int j0 = lane * CH;
+  double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // (j a_j, j^3 a_j) x (even, odd j), re / im
+#pragma unroll
+  for (int i = 0; i < CH; ++i) {
+    if (j0 + i < N) {
+      const double2 v = a[j0 + i];
+      const double j = (double)(j0 + i), j3 = j * j * j;
+      const int o = (i & 1) * 4;
+      t[o + 0] += j * v.x;
+      t[o + 1] += j * v.y;
+      t[o + 2] += j3 * v.x;
+      t[o + 3] += j3 * v.y;
+    }
+  }
+  // inclusive suffix sums over the lanes, then those of the lanes above
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double x = __shfl_down_sync(0xffffffffu, t[k], d);
+      if (lane + d < 32) t[k] += x;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double x = __shfl_down_sync(0xffffffffu, t[k], 1);
+    t[k] = lane < 31 ? x : 0.0;
+  }
+#pragma unroll
+  for (int i = CH - 1; i >= 0; --i) {
+    const int jj = j0 + i;
+    if (jj < N) {
+      const double j = (double)jj, j2 = j * j;
+      const int o = (i & 1) * 4;  // j' >= j + 2 of the same parity
+      double2 out = make_double2(t[o + 2] - j2 * t[o + 0], t[o + 3] - j2 * t[o + 1]);
+      if (jj == 0) out = out * 0.5;
+      const double2 v = a[jj];
+      b[jj] = out;
+      t[o + 0] += j * v.x;
+      t[o + 1] += j * v.y;
+      t[o + 2] += j * j2 * v.x;
+      t[o + 3] += j * j2 * v.y;
+    }
+  }
+}
+// lanes' run length for Ny coefficients
+__host__ __device__ constexpr int ddz_run(int Ny) { return 2 * ((Ny + 63) / 64); }
+
 // even extension for the padded s2p (cheby_pre_s2p_pad): e[0] = c0,
 // e[k] = e[M-k] = c_k/2 for 1 <= k <= Ny-1, zero otherwise; M = 4(Ny-1).
 template <typename C>
@@ -416,12 +515,13 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   // derivatives from D^2 w, D oz (source/velocity.cu:90-170).  The mean
   // mode holds u0, w0 in (w, oz): u = w, v = oz, omega_x = D oz, omega_y = -D w.
   const int warp = threadIdx.x >> 5;
+  constexpr int CH = ddz_run(Ny);
   if (warp == 0) {
-    ddz_warp(w, Dw, Ny);
+    ddz_fast<CH>(w, Dw, Ny);
     __syncwarp();
-    if (!zero) ddz_warp(Dw, D2w, Ny);
+    if (!zero) ddz_fast<CH>(Dw, D2w, Ny);
   } else if (warp == 1) {
-    ddz_warp(oz, Doz, Ny);
+    ddz_fast<CH>(oz, Doz, Ny);
   }
   __syncthreads();
   for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
@@ -741,8 +841,9 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
 }
 
 // Same pass with warp FFTs: warps 0-2 transform one Lamb line each (0 and 1
-// also differentiate theirs), while warps 3 and 4 build the derivative
-// chains of v and omega_y; no block barrier inside the transforms.
+// also differentiate theirs), while warp 3 forms D^2 v and D^4 v (two
+// second-derivative sweeps) and warp 4 D^2 omega_y; no block barrier inside
+// the transforms.
 template <typename C, int M>
 __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr lam, const double2* __restrict__ V,
                                             const double2* __restrict__ O, double2* Nvp,
@@ -759,11 +860,8 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   double2* Oc = cv.take<double2>(Ny);
   double2* nvc = cv.take<double2>(Ny);
   double2* noc = cv.take<double2>(Ny);
-  double2* DV = cv.take<double2>(Ny);
   double2* D2V = cv.take<double2>(Ny);
-  double2* D3V = DV;  // DV is dead once D2V is formed
   double2* D4V = cv.take<double2>(Ny);
-  double2* DO = cv.take<double2>(Ny);
   double2* D2O = cv.take<double2>(Ny);
   double2* red = cv.take<double2>(8);
   const size_t bytesL = (size_t)3 * wlen<C>(M) * sizeof(C), bytesI = (size_t)4 * LB * 16;
@@ -832,19 +930,14 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
       }
     };
     wfft_io<C, M, 1, false>(wline, wtw_of(tabP, 0), ld, st);
-    if (warp < 2) ddz_warp(lf, lf + VS, Ny);
+    if (warp < 2) ddz_fast<ddz_run(Ny)>(lf, lf + VS, Ny);
   } else if (!boot && warp == 3) {
-    ddz_warp(Vc, DV, Ny);
+    // D^2 v in one sweep, D^4 v = D^2 (D^2 v)
+    d2z_fast<ddz_run(Ny)>(Vc, D2V, Ny);
     __syncwarp();
-    ddz_warp(DV, D2V, Ny);
-    __syncwarp();
-    ddz_warp(D2V, D3V, Ny);
-    __syncwarp();
-    ddz_warp(D3V, D4V, Ny);
+    d2z_fast<ddz_run(Ny)>(D2V, D4V, Ny);
   } else if (!boot && warp == 4) {
-    ddz_warp(Oc, DO, Ny);
-    __syncwarp();
-    ddz_warp(DO, D2O, Ny);
+    d2z_fast<ddz_run(Ny)>(Oc, D2O, Ny);
   }
   __syncthreads();
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
@@ -1054,7 +1147,7 @@ cudaError_t launch_y1(PencilArr lam, const double2* V, const double2* O, double2
       if (probe) return cudaSuccess;
       auto a = [](size_t b) { return (b + 15) & ~(size_t)15; };
       const size_t bl = (size_t)3 * wlen<C>(L) * sizeof(C), bi = (size_t)4 * (g.Ny + 8) * 16;
-      const size_t sm = 9 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
+      const size_t sm = 7 * a((size_t)g.Ny * 16) + a(8 * 16) + a(bl > bi ? bl : bi);
       cudaFuncSetAttribute(k_y1w<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_y1w<C, L><<<(unsigned)g.H, 160, sm, st>>>(lam, V, O, Nvp, Nop, gv, go, rd, tb, g, ph, tabP, boot,
                                                     status);
