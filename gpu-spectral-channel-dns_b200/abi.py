@@ -36,14 +36,15 @@ EXPORTS = [
     "dns_autotune", "dns_solve_residual",
 ]
 
-PASS_Y3, PASS_Y1, PASS_ZB, PASS_ZF, PASS_Y2, NUM_PASSES, MAX_VARIANTS = 0, 1, 2, 3, 4, 5, 4
+PASS_Y3, PASS_Y1, PASS_ZB, PASS_ZF, PASS_Y2, PASS_X, NUM_PASSES, MAX_VARIANTS = 0, 1, 2, 3, 4, 5, 6, 4
 Y3_FFT, Y3_TENSOR, Y3_BLOCK = 0, 1, 2
 Y1_WARP, Y1_BLOCK = 0, 1
 Z_TENSOR_COPY, Z_WARP, Z_BLOCK = 0, 1, 2
 Y2_RING3_12K, Y2_RING3_12K_EF, Y2_RING2_8K_EF, Y2_RING3_8K_EF = 0, 1, 2, 3
+X_WARP3, X_WARP6, X_BLOCK = 0, 1, 2
 # names of the tunable passes and their variants (bench and test reports)
 PASS_NAMES = {PASS_Y3: "y3_uvw_s2p", PASS_Y1: "y1_p2s_rhs", PASS_ZB: "zb_span_inverse", PASS_ZF: "zf_span_forward",
-              PASS_Y2: "y2_solve"}
+              PASS_Y2: "y2_solve", PASS_X: "x_c2r_lamb_r2c"}
 VARIANT_NAMES = {
     PASS_Y3: {Y3_FFT: "warp_fft", Y3_TENSOR: "tensor_core_3xtf32", Y3_BLOCK: "block_fft"},
     PASS_Y1: {Y1_WARP: "warp_fft", Y1_BLOCK: "block_fft"},
@@ -51,6 +52,7 @@ VARIANT_NAMES = {
     PASS_ZF: {Z_TENSOR_COPY: "warp_fft_tensor_copy", Z_WARP: "warp_fft", Z_BLOCK: "block_fft"},
     PASS_Y2: {Y2_RING3_12K: "ring_3x12k", Y2_RING3_12K_EF: "ring_3x12k_evict_first",
               Y2_RING2_8K_EF: "ring_2x8k_evict_first", Y2_RING3_8K_EF: "ring_3x8k_evict_first"},
+    PASS_X: {X_WARP3: "warp_fft_3_warps", X_WARP6: "warp_fft_6_warps", X_BLOCK: "block_fft"},
 }
 
 SLAB_PENCILS, SLAB_PLANES = 0, 1

@@ -203,7 +203,10 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   if ((e = var(DNS_PASS_ZB, [&](int v) { return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v); })))
     return e;
   mark();
-  if ((e = launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st))) return e;
+  if ((e = var(DNS_PASS_X, [&](int v) {
+         return launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v);
+       })))
+    return e;
   mark();
   if ((e = var(DNS_PASS_ZF, [&](int v) { return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v); })))
     return e;
@@ -263,6 +266,11 @@ bool probe_pass(const dns_ctx* c, int pass, int v, const DevFft<C>& fz, const De
       return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
     case DNS_PASS_Y2:
       return v < DNS_WALL_VARIANTS && wall_smem_bytes(c->wd, v) <= 227 * 1024;
+    case DNS_PASS_X: {
+      const DevFft<C>& fx = *(const DevFft<C>*)(std::is_same<C, float2>::value ? (const void*)&c->fx_f
+                                                                               : (const void*)&c->fx_d);
+      return launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v, true) == cudaSuccess;
+    }
   }
   return false;
 }
@@ -277,11 +285,11 @@ void default_variants(dns_ctx* c) {
   static const int order_mixed[DNS_NUM_PASSES][3] = {
       {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
       {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK}, {DNS_Z_TENSOR_COPY, DNS_Z_WARP, DNS_Z_BLOCK},
-      {DNS_Y2_RING3_12K, DNS_Y2_RING2_8K_EF, -1}};
+      {DNS_Y2_RING3_12K_EF, DNS_Y2_RING2_8K_EF, -1}, {DNS_X_WARP3, DNS_X_BLOCK, -1}};
   static const int order_fp64[DNS_NUM_PASSES][3] = {
       {DNS_Y3_FFT, DNS_Y3_BLOCK, -1}, {DNS_Y1_WARP, DNS_Y1_BLOCK, -1},
       {DNS_Z_WARP, DNS_Z_BLOCK, -1}, {DNS_Z_WARP, DNS_Z_BLOCK, -1},
-      {DNS_Y2_RING3_12K, DNS_Y2_RING2_8K_EF, -1}};
+      {DNS_Y2_RING3_12K_EF, DNS_Y2_RING2_8K_EF, -1}, {DNS_X_WARP3, DNS_X_BLOCK, -1}};
   for (int p = 0; p < DNS_NUM_PASSES; ++p) {
     const int* ord = mixed ? order_mixed[p] : order_fp64[p];
     c->variant[p] = ord[0];
@@ -765,7 +773,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   int keep[DNS_NUM_PASSES];
   for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = c->variant[p];
   // kernel slot of each pass in a step's events
-  static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3, 5};
+  static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3, 5, 2};
   const int ne = DNS_NUM_KERNELS + 1, nt = 3;
   std::vector<cudaEvent_t> ev((size_t)ne * (nt + 1));
   for (auto& x : ev)

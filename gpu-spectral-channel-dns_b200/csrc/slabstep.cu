@@ -146,7 +146,10 @@ cudaError_t part_xz(dns_ctx* c, const void* recv, void* send) {
   PencilArr Q3{c->G6, S.nyS, g.H * S.nyS};
   e = launch_zb<C>(Q6, R6, 6, gs, fz.tab(), c->st, c->status, c->variant[DNS_PASS_ZB]);
   if (e == cudaErrorNotSupported) e = launch_zb<C>(Q6, R6, 6, gs, fz.tab(), c->st, c->status);
-  if (!e) e = launch_x_fused<C>(R6, R3, gs, fx.tab(), c->Uy + S.y0, c->ph.Ro, c->status, c->st);
+  if (!e) {
+    e = launch_x_fused<C>(R6, R3, gs, fx.tab(), c->Uy + S.y0, c->ph.Ro, c->status, c->st, c->variant[DNS_PASS_X]);
+    if (e == cudaErrorNotSupported) e = launch_x_fused<C>(R6, R3, gs, fx.tab(), c->Uy + S.y0, c->ph.Ro, c->status, c->st);
+  }
   if (!e) {
     e = launch_zf<C>(R3, Q3, 3, gs, fz.tab(), c->st, c->status, c->variant[DNS_PASS_ZF]);
     if (e == cudaErrorNotSupported) e = launch_zf<C>(R3, Q3, 3, gs, fz.tab(), c->st, c->status);

@@ -550,17 +550,23 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
   }
 }
 
-// Same pass with warp FFTs: a CTA of three warps owns four rows of one
-// wall-normal plane.  Warp w inverse-transforms lines 4w..4w+3 (line 3r+q
-// holds row r's packed pair q), reading the half spectra straight from the
-// row arrays in the first FFT pass; after a block barrier the Lamb vector of
-// the four rows is formed pointwise into lines 0-5 (lines r < 4: lambda_x +
-// i lambda_y of row r; lines 4, 5: lambda_z of rows (0, 1), (2, 3)); each
-// warp forward-transforms two of them, and the half spectra are unpacked to
-// the output rows.
-template <typename C, int L>
-__global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
-                                          const double* __restrict__ Uy, double Ro, int* status) {
+// Same pass with warp FFTs: a CTA of NW warps (3 or 6) owns four rows of
+// one wall-normal plane.  Warp w inverse-transforms lines LPW w .. LPW w +
+// LPW - 1, LPW = 12 / NW (line 3r+q holds row r's packed pair q), reading
+// the half spectra straight from the row arrays in the first FFT pass;
+// after a block barrier the Lamb vector of the four rows is formed
+// pointwise into lines 0-5 (lines r < 4: lambda_x + i lambda_y of row r;
+// lines 4, 5: lambda_z of rows (0, 1), (2, 3)); each warp forward-transforms
+// 6 / NW of them, and the half spectra are unpacked to the output rows.
+// Six warps hold half the lines each: half the registers per thread, twice
+// the warps per SM.
+template <typename C, int L, int NW>
+__global__ void __launch_bounds__(32 * NW, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, RowArr out, DnsGeom g,
+                                                                      FftTab<C> tab, const double* __restrict__ Uy,
+                                                                      double Ro, int* status) {
+  static_assert(NW == 3 || NW == 6, "three or six warps");
+  constexpr int LPW = 12 / NW;  // inverse lines per warp
+  constexpr int FPW = 6 / NW;   // forward lines per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   typedef T_of<C> T;
   constexpr int Px = L;
@@ -571,20 +577,20 @@ __global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, Ro
   const long long r0 = (long long)blockIdx.x * 4;
   const long long nrows = (long long)g.Py * g.Pz;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* zw = z + (size_t)4 * warp * LW;
-  // stage this warp's 8 half-spectrum rows (bins 0..hx-1, 16 B aligned) at
-  // the start of its own lines: the first FFT pass reads them all before it
-  // writes its output over them
+  C* zw = z + (size_t)LPW * warp * LW;
+  // stage this warp's 2 LPW half-spectrum rows (bins 0..hx-1, 16 B aligned)
+  // at the start of its own lines: the first FFT pass reads them all before
+  // it writes its output over them
   constexpr int SR = 128;  // staged bins per row (>= hx)
   uint64_t* bar = bars + warp;
   if (lane == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
-    mbar_expect_tx(bar, 8 * SR * sizeof(C));
+    mbar_expect_tx(bar, 2 * LPW * SR * sizeof(C));
   }
   __syncwarp();
-  if (lane < 8) {
-    const int line = 4 * warp + (lane >> 1);
+  if (lane < 2 * LPW) {
+    const int line = LPW * warp + (lane >> 1);
     const int rl = line / 3, q = line - 3 * (line / 3);
     long long row = r0 + rl;
     if (row >= nrows) row = nrows - 1;  // duplicate work, not stored
@@ -606,7 +612,7 @@ __global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, Ro
     const C* stg = zw;
     auto ld = [&](int l, int n) -> C { return pack_c2r<C>(stg + (size_t)(2 * l) * SR, stg + (size_t)(2 * l + 1) * SR, n, Px, hx); };
     auto st = [&](int l, int k, C v) { zw[(size_t)l * LW + wsw<C>(k)] = v; };
-    wfft_io<C, L, 4, true>(zw, wtw_of(tab, 2), ld, st);
+    wfft_io<C, L, LPW, true>(zw, wtw_of(tab, LPW == 4 ? 2 : 1), ld, st);
   }
   __syncthreads();
   const T ro = (T)Ro;
@@ -635,14 +641,14 @@ __global__ void __launch_bounds__(96, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, Ro
     z[(size_t)5 * LW + op] = B1;
   }
   __syncthreads();
-  wfft<C, L, 2, false>(z + (size_t)2 * warp * LW, wtw_of(tab, 1));
+  wfft<C, L, FPW, false>(z + (size_t)FPW * warp * LW, wtw_of(tab, FPW - 1));
   __syncthreads();
   // unpack: output row o = 3 rl + fl (field fl of row rl) by warp o mod 3,
   // lanes over the bins k; shared loads of a batch before its stores
   const int Kx = g.Kx;
   const T sc = (T)(0.5 / ((double)g.Px * (double)g.Pz));
   constexpr int XB = 5;
-  for (int o = warp; o < 12; o += 3) {
+  for (int o = warp; o < 12; o += NW) {
     const int rl = o / 3, fl = o - 3 * rl;
     const long long row = r0 + rl;
     if (row >= nrows) continue;
@@ -912,23 +918,35 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
 }
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
-                           double Ro, int* status, cudaStream_t st) {
-  return with_len_xz(g.Px, [&](auto LL) {
+                           double Ro, int* status, cudaStream_t st, int variant, bool probe) {
+  const bool any = variant == VAR_AUTO;
+  return with_len_xz(g.Px, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+    if constexpr (L > 0 && WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok &&
+                  WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
       const long long nrows = (long long)g.Py * g.Pz;
-      // four rows per CTA within one wall-normal plane; a warp's 8 staged
-      // rows of 128 bins fit in its 4 lines
+      // four rows per CTA within one wall-normal plane; a warp's staged
+      // rows of 128 bins fit in its lines
       // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
-      const bool tw_ok = wtw_of(tab, 1) && wtw_of(tab, 2);
-      if (tw_ok && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) &&
-          in.rs >= 128 && (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0) {
-        const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
-        cudaFuncSetAttribute(k_xw<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
+      const bool tw_ok = wtw_of(tab, 0) && wtw_of(tab, 1) && wtw_of(tab, 2);
+      const bool ok = tw_ok && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) &&
+                      in.rs >= 128 && (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0;
+      const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
+      if (ok && (any || variant == DNS_X_WARP3)) {
+        if (probe) return cudaSuccess;
+        cudaFuncSetAttribute(k_xw<C, L, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xw<C, L, 3><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
+        return cudaGetLastError();
+      }
+      if (ok && variant == DNS_X_WARP6) {
+        if (probe) return cudaSuccess;
+        cudaFuncSetAttribute(k_xw<C, L, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_xw<C, L, 6><<<(unsigned)((nrows + 3) / 4), 192, sm, st>>>(in, out, g, tab, Uy, Ro, status);
         return cudaGetLastError();
       }
     }
+    if (!any && variant != DNS_X_BLOCK) return cudaErrorNotSupported;
+    if (probe) return cudaSuccess;
     const size_t sm = (size_t)(L > 0 ? 6 : 9) * FLine<C, L>::stride(g.Px) * sizeof(C);
     cudaFuncSetAttribute(k_x_fused<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     const long long nrows = (long long)g.Py * g.Pz;  // Pz is even: row pairs share a plane
@@ -969,7 +987,7 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
   template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
   template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
-                                         double, int*, cudaStream_t);                             \
+                                         double, int*, cudaStream_t, int, bool);                  \
   template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \
                                        FftTab<C>, cudaStream_t);                                  \
   template cudaError_t launch_x_r2c<C>(const T_of<C>*, long long, RowArr, long long, DnsGeom,     \

@@ -10,7 +10,8 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
                       int* status = nullptr, int variant = VAR_AUTO, bool probe = false);
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
-                           double Ro, int* status, cudaStream_t st);
+                           double Ro, int* status, cudaStream_t st, int variant = VAR_AUTO,
+                           bool probe = false);
 template <typename C>
 cudaError_t launch_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
                          FftTab<C> tab, cudaStream_t st);

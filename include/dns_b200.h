@@ -194,6 +194,10 @@ dns_status dns_set_wait_limit(dns_ctx* ctx, long long cycles);
  *                        form, Nz <= 256);
  *     DNS_Z_WARP         warp FFTs on tiles gathered through L1;
  *     DNS_Z_BLOCK        block-wide FFT (every grid).
+ *   DNS_PASS_X: the streamwise pass (C2R, Lamb vector, R2C) on four rows
+ *     per CTA: DNS_X_WARP3 (three warps, four lines each), DNS_X_WARP6 (six
+ *     warps, two lines each) for lengths with warp plans, DNS_X_BLOCK (block
+ *     FFT, every grid).
  *   DNS_PASS_Y2: the banded wall-normal solves; the block shape of the
  *     factor stream (ring stages x bytes per stage; the tilting table in
  *     shared memory or read through L1; the stream read with the L2
@@ -214,13 +218,15 @@ enum {
   DNS_PASS_ZB = 2,
   DNS_PASS_ZF = 3,
   DNS_PASS_Y2 = 4,
-  DNS_NUM_PASSES = 5,
+  DNS_PASS_X = 5,
+  DNS_NUM_PASSES = 6,
   DNS_MAX_VARIANTS = 4
 };
 enum { DNS_Y3_FFT = 0, DNS_Y3_TENSOR = 1, DNS_Y3_BLOCK = 2 };
 enum { DNS_Y1_WARP = 0, DNS_Y1_BLOCK = 1 };
 enum { DNS_Z_TENSOR_COPY = 0, DNS_Z_WARP = 1, DNS_Z_BLOCK = 2 };
 enum { DNS_Y2_RING3_12K = 0, DNS_Y2_RING3_12K_EF = 1, DNS_Y2_RING2_8K_EF = 2, DNS_Y2_RING3_8K_EF = 3 };
+enum { DNS_X_WARP3 = 0, DNS_X_WARP6 = 1, DNS_X_BLOCK = 2 };
 dns_status dns_set_variant(dns_ctx* ctx, int pass, int variant);
 dns_status dns_get_variant(const dns_ctx* ctx, int pass, int* variant);
 dns_status dns_autotune(dns_ctx* ctx, double* ms);

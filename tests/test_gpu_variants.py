@@ -1,10 +1,10 @@
 """GPU: every compiled variant of every tunable pass (wall-normal backward and
-forward passes, spanwise inverse and forward passes, the block shapes of the
-banded solve) gives the step of the
+forward passes, spanwise inverse and forward passes, the streamwise pass,
+the block shapes of the banded solve) gives the step of the
 default variants: in FP64 to 1e-12 relative (the parity bar; measured
 differences are rounding, ~1e-15), in the mixed form to 1e-6 against the
-FP64 step.  192x192x128 (128x33x128 modes): lengths with warp plans in both
-precisions (Pz = 192, M = 128), so every variant is available; 3 steps after
+FP64 step.  384x384x128 (256x33x256 modes): lengths with warp plans in both
+precisions (Px = Pz = 384, M = 128), so every variant is available; 3 steps after
 the bootstrap from the seeded state, Re 1300, Ro 0.1, dt 0.005."""
 import numpy as np
 import pytest
@@ -24,10 +24,10 @@ def _rel(a, b):
 
 
 def _run(pkg, prec, variants=None, steps=3):
-    c = pkg.Context(pkg.make_params(192, 192, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+    c = pkg.Context(pkg.make_params(384, 384, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
     for p, v in (variants or {}).items():
         c.set_variant(p, v)
-    c.set_state(*pkg.seeded_state(128, 33, 128, amplitude=0.1, seed=0))
+    c.set_state(*pkg.seeded_state(256, 33, 256, amplitude=0.1, seed=0))
     c.bootstrap()
     c.step(steps)
     V, O = c.get_state()
@@ -37,7 +37,7 @@ def _run(pkg, prec, variants=None, steps=3):
 
 
 def _available(pkg, prec):
-    c = pkg.Context(pkg.make_params(192, 192, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+    c = pkg.Context(pkg.make_params(384, 384, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
     out = {}
     for p in range(pkg.NUM_PASSES):
         out[p] = []
@@ -57,7 +57,8 @@ def test_available_variants(pkg):
     rings = [pkg.Y2_RING3_12K, pkg.Y2_RING3_12K_EF, pkg.Y2_RING2_8K_EF, pkg.Y2_RING3_8K_EF]
     assert a64 == {pkg.PASS_Y3: [pkg.Y3_FFT, pkg.Y3_BLOCK], pkg.PASS_Y1: [pkg.Y1_WARP, pkg.Y1_BLOCK],
                    pkg.PASS_ZB: [pkg.Z_WARP, pkg.Z_BLOCK], pkg.PASS_ZF: [pkg.Z_WARP, pkg.Z_BLOCK],
-                   pkg.PASS_Y2: rings}
+                   pkg.PASS_Y2: rings, pkg.PASS_X: [pkg.X_WARP3, pkg.X_WARP6, pkg.X_BLOCK]}
+    assert amx[pkg.PASS_X] == [pkg.X_WARP3, pkg.X_WARP6, pkg.X_BLOCK]
     assert amx[pkg.PASS_Y2] == rings
     assert amx[pkg.PASS_ZB] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
     assert amx[pkg.PASS_ZF] == [pkg.Z_TENSOR_COPY, pkg.Z_WARP, pkg.Z_BLOCK]
@@ -80,5 +81,5 @@ def test_every_variant_same_step(pkg, prec, parity_log):
             e = max(_rel(V, base[0]), _rel(O, base[1]))
             worst[f"{pkg.PASS_NAMES[p]}:{pkg.VARIANT_NAMES[p][v]}"] = e
             assert e < tol, (prec, pkg.PASS_NAMES[p], pkg.VARIANT_NAMES[p][v], e)
-    parity_log.append(f"variants, {prec}, 3 steps at 192x192x128 vs the FP64 default step: " +
+    parity_log.append(f"variants, {prec}, 3 steps at 384x384x128 vs the FP64 default step: " +
                       ", ".join(f"{k} {e:.1e}" for k, e in worst.items()))
