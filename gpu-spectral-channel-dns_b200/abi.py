@@ -30,7 +30,7 @@ EXPORTS = [
     "dns_init_aux_matrix", "dns_transform_3d_one_noalloc",
     "dns_write_recovery", "dns_read_recovery", "dns_write_fields", "dns_init_flow",
     "dns_solve_wall", "dns_step_many", "dns_slab_ranges", "dns_slab_segments", "dns_check_state",
-    "dns_slab_create", "dns_slab_exchange_bytes", "dns_slab_local", "dns_slab_part",
+    "dns_slab_create", "dns_slab_exchange_bytes", "dns_slab_local", "dns_slab_part", "dns_create_batch",
     "dns_nonlinear", "dns_rhs_v", "dns_rhs_omega", "dns_rhs_mean", "dns_operator_matrices",
     "dns_operator_tables", "dns_set_wait_limit", "dns_set_variant", "dns_get_variant",
     "dns_autotune", "dns_solve_residual",
@@ -159,6 +159,7 @@ def load_library(path: str | None = None):
         "dns_slab_ranges": [i, i, i, i, i, C.POINTER(C.c_int)],
         "dns_slab_segments": [i, i, i, i, i, i, C.POINTER(SlabSegment), i, C.POINTER(C.c_int)],
         "dns_slab_create": [C.POINTER(DnsParams), i, i, C.POINTER(vp)],
+        "dns_create_batch": [C.POINTER(DnsParams), i, C.POINTER(vp)],
         "dns_slab_exchange_bytes": [vp, i, C.POINTER(sz), C.POINTER(sz)],
         "dns_slab_local": [vp, i, vp, i, i],
         "dns_slab_part": [vp, i, i, vp, vp],
@@ -279,10 +280,15 @@ class Context:
         self._call("dns_synchronize")
 
     # -- state (numpy host arrays, shape (Nz, Kx, Ny) complex128) -----------
+    @property
+    def shape(self):
+        """Shape of the state and history arrays: (Nz, Kx, Ny), a batch (n, Nz, Kx, Ny)."""
+        return (self.Nz, self.Kx, self.Ny)
+
     def _pencils(self, a):
         a = np.ascontiguousarray(a, dtype=np.complex128)
-        if a.shape != (self.Nz, self.Kx, self.Ny):
-            raise ValueError(f"expected shape {(self.Nz, self.Kx, self.Ny)}, got {a.shape}")
+        if a.shape != self.shape:
+            raise ValueError(f"expected shape {self.shape}, got {a.shape}")
         return a
 
     def set_state(self, V, O):
@@ -291,13 +297,13 @@ class Context:
         self._call("dns_set_state", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
 
     def get_state(self):
-        V = np.empty((self.Nz, self.Kx, self.Ny), dtype=np.complex128)
+        V = np.empty(self.shape, dtype=np.complex128)
         O = np.empty_like(V)
         self._call("dns_get_state", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
         return V, O
 
     def get_history(self):
-        V = np.empty((self.Nz, self.Kx, self.Ny), dtype=np.complex128)
+        V = np.empty(self.shape, dtype=np.complex128)
         O = np.empty_like(V)
         self._call("dns_get_history", V.ctypes.data, O.ctypes.data, self.Ny * 16, HOST)
         return V, O
@@ -525,3 +531,26 @@ class SlabContext(Context):
         """Enqueue one part on the context's stream (asynchronous)."""
         self._call("dns_slab_part", int(part), int(bool(boot)), C.c_void_p(send_ptr or None),
                    C.c_void_p(recv_ptr or None))
+
+
+class BatchContext(Context):
+    """A batch of independent runs of one grid (``dns_create_batch``): every
+    pass one launch for all runs; Re, Ro and dt may differ between runs.
+    State and history arrays have shape (n, Nz, Kx, Ny)."""
+
+    def __init__(self, params_list):
+        self.lib = load_library()
+        plist = list(params_list)
+        arr = (DnsParams * len(plist))(*plist)
+        h = C.c_void_p()
+        _check(self.lib, self.lib.dns_create_batch(arr, len(plist), C.byref(h)))
+        self.h = h
+        self.params = plist[0]
+        self.n = len(plist)
+        g = (C.c_int * 8)()
+        _check(self.lib, self.lib.dns_geometry(self.h, g))
+        self.Nx, self.Ny, self.Nz, self.Kx, self.Px, self.Py, self.Pz, self.H = list(g)
+
+    @property
+    def shape(self):
+        return (self.n, self.Nz, self.Kx, self.Ny)

@@ -146,14 +146,27 @@ dns_status ctx_build_wall_solver(dns_ctx* c) {
   }
   std::vector<wall::cx> fac;
   unsigned nt = std::thread::hardware_concurrency();
-  const std::string err = wall::pack_grid(gr, sv, so, fac, (int)std::min(32u, std::max(1u, nt)));
-  if (!err.empty()) return fail(DNS_ERR_SINGULAR, err);
+  // a batch: each member's factors (its Re, dt), one after another
+  for (int r = 0; r < g.nrun; ++r) {
+    std::vector<wall::cx> f1;
+    if (g.nrun > 1) {
+      gr.Re = c->runs_h[3 * (size_t)r];
+      gr.dt = c->runs_h[3 * (size_t)r + 2];
+    }
+    const std::string err = wall::pack_grid(gr, sv, so, g.nrun > 1 ? f1 : fac, (int)std::min(32u, std::max(1u, nt)));
+    if (!err.empty()) return fail(DNS_ERR_SINGULAR, err);
+    if (g.nrun > 1) fac.insert(fac.end(), f1.begin(), f1.end());
+  }
   std::vector<double> Q((size_t)7 * wd.no);
   if (!wall::tilting_table(N, wd.no, c->ph.U1, c->ph.U2, Q.data()))
     return fail(DNS_ERR_ARG, "tilting table outside its band");
   wd.group_complex = pk.group_complex;
   wd.nslots = (long long)g.Kx * (sl ? sl->s1 - sl->s0 : g.Kh);
   wd.ngroups = (wd.nslots + 15) / 16;
+  if (g.nrun > 1) {
+    wd.groups_per_run = wd.ngroups;
+    wd.ngroups *= g.nrun;
+  }
   if (wall_smem_bytes(wd, DNS_Y2_RING2_8K_EF) > 227 * 1024) return fail(DNS_ERR_ARG, "Ny too large for the wall solve");
   if (wall_scratch_complex(wd) * 16 > c->F6_bytes)
     return fail(DNS_ERR_ARG, "wall solve scratch does not fit the transform buffer");
@@ -177,12 +190,21 @@ struct StepBufs {
 template <typename C>
 cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const DevFft<C>& fx,
                              const DevFft<C>& fyP, cudaEvent_t* ev, StepBufs b) {
-  const DnsGeom& g = c->g;
-  const long long H = g.H;
-  PencilArr F6p{c->F6, c->PyS, H * c->PyS};
-  RowArr G6r{c->G6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
-  RowArr G3r{c->F6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
-  PencilArr F3p{c->G6, c->PyS, H * c->PyS};
+  const DnsGeom& g = c->g;  // one member's grid (g.nrun members in a batch)
+  const long long H = g.H, NR = g.nrun, PR = (long long)g.Py * g.Pz * c->KxS;
+  // a batch keeps every field field-major, then member-major: the
+  // wall-normal passes see NR H pencils (gb), the spanwise passes 6 NR or
+  // 3 NR fields, the streamwise pass NR Py Pz rows
+  DnsGeom gb = g;
+  gb.H = NR * H;
+  PencilArr F6p{c->F6, c->PyS, NR * H * c->PyS};  // y3 out
+  PencilArr F6z{c->F6, c->PyS, H * c->PyS};       // zb in
+  RowArr G6r{c->G6, c->KxS, PR};                  // zb out
+  RowArr G6x{c->G6, c->KxS, NR * PR};             // x in
+  RowArr G3x{c->F6, c->KxS, NR * PR};             // x out
+  RowArr G3r{c->F6, c->KxS, PR};                  // zf in
+  PencilArr F3p{c->G6, c->PyS, H * c->PyS};       // zf out
+  PencilArr F3y{c->G6, c->PyS, NR * H * c->PyS};  // y1 in
   cudaError_t e;
   int k = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[k++], c->st); };
@@ -195,20 +217,20 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
     return r == cudaErrorNotSupported ? launch(VAR_AUTO) : r;
   };
   if (std::is_same<C, float2>::value && c->variant[DNS_PASS_Y3] == DNS_Y3_TENSOR)
-    e = launch_y3tc(b.V, b.O, F6p, g, c->ph, c->y3tc_tab, c->status, c->st);
+    e = launch_y3tc(b.V, b.O, F6p, gb, c->ph, c->y3tc_tab, c->status, c->st);
   else
-    e = var(DNS_PASS_Y3, [&](int v) { return launch_y3<C>(b.V, b.O, F6p, g, c->ph, fyP.tab(), c->status, c->st, v); });
+    e = var(DNS_PASS_Y3, [&](int v) { return launch_y3<C>(b.V, b.O, F6p, gb, c->ph, fyP.tab(), c->status, c->st, v); });
   if (e) return e;
   mark();
-  if ((e = var(DNS_PASS_ZB, [&](int v) { return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v); })))
+  if ((e = var(DNS_PASS_ZB, [&](int v) { return launch_zb<C>(F6z, G6r, 6 * (int)NR, g, fz.tab(), c->st, c->status, v); })))
     return e;
   mark();
   if ((e = var(DNS_PASS_X, [&](int v) {
-         return launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v);
+         return launch_x_fused<C>(G6x, G3x, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v, false, c->ph.runs);
        })))
     return e;
   mark();
-  if ((e = var(DNS_PASS_ZF, [&](int v) { return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v); })))
+  if ((e = var(DNS_PASS_ZF, [&](int v) { return launch_zf<C>(G3r, F3p, 3 * (int)NR, g, fz.tab(), c->st, c->status, v); })))
     return e;
   mark();
   const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
@@ -217,7 +239,7 @@ cudaError_t enqueue_pipeline(dns_ctx* c, int boot, const DevFft<C>& fz, const De
   const RhsTabs tb{t0, t0 + 4 * nv, t0 + 4 * nv + 2 * no, t0 + 4 * nv + 2 * no + g.Ny,
                    t0 + 4 * nv + 2 * no + g.Ny + 5 * nv};
   if ((e = var(DNS_PASS_Y1, [&](int v) {
-         return launch_y1<C>(F3p, b.V, b.O, b.Nvp, b.Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(), boot,
+         return launch_y1<C>(F3y, b.V, b.O, b.Nvp, b.Nop, c->rv, c->ro, rd, tb, gb, c->ph, fyP.tab(), boot,
                              c->status, c->st, v);
        })))
     return e;
@@ -244,32 +266,39 @@ cudaError_t enqueue(dns_ctx* c, int boot, cudaEvent_t* ev = nullptr, const StepB
 template <typename C>
 bool probe_pass(const dns_ctx* c, int pass, int v, const DevFft<C>& fz, const DevFft<C>& fyP) {
   const DnsGeom& g = c->g;
-  const long long H = g.H;
-  PencilArr F6p{c->F6, c->PyS, H * c->PyS};
-  RowArr G6r{c->G6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
-  RowArr G3r{c->F6, c->KxS, (long long)g.Py * g.Pz * c->KxS};
+  const long long H = g.H, NR = g.nrun, PR = (long long)g.Py * g.Pz * c->KxS;
+  DnsGeom gb = g;
+  gb.H = NR * H;
+  PencilArr F6p{c->F6, c->PyS, NR * H * c->PyS};
+  PencilArr F6z{c->F6, c->PyS, H * c->PyS};
+  RowArr G6r{c->G6, c->KxS, PR};
+  RowArr G6x{c->G6, c->KxS, NR * PR};
+  RowArr G3x{c->F6, c->KxS, NR * PR};
+  RowArr G3r{c->F6, c->KxS, PR};
   PencilArr F3p{c->G6, c->PyS, H * c->PyS};
+  PencilArr F3y{c->G6, c->PyS, NR * H * c->PyS};
   switch (pass) {
     case DNS_PASS_Y3:
       if (v == DNS_Y3_TENSOR)
         return std::is_same<C, float2>::value && g.Ny == 129 && g.Py == 257;
-      return launch_y3<C>(c->V, c->O, F6p, g, c->ph, fyP.tab(), c->status, c->st, v, true) == cudaSuccess;
+      return launch_y3<C>(c->V, c->O, F6p, gb, c->ph, fyP.tab(), c->status, c->st, v, true) == cudaSuccess;
     case DNS_PASS_Y1: {
       const RhsDims rd{c->wd.nv, c->wd.no, c->wd.gp};
       const RhsTabs tb{};
-      return launch_y1<C>(F3p, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, g, c->ph, fyP.tab(), 0,
+      return launch_y1<C>(F3y, c->V, c->O, c->Nvp, c->Nop, c->rv, c->ro, rd, tb, gb, c->ph, fyP.tab(), 0,
                           c->status, c->st, v, true) == cudaSuccess;
     }
     case DNS_PASS_ZB:
-      return launch_zb<C>(F6p, G6r, 6, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
+      return launch_zb<C>(F6z, G6r, 6 * (int)NR, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
     case DNS_PASS_ZF:
-      return launch_zf<C>(G3r, F3p, 3, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
+      return launch_zf<C>(G3r, F3p, 3 * (int)NR, g, fz.tab(), c->st, c->status, v, true) == cudaSuccess;
     case DNS_PASS_Y2:
       return v < DNS_WALL_VARIANTS && wall_smem_bytes(c->wd, v) <= 227 * 1024;
     case DNS_PASS_X: {
       const DevFft<C>& fx = *(const DevFft<C>*)(std::is_same<C, float2>::value ? (const void*)&c->fx_f
                                                                                : (const void*)&c->fx_d);
-      return launch_x_fused<C>(G6r, G3r, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v, true) == cudaSuccess;
+      return launch_x_fused<C>(G6x, G3x, g, fx.tab(), c->Uy, c->ph.Ro, c->status, c->st, v, true, c->ph.runs) ==
+             cudaSuccess;
     }
   }
   return false;
@@ -373,12 +402,31 @@ dns_status dns_read_parameter_file(const char* path, dns_params* p, dns_run_para
 
 dns_status dns_create(const dns_params* p, dns_ctx** out) { return ctx_create(p, nullptr, out); }
 
+dns_status dns_create_batch(const dns_params* runs, int nruns, dns_ctx** out) {
+  if (!runs || !out || nruns < 1) return fail(DNS_ERR_ARG, "null argument or no runs");
+  if (nruns > DNS_MAX_BATCH) return fail(DNS_ERR_ARG, "too many runs in one batch");
+  std::vector<double> t(3 * (size_t)nruns);
+  const dns_params& a = runs[0];
+  for (int r = 0; r < nruns; ++r) {
+    const dns_params& b = runs[r];
+    if (b.mx != a.mx || b.my != a.my || b.mz != a.mz || b.n_pi_x != a.n_pi_x || b.n_pi_y != a.n_pi_y ||
+        b.U0 != a.U0 || b.U1 != a.U1 || b.U2 != a.U2 || b.precision != a.precision || b.device != a.device)
+      return fail(DNS_ERR_ARG, "the runs of a batch share grid, box, base flow, precision and device");
+    if (!(b.Re > 0) || !(b.dt > 0)) return fail(DNS_ERR_ARG, "Re and dt must be positive");
+    t[3 * (size_t)r] = b.Re;
+    t[3 * (size_t)r + 1] = b.Ro;
+    t[3 * (size_t)r + 2] = b.dt;
+  }
+  return ctx_create(&a, nullptr, out, nruns, t.data());
+}
+
 // A context of the whole grid (slab == NULL) or of one slab rank: then the
 // pencil arrays hold the rank's pencils only and the transform buffers its
 // pencils (all planes) and its planes (all pencils); the context takes
 // ownership of slab.
-dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out) {
+dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out, int nrun, const double* runs) {
   std::unique_ptr<SlabState> own(slab);
+  if (nrun < 1 || (nrun > 1 && (!runs || slab))) return fail(DNS_ERR_ARG, "bad batch");
   if (!p || !out) return fail(DNS_ERR_ARG, "null argument");
   *out = nullptr;
   if (p->mx <= 0 || p->my <= 0 || p->mz <= 0 || p->mz % 4 != 0)
@@ -388,6 +436,7 @@ dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out) {
   if (p->precision != DNS_PREC_FP64 && p->precision != DNS_PREC_MIXED)
     return fail(DNS_ERR_ARG, "unknown precision");
   DnsGeom g = dns_make_geom(p->mx, p->my, p->mz);
+  g.nrun = nrun;
   if (g.Nx < 2 || g.Nz < 2 || g.Nx % 2 || g.Nz % 2 || g.Ny < 5)
     return fail(DNS_ERR_ARG, "need even Nx, Nz >= 2 and Ny >= 5");
   if (!fft_len_ok(g.Px) || !fft_len_ok(g.Pz) || !fft_len_ok(p->mz) || !fft_len_ok(p->mz / 2))
@@ -445,13 +494,15 @@ dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out) {
     f6 = (size_t)6 * sl->np * c->PyS;
     g6 = std::max((size_t)6 * sl->ny * g.Pz * c->KxS, (size_t)3 * g.H * sl->nyS);
   }
-  const size_t hn = (size_t)(sl ? sl->np : g.H) * Ny;
+  f6 *= (size_t)nrun;  // a batch: every member's fields
+  g6 *= (size_t)nrun;
+  const size_t hn = (size_t)(sl ? sl->np : g.H * nrun) * Ny;
   // integrated right-hand sides: N + deg(U) + 1 rows per pencil
   c->wd.delta = wall::base_degree(p->U1, p->U2);
   c->wd.nv = c->wd.no = Ny + c->wd.delta;
   c->wd.gp = c->wd.nv;
   c->wd.qbytes = (int)((7 * (size_t)c->wd.no * 8 + 15) & ~(size_t)15);
-  const size_t gn = (size_t)(sl ? sl->np : g.H) * c->wd.gp;
+  const size_t gn = (size_t)(sl ? sl->np : g.H * nrun) * c->wd.gp;
   if ((e = c->alloc(&c->T0, NN)) || (e = c->alloc(&c->T2, NN)) || (e = c->alloc(&c->T4, NN)) ||
       (e = c->alloc(&c->Ut, Ny)) || (e = c->alloc(&c->dUt, Ny)) || (e = c->alloc(&c->ddUt, Ny)) ||
       (e = c->alloc(&c->Uy, g.Py)) || (e = c->alloc(&c->V, hn)) || (e = c->alloc(&c->O, hn)) ||
@@ -493,6 +544,13 @@ dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out) {
     }
     cudaMemcpy(c->rtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice);
   }
+  if (nrun > 1) {
+    c->runs_h.assign(runs, runs + 3 * (size_t)nrun);
+    if ((e = c->alloc(&c->runs_d, 3 * (size_t)nrun)) ||
+        (e = cudaMemcpy(c->runs_d, runs, 3 * (size_t)nrun * 8, cudaMemcpyHostToDevice)))
+      return bail(fail(DNS_ERR_CUDA, std::string("device allocation: ") + cudaGetErrorString(e)));
+    c->ph.runs = c->runs_d;
+  }
   cudaMemset(c->status, 0, sizeof(int));
   cudaMemset(c->Nvp, 0, hn * 16);
   cudaMemset(c->Nop, 0, hn * 16);
@@ -514,6 +572,7 @@ dns_status dns_destroy(dns_ctx* c) {
                   c->y3tc_tab};
   for (void* q : ptrs) cudaFree(q);
   if (c->slab) cudaFree(c->slab->A);
+  cudaFree(c->runs_d);
   delete c->slab;
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -551,16 +610,17 @@ dns_status dns_memory_bytes(const dns_ctx* c, size_t* b) {
 static dns_status copy_pencils(dns_ctx* c, double2* dev, const void* src, void* dst, size_t pitch,
                                int where, bool to_dev) {
   const size_t w = (size_t)c->g.Ny * 16;
+  const long long nH = c->g.H * c->g.nrun;  // every member of a batch
   if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
   const cudaMemcpyKind k = kind_of(where, to_dev);
   if (pitch == w) {
-    if (to_dev) CK(cudaMemcpyAsync(dev, src, w * (size_t)c->g.H, k, c->st));
-    else CK(cudaMemcpyAsync(dst, dev, w * (size_t)c->g.H, k, c->st));
+    if (to_dev) CK(cudaMemcpyAsync(dev, src, w * (size_t)nH, k, c->st));
+    else CK(cudaMemcpyAsync(dst, dev, w * (size_t)nH, k, c->st));
   } else if (to_dev) {
-    CK(cudaMemcpy2DAsync(dev, w, src, pitch, w, (size_t)c->g.H, k, c->st));
+    CK(cudaMemcpy2DAsync(dev, w, src, pitch, w, (size_t)nH, k, c->st));
   } else {
-    CK(cudaMemcpy2DAsync(dst, pitch, dev, w, w, (size_t)c->g.H, k, c->st));
+    CK(cudaMemcpy2DAsync(dst, pitch, dev, w, w, (size_t)nH, k, c->st));
   }
   return DNS_OK;
 }
@@ -595,12 +655,17 @@ static dns_status history_out(dns_ctx* c, const double2* src, void* dst, size_t 
   dns_status s = need_scratch(c);
   if (s) return s;
   const size_t w = (size_t)c->g.Ny * 16, ps = (size_t)(c->P.mz / 2);
-  CK(cudaMemcpy2DAsync(c->scratch, ps * 16, src, w, w, (size_t)c->g.H, cudaMemcpyDeviceToDevice, c->st));
-  PencilArr a{c->scratch, (long long)ps, 0};
-  CK(launch_cheby_inplace<double2>(a, c->g.H, 1, c->g.Ny, c->fy0_d.tab(), c->st));
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
   if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
-  CK(cudaMemcpy2DAsync(dst, pitch, c->scratch, ps * 16, w, (size_t)c->g.H, kind_of(where, false), c->st));
+  const long long H = c->g.H;
+  for (int r = 0; r < c->g.nrun; ++r) {  // a batch: member by member through the scratch
+    CK(cudaMemcpy2DAsync(c->scratch, ps * 16, src + r * H * c->g.Ny, w, w, (size_t)H, cudaMemcpyDeviceToDevice,
+                         c->st));
+    PencilArr a{c->scratch, (long long)ps, 0};
+    CK(launch_cheby_inplace<double2>(a, H, 1, c->g.Ny, c->fy0_d.tab(), c->st));
+    CK(cudaMemcpy2DAsync((char*)dst + (size_t)r * H * pitch, pitch, c->scratch, ps * 16, w, (size_t)H,
+                         kind_of(where, false), c->st));
+  }
   CK(cudaStreamSynchronize(c->st));
   return DNS_OK;
 }
@@ -610,10 +675,15 @@ static dns_status history_in(dns_ctx* c, double2* dst, const void* src, size_t p
   const size_t w = (size_t)c->g.Ny * 16, ps = (size_t)(c->P.mz / 2);
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "where must be DNS_HOST or DNS_DEVICE");
   if (pitch < w || pitch % 16) return fail(DNS_ERR_ARG, "pencil pitch must be >= Ny*16 and a multiple of 16");
-  CK(cudaMemcpy2DAsync(c->scratch, ps * 16, src, pitch, w, (size_t)c->g.H, kind_of(where, true), c->st));
-  PencilArr a{c->scratch, (long long)ps, 0};
-  CK(launch_cheby_inplace<double2>(a, c->g.H, 3, c->g.Ny, c->fy0_d.tab(), c->st));
-  CK(cudaMemcpy2DAsync(dst, w, c->scratch, ps * 16, w, (size_t)c->g.H, cudaMemcpyDeviceToDevice, c->st));
+  const long long H = c->g.H;
+  for (int r = 0; r < c->g.nrun; ++r) {
+    CK(cudaMemcpy2DAsync(c->scratch, ps * 16, (const char*)src + (size_t)r * H * pitch, pitch, w, (size_t)H,
+                         kind_of(where, true), c->st));
+    PencilArr a{c->scratch, (long long)ps, 0};
+    CK(launch_cheby_inplace<double2>(a, H, 3, c->g.Ny, c->fy0_d.tab(), c->st));
+    CK(cudaMemcpy2DAsync(dst + r * H * c->g.Ny, w, c->scratch, ps * 16, w, (size_t)H, cudaMemcpyDeviceToDevice,
+                         c->st));
+  }
   CK(cudaStreamSynchronize(c->st));
   return DNS_OK;
 }
@@ -650,6 +720,7 @@ dns_status dns_bootstrap(dns_ctx* c) {
 
 dns_status dns_nonlinear(dns_ctx* c, const void* v, const void* o, void* nv, void* no, size_t tpitch,
                          int where) {
+  if (c && c->g.nrun > 1) return fail(DNS_ERR_STATE, "a batch context: this entry point takes one run");
   if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || !v || !o || !nv || !no) return fail(DNS_ERR_ARG, "null argument");
   CK(cudaSetDevice(c->P.device));
@@ -764,7 +835,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   // pass that has one (the current variant elsewhere), one warm-up step and
   // three timed steps with events around each kernel.  The state and the
   // AB2 history are saved first and put back after.
-  const size_t hn = (size_t)c->g.H * c->g.Ny;
+  const size_t hn = (size_t)c->g.H * c->g.nrun * c->g.Ny;
   double2* save = nullptr;
   CK(cudaMalloc(&save, 4 * hn * 16));
   double2* const bufs[4] = {c->V, c->O, c->Nvp, c->Nop};
@@ -1065,10 +1136,10 @@ dns_status dns_check_state(dns_ctx* c) {
   CK(cudaSetDevice(c->P.device));
   if (!c->probe) CK(c->alloc(&c->probe, 1));
   CK(cudaMemsetAsync(c->probe, 0, sizeof(int), c->st));
-  CK(launch_nonfinite(c->V, c->O, c->g.H * c->g.Ny, c->probe, c->st));
+  CK(launch_nonfinite(c->V, c->O, c->g.H * c->g.nrun * c->g.Ny, c->probe, c->st));
   // the AB2 history too: it is written to recovery files, and a non-finite
   // nonlinear term reaches the state only one step later
-  CK(launch_nonfinite(c->Nvp, c->Nop, c->g.H * c->g.Ny, c->probe, c->st));
+  CK(launch_nonfinite(c->Nvp, c->Nop, c->g.H * c->g.nrun * c->g.Ny, c->probe, c->st));
   int bad = 0;
   CK(cudaMemcpyAsync(&bad, c->probe, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -1105,6 +1176,7 @@ cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo,
 }  // namespace
 
 dns_status dns_solve_wall(dns_ctx* c, void* v, void* omega, size_t tpitch, int where) {
+  if (c && c->g.nrun > 1) return fail(DNS_ERR_STATE, "a batch context: this entry point takes one run");
   if (c && c->slab) return fail(DNS_ERR_STATE, "a slab rank's context: use dns_slab_local and dns_slab_part");
   if (!c || (!v && !omega)) return fail(DNS_ERR_ARG, "null argument");
   if (where != DNS_HOST && where != DNS_DEVICE) return fail(DNS_ERR_ARG, "bad where");

@@ -80,6 +80,8 @@ struct dns_ctx {
   const void* solve_key[2] = {nullptr, nullptr};
   size_t solve_pitch = 0;
   SlabState* slab = nullptr;  // set on the contexts of dns_slab_create
+  std::vector<double> runs_h;  // a batch (g.nrun > 1): per-member (Re, Ro, dt)
+  double* runs_d = nullptr;    // the same on the device (ph.runs)
 
   template <typename T> cudaError_t alloc(T** p, size_t n) {
     bytes += n * sizeof(T);
@@ -92,7 +94,10 @@ struct dns_ctx {
 dns_status dns_internal_fail(dns_status s, const char* msg);
 
 // context.cu internals used by the slab-decomposed step (slabstep.cu)
-extern "C" dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out);
+// nrun > 1: a batch of nrun runs of p's grid with per-member (Re, Ro, dt)
+// in runs (3 each)
+extern "C" dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out, int nrun = 1,
+                                 const double* runs = nullptr);
 dns_status ctx_check_status(dns_ctx* c);
 dns_status ctx_build_wall_solver(dns_ctx* c);
 // slab.cpp: the runs of pencils of a rank (their count, or -1)

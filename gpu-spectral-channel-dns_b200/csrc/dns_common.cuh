@@ -62,6 +62,9 @@ struct DnsGeom {
   int Kh;           // spanwise pencils that own an operator: Nz/2 + 1
   int kz0;          // spanwise index of a launch's first pencil (wall-normal passes
                     // on a run of pencils kz0 .. kz0 + H/Kx - 1; 0 for the whole grid)
+  long long Hrun;   // pencils per member of a batch of runs (= H for one run): pencil
+                    // p of a launch is pencil p mod Hrun of member p / Hrun
+  int nrun;         // members of a batch (1 for one run)
 };
 
 static inline DnsGeom dns_make_geom(int mx, int my, int mz) {
@@ -73,7 +76,17 @@ static inline DnsGeom dns_make_geom(int mx, int my, int mz) {
   g.H = (long long)g.Kx * g.Nz;
   g.Kh = g.Nz / 2 + 1;
   g.kz0 = 0;
+  g.Hrun = g.H;
+  g.nrun = 1;
   return g;
+}
+
+// member, streamwise and spanwise index of pencil p of a wall-normal launch
+DNS_HD void pencil_modes(const DnsGeom& g, long long p, int& run, int& kx, int& kz) {
+  run = (int)(p / g.Hrun);
+  const long long q = p - (long long)run * g.Hrun;
+  kx = (int)(q % g.Kx);
+  kz = g.kz0 + (int)(q / g.Kx);
 }
 
 // ia^2 + ib^2 rounded like the reference's host code (no FMA contraction)

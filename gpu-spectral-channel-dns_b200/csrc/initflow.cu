@@ -51,6 +51,8 @@ __global__ void k_init_flow(double* __restrict__ w, double* __restrict__ oz, lon
 }  // namespace
 
 extern "C" dns_status dns_init_flow(dns_ctx* c) {
+  if (c && (c->g.nrun > 1 || c->slab))
+    return dns_internal_fail(DNS_ERR_STATE, "a batch or slab context: this entry point takes one whole run");
   if (!c) return dns_internal_fail(DNS_ERR_ARG, "null context");
   if (cudaSetDevice(c->P.device)) return dns_internal_fail(DNS_ERR_CUDA, "cudaSetDevice");
   const DnsGeom& g = c->g;

@@ -47,6 +47,8 @@ struct File {
 extern "C" {
 
 dns_status dns_write_recovery(dns_ctx* c, const char* path) {
+  if (c && (c->g.nrun > 1 || c->slab))
+    return dns_internal_fail(DNS_ERR_STATE, "a batch or slab context: this entry point takes one whole run");
   if (!c || !path) return dns_internal_fail(DNS_ERR_ARG, "null argument");
   if (cudaSetDevice(c->P.device)) return dns_internal_fail(DNS_ERR_CUDA, "cudaSetDevice");
   const DnsGeom& g = c->g;
@@ -79,6 +81,8 @@ dns_status dns_write_recovery(dns_ctx* c, const char* path) {
 }
 
 dns_status dns_read_recovery(dns_ctx* c, const char* path) {
+  if (c && (c->g.nrun > 1 || c->slab))
+    return dns_internal_fail(DNS_ERR_STATE, "a batch or slab context: this entry point takes one whole run");
   if (!c || !path) return dns_internal_fail(DNS_ERR_ARG, "null argument");
   if (cudaSetDevice(c->P.device)) return dns_internal_fail(DNS_ERR_CUDA, "cudaSetDevice");
   const DnsGeom& g = c->g;
@@ -109,6 +113,8 @@ dns_status dns_read_recovery(dns_ctx* c, const char* path) {
 }
 
 dns_status dns_write_fields(dns_ctx* c, const char* velocity_path, const char* vorticity_path) {
+  if (c && (c->g.nrun > 1 || c->slab))
+    return dns_internal_fail(DNS_ERR_STATE, "a batch or slab context: this entry point takes one whole run");
   if (!c || (!velocity_path && !vorticity_path)) return dns_internal_fail(DNS_ERR_ARG, "null argument");
   if (cudaSetDevice(c->P.device)) return dns_internal_fail(DNS_ERR_CUDA, "cudaSetDevice");
   const DnsGeom& g = c->g;

@@ -56,7 +56,12 @@ struct PhysParams {
   double Re, Ro, dt;
   double U0, U1, U2;    // base flow U(y) = U0 + U1 y + U2 y^2
   long long wait_limit = DNS_WAIT_LIMIT;  // staging waits of the wall-normal warp passes
+  const double* runs = nullptr;  // a batch's per-member (Re, Ro, dt), 3 each; null: one run
 };
+// a batch member's parameters (the context's own for one run)
+DNS_HD double run_Re(const PhysParams& ph, int r) { return ph.runs ? ph.runs[3 * r] : ph.Re; }
+DNS_HD double run_Ro(const PhysParams& ph, int r) { return ph.runs ? ph.runs[3 * r + 1] : ph.Ro; }
+DNS_HD double run_dt(const PhysParams& ph, int r) { return ph.runs ? ph.runs[3 * r + 2] : ph.dt; }
 
 // 16-byte alignment of a device pointer (bulk-copy sources)
 inline bool aligned16(const void* p) { return ((unsigned long long)p & 15ull) == 0; }

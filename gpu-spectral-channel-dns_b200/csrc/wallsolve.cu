@@ -98,19 +98,23 @@ __global__ void __launch_bounds__(32) k_wall_solve(const double2* __restrict__ f
 
   const int lane = threadIdx.x;
   const int q = lane >> 1, b = lane & 1;
-  const long long slot = (long long)blockIdx.x * 16 + q;
+  // member of a batch (its groups are consecutive CTAs)
+  const long long gpr = wd.groups_per_run > 0 ? wd.groups_per_run : (long long)gridDim.x;
+  const int run = (int)(blockIdx.x / gpr);
+  const long long slot = ((long long)blockIdx.x - run * gpr) * 16 + q;
   const bool valid = slot < wd.nslots;
   const int kx = valid ? (int)(slot % g.Kx) : 0;
   const int kzs = valid ? wd.kzs0 + (int)(slot / g.Kx) : 0;
   const int npen = (kzs == 0 || kzs == g.Nz / 2) ? 1 : 2;
   const bool active = valid && b < npen;
   const int kz = (b == 0) ? kzs : g.Nz - kzs;
-  const long long pen = (b == 0) ? wd.rowa + (long long)(kz - wd.kza) * g.Kx + kx
-                                 : wd.rowb + (long long)(kz - wd.kzb) * g.Kx + kx;
+  const long long pen = (long long)run * g.Hrun +
+                        ((b == 0) ? wd.rowa + (long long)(kz - wd.kza) * g.Kx + kx
+                                  : wd.rowb + (long long)(kz - wd.kzb) * g.Kx + kx);
   const bool zero = valid && kzs == 0 && kx == 0;
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-  const double kap = (zero || !wd.tilt) ? 0.0 : -0.5 * ib * ph.dt;  // tilting weight of this pencil
+  const double kap = (zero || !wd.tilt) ? 0.0 : -0.5 * ib * run_dt(ph, run);  // tilting weight of this pencil
   const int N = g.Ny - 1, Ny = g.Ny;
   // this lane's vector (right-hand side, intermediate solution, tilting
   // term) in the group's scratch, rows interleaved over the 32 lanes: a

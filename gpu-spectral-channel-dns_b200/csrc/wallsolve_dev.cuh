@@ -18,6 +18,9 @@ struct WallDims {
   // whole grid: all zero, row kz Kx + kx)
   int kzs0 = 0, kza = 0, kzb = 0;
   long long rowa = 0, rowb = 0;
+  // a batch of runs: groups per member (its factors, then the next
+  // member's); 0 for one run
+  long long groups_per_run = 0;
 };
 
 // band instance (v lower/upper, omega lower/upper) for base-flow degree delta

@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
       for (int j = 0; j < TC_NP; ++j) {
         const long long p = t * TC_NP + j;
-        const int kx = (int)(p % g.Kx), kz = g.kz0 + (int)(p / g.Kx);
+        int run, kx, kz;
+        pencil_modes(g, p, run, kx, kz);
         double ia, ib;
         wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
         const bool zero = kx == 0 && kz == 0;
@@ -405,7 +406,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (p < H) {
           float2 x[5];
           for (int q = 0; q < 5; ++q) x[q] = make_float2(sd.centre[j * 10 + 2 * q], sd.centre[j * 10 + 2 * q + 1]);
-          const int kx = (int)(p % g.Kx), kz = g.kz0 + (int)(p / g.Kx);
+          int run, kx, kz;
+        pencil_modes(g, p, run, kx, kz);
           double ia, ib;
           wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
           const bool zero = kx == 0 && kz == 0;

@@ -263,8 +263,8 @@ __global__ void k_get_uvw(SixPtr a, DnsGeom g, PhysParams ph) {
   double2* Du = cv.take<double2>(Ny);
   double2* Dv = cv.take<double2>(Ny);
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -321,8 +321,8 @@ __global__ void k_rhs_nonlinear(double2* lx, double2* ly, const double2* lz, lon
   double2* Dx = cv.take<double2>(Ny);
   double2* Dy = cv.take<double2>(Ny);
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   if (kx == 0 && kz == 0) return;  // source/nonlinear.cu:157
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -404,8 +404,8 @@ __global__ void __launch_bounds__(256, 3) k_y3(const double2* __restrict__ V, co
   double2* oy = cv.take<double2>(Ny);
   C* lines = cv.take<C>((size_t)6 * ls);
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -486,8 +486,8 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   C* foy = (C*)(rb2 + 2 * VS * 16);
   C* foz = (C*)(rb2 + 2 * VS * 16 + FS);
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -676,8 +676,8 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   C* linesP = (C*)region;
 
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -729,7 +729,7 @@ __global__ void __launch_bounds__(256, 3) k_y1(PencilArr lam, const double2* __r
   }
   __syncthreads();
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
-  const double dt = ph.dt, Re = ph.Re, gam = ia * dt * 0.5;
+  const double dt = run_dt(ph, run), Re = run_Re(ph, run), gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
   double2* fv = lc;
   double2* fo = lc + Ny;
@@ -879,8 +879,8 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   double2* D1y = ly + VS;
 
   const long long p = blockIdx.x;
-  const int kx = (int)(p % g.Kx);
-  const int kz = g.kz0 + (int)(p / g.Kx);
+  int run, kx, kz;
+  pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
@@ -941,7 +941,7 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   }
   __syncthreads();
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
-  const double dt = ph.dt, Re = ph.Re, gam = ia * dt * 0.5;
+  const double dt = run_dt(ph, run), Re = run_Re(ph, run), gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
   double2* fv = lx;
   double2* fo = ly;

@@ -467,7 +467,8 @@ __device__ __forceinline__ C unpack_r2c(const C* Z, int k, int Px, bool imag_par
 // ---------------------------------------------------------------------------
 template <typename C, int L>
 __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab,
-                                                   const double* __restrict__ Uy, double Ro) {
+                                                   const double* __restrict__ Uy, double Ro,
+                                                   const double* __restrict__ runs) {
   // two rows per CTA: lines 0-2 hold row 0's packed fields (u,v) (ox,oy)
   // (w,oz), lines 3-5 row 1's; after the inverse transform a thread owning
   // point j of both rows writes lambda_x + i lambda_y of row 0 / row 1 into
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
   const int ls = FL::stride(Px);
   C* z = (C*)smem_raw;  // 6 lines (9 for the runtime-length FFT)
   const long long r0 = (long long)blockIdx.x * 2;
-  const long long nrows = (long long)g.Py * g.Pz;
+  const long long nrows = (long long)g.Py * g.Pz * g.nrun;  // a batch: members' rows one after another
   for (int t = threadIdx.x; t < 2 * 3 * Px; t += blockDim.x) {
     const int rl = t / (3 * Px);
     const int rem = t - rl * 3 * Px;
@@ -499,8 +500,11 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
     z[(size_t)(rl * 3 + q) * ls + FL::in_pos(tab, n)] = zz;
   }
   FL::template fft<true>(z, 6, ls, tab);
-  const T ro = (T)Ro;
-  const int y = (int)(r0 / g.Pz);  // both rows lie in one wall-normal plane
+  // both rows lie in one wall-normal plane of one member
+  const long long pr = (long long)g.Py * g.Pz;
+  const int run = (int)(r0 / pr);
+  const T ro = (T)(runs ? runs[3 * run + 1] : Ro);
+  const int y = (int)((r0 - run * pr) / g.Pz);
   const T Ub = (T)Uy[y < g.Py ? y : 0];
   for (int j = threadIdx.x; j < Px; j += blockDim.x) {
     const int op = FL::out_pos(j);
@@ -563,7 +567,8 @@ __global__ void __launch_bounds__(256, 3) k_x_fused(RowArr in, RowArr out, DnsGe
 template <typename C, int L, int NW>
 __global__ void __launch_bounds__(32 * NW, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr in, RowArr out, DnsGeom g,
                                                                       FftTab<C> tab, const double* __restrict__ Uy,
-                                                                      double Ro, int* status) {
+                                                                      double Ro, const double* __restrict__ runs,
+                                                                      int* status) {
   static_assert(NW == 3 || NW == 6, "three or six warps");
   constexpr int LPW = 12 / NW;  // inverse lines per warp
   constexpr int FPW = 6 / NW;   // forward lines per warp
@@ -575,7 +580,7 @@ __global__ void __launch_bounds__(32 * NW, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr i
   C* z = (C*)smem_raw;                                  // 12 lines
   uint64_t* bars = (uint64_t*)(z + (size_t)12 * LW);     // one per warp
   const long long r0 = (long long)blockIdx.x * 4;
-  const long long nrows = (long long)g.Py * g.Pz;
+  const long long nrows = (long long)g.Py * g.Pz * g.nrun;  // a batch: members' rows one after another
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C* zw = z + (size_t)LPW * warp * LW;
   // stage this warp's 2 LPW half-spectrum rows (bins 0..hx-1, 16 B aligned)
@@ -615,8 +620,11 @@ __global__ void __launch_bounds__(32 * NW, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr i
     wfft_io<C, L, LPW, true>(zw, wtw_of(tab, LPW == 4 ? 2 : 1), ld, st);
   }
   __syncthreads();
-  const T ro = (T)Ro;
-  const int y = (int)(r0 / g.Pz);  // the four rows lie in one wall-normal plane
+  // the four rows lie in one wall-normal plane of one member
+  const long long pr = (long long)g.Py * g.Pz;
+  const int run = (int)(r0 / pr);
+  const T ro = (T)(runs ? runs[3 * run + 1] : Ro);
+  const int y = (int)((r0 - run * pr) / g.Pz);
   const T Ub = (T)Uy[y < g.Py ? y : 0];
   for (int j = threadIdx.x; j < Px; j += blockDim.x) {
     const int op = wsw<C>(j);
@@ -918,13 +926,14 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
 }
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
-                           double Ro, int* status, cudaStream_t st, int variant, bool probe) {
+                           double Ro, int* status, cudaStream_t st, int variant, bool probe,
+                           const double* runs) {
   const bool any = variant == VAR_AUTO;
   return with_len_xz(g.Px, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
     if constexpr (L > 0 && WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok &&
                   WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
-      const long long nrows = (long long)g.Py * g.Pz;
+      const long long nrows = (long long)g.Py * g.Pz * g.nrun;
       // four rows per CTA within one wall-normal plane; a warp's staged
       // rows of 128 bins fit in its lines
       // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
@@ -935,13 +944,13 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
       if (ok && (any || variant == DNS_X_WARP3)) {
         if (probe) return cudaSuccess;
         cudaFuncSetAttribute(k_xw<C, L, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L, 3><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, status);
+        k_xw<C, L, 3><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
         return cudaGetLastError();
       }
       if (ok && variant == DNS_X_WARP6) {
         if (probe) return cudaSuccess;
         cudaFuncSetAttribute(k_xw<C, L, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L, 6><<<(unsigned)((nrows + 3) / 4), 192, sm, st>>>(in, out, g, tab, Uy, Ro, status);
+        k_xw<C, L, 6><<<(unsigned)((nrows + 3) / 4), 192, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
         return cudaGetLastError();
       }
     }
@@ -949,8 +958,8 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
     if (probe) return cudaSuccess;
     const size_t sm = (size_t)(L > 0 ? 6 : 9) * FLine<C, L>::stride(g.Px) * sizeof(C);
     cudaFuncSetAttribute(k_x_fused<C, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    const long long nrows = (long long)g.Py * g.Pz;  // Pz is even: row pairs share a plane
-    k_x_fused<C, L><<<(unsigned)((nrows + 1) / 2), 256, sm, st>>>(in, out, g, tab, Uy, Ro);
+    const long long nrows = (long long)g.Py * g.Pz * g.nrun;  // Pz is even: row pairs share a plane
+    k_x_fused<C, L><<<(unsigned)((nrows + 1) / 2), 256, sm, st>>>(in, out, g, tab, Uy, Ro, runs);
     return cudaGetLastError();
   });
 }
@@ -987,7 +996,7 @@ cudaError_t launch_lamb_rows(const double* const in6[6], double* const out3[3], 
   template cudaError_t launch_zb<C>(PencilArr, RowArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
   template cudaError_t launch_zf<C>(RowArr, PencilArr, int, DnsGeom, FftTab<C>, cudaStream_t, int*, int, bool); \
   template cudaError_t launch_x_fused<C>(RowArr, RowArr, DnsGeom, FftTab<C>, const double*,       \
-                                         double, int*, cudaStream_t, int, bool);                  \
+                                         double, int*, cudaStream_t, int, bool, const double*);   \
   template cudaError_t launch_x_c2r<C>(RowArr, T_of<C>*, long long, long long, DnsGeom,           \
                                        FftTab<C>, cudaStream_t);                                  \
   template cudaError_t launch_x_r2c<C>(const T_of<C>*, long long, RowArr, long long, DnsGeom,     \

@@ -11,7 +11,7 @@ cudaError_t launch_zf(RowArr in, PencilArr out, int nf, DnsGeom g, FftTab<C> tab
 template <typename C>
 cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, const double* Uy,
                            double Ro, int* status, cudaStream_t st, int variant = VAR_AUTO,
-                           bool probe = false);
+                           bool probe = false, const double* runs = nullptr);
 template <typename C>
 cudaError_t launch_x_c2r(RowArr in, T_of<C>* outr, long long rps, long long nrows, DnsGeom g,
                          FftTab<C> tab, cudaStream_t st);

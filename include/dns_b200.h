@@ -92,6 +92,18 @@ dns_status dns_read_parameter_file(const char* path, dns_params* p, dns_run_para
  * inverses (source/solver.cpp:260-320) are built on the device on the first
  * dns_bootstrap / dns_step. */
 dns_status dns_create(const dns_params* p, dns_ctx** out);
+
+/* No counterpart in the reference.  A batch of nruns independent runs of one
+ * grid (runs[i] share mx, my, mz, box, base flow, precision and device; Re,
+ * Ro and dt may differ): one context whose every pass is one launch for all
+ * runs.  State and history arrays (dns_set_state, dns_get_state,
+ * dns_set_history, dns_get_history) hold the runs one after another, H
+ * pencils each; dns_step, dns_bootstrap, dns_step_profiled, dns_autotune
+ * and dns_check_state act on all of them.  The entry points that take one
+ * run's data (recovery files, initFlow, the per-function drop-ins of the
+ * step, dns_solve_wall) refuse a batch.  nruns <= DNS_MAX_BATCH. */
+#define DNS_MAX_BATCH 1024
+dns_status dns_create_batch(const dns_params* runs, int nruns, dns_ctx** ctx);
 dns_status dns_destroy(dns_ctx* ctx);
 
 /* sizes: Nx, Ny, Nz, Kx, Px, Py, Pz, H (= Kx*Nz pencils) */
