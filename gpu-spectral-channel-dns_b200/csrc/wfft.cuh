@@ -57,6 +57,7 @@ WPLAN(512, 2, 16, 32, 16)
 WPLAN(768, 2, 16, 16, 48)
 WPLAN(384, 3, 16, 12, 4, 4, 2)
 WPLAN(384, 4, 16, 16, 24)
+WPLAN(192, 4, 16, 8, 24)
 // FP64
 WPLAN(128, 1, 8, 4, 4, 4, 2)
 WPLAN(256, 1, 8, 8, 8, 4)
@@ -71,6 +72,7 @@ WPLAN(512, 2, 8, 8, 8, 8)
 WPLAN(768, 2, 8, 8, 8, 4, 3)
 WPLAN(384, 3, 8, 6, 4, 4, 4)
 WPLAN(384, 4, 8, 8, 8, 6)
+WPLAN(192, 4, 8, 8, 4, 6)
 #undef WPLAN
 
 // One pass, split into the load (inputs of the lane's butterfly q, twiddled,

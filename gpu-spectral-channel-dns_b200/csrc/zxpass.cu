@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(32 * NW, sizeof(C) == 8 ? 5 : 2) k_xw(RowArr i
   // stage this warp's 2 LPW half-spectrum rows (bins 0..hx-1, 16 B aligned)
   // at the start of its own lines: the first FFT pass reads them all before
   // it writes its output over them
-  constexpr int SR = 128;  // staged bins per row (>= hx)
+  constexpr int SR = (hx + 15) / 16 * 16;  // staged bins per row (>= hx; 128 at L = 384)
   uint64_t* bar = bars + warp;
   if (lane == 0) {
     mbar_init(bar, 1);
@@ -931,27 +931,30 @@ cudaError_t launch_x_fused(RowArr in, RowArr out, DnsGeom g, FftTab<C> tab, cons
   const bool any = variant == VAR_AUTO;
   return with_len_xz(g.Px, [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
-    if constexpr (L > 0 && WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok &&
-                  WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
+    if constexpr (L > 0) {
       const long long nrows = (long long)g.Py * g.Pz * g.nrun;
       // four rows per CTA within one wall-normal plane; a warp's staged
-      // rows of 128 bins fit in its lines
-      // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
-      const bool tw_ok = wtw_of(tab, 0) && wtw_of(tab, 1) && wtw_of(tab, 2);
-      const bool ok = tw_ok && g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && g.Nx / 2 <= 128 && 8 * 128 <= 4 * wlen<C>(L) &&
-                      in.rs >= 128 && (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0;
+      // rows of SR >= Nx/2 bins (2 SR <= a line) fit in its lines
+      constexpr int SR = (L / 3 + 15) / 16 * 16;
+      const bool ok = g.Pz % 4 == 0 && g.Nx / 2 == L / 3 && 2 * SR <= wlen<C>(L) && in.rs >= SR &&
+                      (in.rs * sizeof(C)) % 16 == 0 && (in.fs * sizeof(C)) % 16 == 0;
       const size_t sm = ((size_t)12 * wlen<C>(L)) * sizeof(C) + 64;
-      if (ok && (any || variant == DNS_X_WARP3)) {
-        if (probe) return cudaSuccess;
-        cudaFuncSetAttribute(k_xw<C, L, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L, 3><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
-        return cudaGetLastError();
+      // FP32: the plans' twiddle tables; FP64: W^j with product recurrences
+      if constexpr (WPlan<L, 4, FftMaxRadix<C>::v>::ok && WPlan<L, 2, FftMaxRadix<C>::v>::ok) {
+        if (ok && wtw_of(tab, 1) && wtw_of(tab, 2) && (any || variant == DNS_X_WARP3)) {
+          if (probe) return cudaSuccess;
+          cudaFuncSetAttribute(k_xw<C, L, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+          k_xw<C, L, 3><<<(unsigned)((nrows + 3) / 4), 96, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
+          return cudaGetLastError();
+        }
       }
-      if (ok && variant == DNS_X_WARP6) {
-        if (probe) return cudaSuccess;
-        cudaFuncSetAttribute(k_xw<C, L, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_xw<C, L, 6><<<(unsigned)((nrows + 3) / 4), 192, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
-        return cudaGetLastError();
+      if constexpr (WPlan<L, 2, FftMaxRadix<C>::v>::ok && WPlan<L, 1, FftMaxRadix<C>::v>::ok) {
+        if (ok && wtw_of(tab, 0) && wtw_of(tab, 1) && variant == DNS_X_WARP6) {
+          if (probe) return cudaSuccess;
+          cudaFuncSetAttribute(k_xw<C, L, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+          k_xw<C, L, 6><<<(unsigned)((nrows + 3) / 4), 192, sm, st>>>(in, out, g, tab, Uy, Ro, runs, status);
+          return cudaGetLastError();
+        }
       }
     }
     if (!any && variant != DNS_X_BLOCK) return cudaErrorNotSupported;

@@ -4,7 +4,8 @@ the block shapes of the banded solve) gives the step of the
 default variants: in FP64 to 1e-12 relative (the parity bar; measured
 differences are rounding, ~1e-15), in the mixed form to 1e-6 against the
 FP64 step.  384x384x128 (256x33x256 modes): lengths with warp plans in both
-precisions (Px = Pz = 384, M = 128), so every variant is available; 3 steps after
+precisions (Px = Pz = 384, M = 128), so every variant is available, and
+192x192x128 (its streamwise warp form); 3 steps after
 the bootstrap from the seeded state, Re 1300, Ro 0.1, dt 0.005."""
 import numpy as np
 import pytest
@@ -23,11 +24,14 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def _run(pkg, prec, variants=None, steps=3):
-    c = pkg.Context(pkg.make_params(384, 384, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+GRID = (384, 384, 128)
+
+
+def _run(pkg, prec, variants=None, steps=3, grid=GRID):
+    c = pkg.Context(pkg.make_params(*grid, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
     for p, v in (variants or {}).items():
         c.set_variant(p, v)
-    c.set_state(*pkg.seeded_state(256, 33, 256, amplitude=0.1, seed=0))
+    c.set_state(*pkg.seeded_state(c.Nx, c.Ny, c.Nz, amplitude=0.1, seed=0))
     c.bootstrap()
     c.step(steps)
     V, O = c.get_state()
@@ -36,8 +40,8 @@ def _run(pkg, prec, variants=None, steps=3):
     return V, O, got
 
 
-def _available(pkg, prec):
-    c = pkg.Context(pkg.make_params(384, 384, 128, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
+def _available(pkg, prec, grid=GRID):
+    c = pkg.Context(pkg.make_params(*grid, Re=1300.0, Ro=0.1, dt=0.005, precision=prec))
     out = {}
     for p in range(pkg.NUM_PASSES):
         out[p] = []
@@ -66,20 +70,21 @@ def test_available_variants(pkg):
     assert amx[pkg.PASS_Y3] == [pkg.Y3_FFT, pkg.Y3_BLOCK]  # the tensor form needs Ny = 129
 
 
+@pytest.mark.parametrize("grid", [GRID, (192, 192, 128)])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_every_variant_same_step(pkg, prec, parity_log):
+def test_every_variant_same_step(pkg, prec, grid, parity_log):
     P = pkg.PREC_FP64 if prec == "fp64" else pkg.PREC_MIXED
-    V64, O64, _ = _run(pkg, pkg.PREC_FP64)
+    V64, O64, _ = _run(pkg, pkg.PREC_FP64, grid=grid)
     base = (V64, O64)
     tol = 1e-12 if prec == "fp64" else 1e-6
-    avail = _available(pkg, P)
+    avail = _available(pkg, P, grid)
     worst = {}
     for p, vs in avail.items():
         for v in vs:
-            V, O, got = _run(pkg, P, {p: v})
+            V, O, got = _run(pkg, P, {p: v}, grid=grid)
             assert got[p] == v
             e = max(_rel(V, base[0]), _rel(O, base[1]))
             worst[f"{pkg.PASS_NAMES[p]}:{pkg.VARIANT_NAMES[p][v]}"] = e
             assert e < tol, (prec, pkg.PASS_NAMES[p], pkg.VARIANT_NAMES[p][v], e)
-    parity_log.append(f"variants, {prec}, 3 steps at 384x384x128 vs the FP64 default step: " +
+    parity_log.append(f"variants, {prec}, 3 steps at {grid[0]}x{grid[1]}x{grid[2]} vs the FP64 default step: " +
                       ", ".join(f"{k} {e:.1e}" for k, e in worst.items()))
