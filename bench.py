@@ -376,7 +376,17 @@ def run_one(args):
     ctx = pkg.Context(pkg.make_params(CFG["mx"], CFG["my"], CFG["mz"], Re=CFG["Re"], Ro=CFG["Ro"],
                                       dt=CFG["dt"], precision=prec, device=0))
     ctx.set_state(V0, O0)
-    ctx.autotune()
+    if args.variant:
+        # fixed variants, no timing of candidates: under a profiler the
+        # autotuner's event times mean nothing
+        by_name = {pkg.PASS_NAMES[p]: (p, {n: v for v, n in pkg.VARIANT_NAMES[p].items()})
+                   for p in range(pkg.NUM_PASSES)}
+        for item in args.variant:
+            pname, vname = item.split("=")
+            p, names = by_name[pname]
+            ctx.set_variant(p, names[vname])
+    else:
+        ctx.autotune()
     variant = {pkg.PASS_NAMES[p]: pkg.VARIANT_NAMES[p][ctx.get_variant(p)] for p in range(pkg.NUM_PASSES)}
     ctx.bootstrap()
     ctx.step(args.warmup)
@@ -736,6 +746,9 @@ def main():
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="run one precision only (bootstrap + warm-up + timed steps), for "
                          "profiling captures; prints per-kernel times, not the bench line")
+    ap.add_argument("--variant", action="append", default=[],
+                    help="with --only: PASS=VARIANT (names as in the bench line's autotune block) "
+                         "instead of the autotuner; repeatable")
     ap.add_argument("--solve", action="store_true",
                     help="the solve-only workload (dns_solve_wall): prints its own line")
     ap.add_argument("--solve-grid", default="576,576,768",
