@@ -1160,9 +1160,14 @@ cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo,
   double2* sv = (double2*)c->F6;
   double2* so = sv + g.H * ls;
   const double* cosk = c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no;
-  cudaError_t e = launch_colloc_prep(bv, bo, bp, sv, so, ls, pbc, cosk, c->Ut, c->ddUt, g, c->ph, c->st);
-  if (!e) e = launch_cheby_inplace<double2>(PencilArr{sv, ls, 0}, 2 * g.H, 3, g.Ny, c->fy0_d.tab(), c->st);
-  if (!e) e = launch_colloc_integrate(sv, so, ls, c->rv, c->ro, c->wd, g, c->st);
+  // one kernel where the DCT length has a warp plan, else three
+  cudaError_t e = launch_colloc_fused(bv, bo, bp, pbc, cosk, c->Ut, c->ddUt, c->rv, c->ro, c->wd, g, c->ph,
+                                      c->fy0_d.tab(), c->st);
+  if (e == cudaErrorNotSupported) {
+    e = launch_colloc_prep(bv, bo, bp, sv, so, ls, pbc, cosk, c->Ut, c->ddUt, g, c->ph, c->st);
+    if (!e) e = launch_cheby_inplace<double2>(PencilArr{sv, ls, 0}, 2 * g.H, 3, g.Ny, c->fy0_d.tab(), c->st);
+    if (!e) e = launch_colloc_integrate(sv, so, ls, c->rv, c->ro, c->wd, g, c->st);
+  }
   WallDims wd = c->wd;
   wd.tilt = 0;
   if (!e) e = launch_wall_solve(c->wfac, Xv, Xo, c->rv, c->ro, c->wQ, (double2*)c->F6, wd, g, c->ph,

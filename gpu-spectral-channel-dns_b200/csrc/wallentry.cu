@@ -26,9 +26,11 @@
 //   mean:  p                                                          (p'' = 0)
 // with a = kx/aphi the streamwise wavenumber and k^2 = a^2 + b^2.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "wallsolve_dev.cuh"
+#include "wfft.cuh"
 
 namespace {
 
@@ -175,6 +177,105 @@ __global__ void __launch_bounds__(256) k_nonfinite(const double2* __restrict__ a
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
+// 1-3 fused, one CTA per pencil, one warp per system (0: v, 1: omega_y):
+// the point values of step 2 are formed in the first pass of a warp FFT of
+// the even extension (the DCT-I over the Gauss-Lobatto points, length
+// L = 2N), its coefficients written over the consumed line, and the K-fold
+// integration runs in place of the line (two halves as ping-pong buffers).
+// Compile-time L = 2 (Ny - 1); the launcher falls back to the three kernels
+// above for lengths without a warp plan.
+template <int L>
+__global__ void __launch_bounds__(64) k_colloc_fused(const double2* __restrict__ bv, const double2* __restrict__ bo,
+                                                     long long bp, double2* pbc, const double* __restrict__ cosk,
+                                                     const double* __restrict__ Ut, const double* __restrict__ ddUt,
+                                                     double2* gv, double2* go, int nv, int no, long long gp,
+                                                     DnsGeom g, PhysParams ph, FftTab<double2> tab) {
+  constexpr int N = L / 2, Ny = N + 1, LB = Ny + 8;
+  constexpr int LS = (wlen<double2>(L) > 2 * LB) ? wlen<double2>(L) : 2 * LB;  // line stride
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* line = (double2*)smem_raw + (size_t)warp * LS;
+  const long long p = blockIdx.x;
+  const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
+  const bool zero = p == 0;
+  const double2* b = (warp ? bo : bv) + p * bp;
+  // wall polynomial (every lane; rows 0..3 of the right-hand side)
+  double2 pc0, pc1, pc2 = cx(0, 0), pc3 = cx(0, 0);
+  {
+    const double2 r0 = b[0], r1 = b[1];
+    const double2 e = (r0 + r1) * 0.5, o = (r0 - r1) * 0.5;
+    pc0 = e;
+    pc1 = o;
+    if (warp == 0 && !zero) {
+      const double2 r2 = b[2], r3 = b[3];
+      pc2 = (r2 - r3) * 0.125;
+      pc3 = ((r2 + r3) * 0.5 - o) * 0.125;
+      pc0 = e - pc2;
+      pc1 = o - pc3;
+    }
+    if (lane == 0) {
+      if (warp == 0) {
+        pbc[p * 6 + 0] = pc0; pbc[p * 6 + 1] = pc1; pbc[p * 6 + 2] = pc2; pbc[p * 6 + 3] = pc3;
+      } else {
+        pbc[p * 6 + 4] = pc0; pbc[p * 6 + 5] = pc1;
+      }
+    }
+  }
+  double ia, ib;
+  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
+  const double kmn = ia * ia + ib * ib, dt = ph.dt, Re = ph.Re;
+  // point value m of the interior right-hand side minus A p (zero where the
+  // equation has no row)
+  auto fval = [&](int m) -> double2 {
+    const double y = __ldg(cosk + m);
+    if (zero || warp == 1) {
+      if (m < 1 || m > N - 1) return cx(0, 0);
+      const double2 P0 = pc0 + pc1 * y;
+      if (zero) return b[m + 1] - P0;
+      return b[m + 1] - (P0 * (1 + kmn * dt * 0.5 / Re) + muli(P0 * (ia * dt * 0.5 * __ldg(Ut + m))));
+    }
+    if (m < 2 || m > N - 2) return cx(0, 0);
+    const double2 P0 = pc0 + pc1 * y + pc2 * (2 * y * y - 1) + pc3 * (y * (4 * y * y - 3));
+    const double2 P2 = pc2 * 4.0 + pc3 * (24.0 * y);
+    const double U = __ldg(Ut + m), ddU = __ldg(ddUt + m);
+    const double2 re = P2 * (1 + kmn * dt / Re) - P0 * (kmn * (1 + kmn * dt * 0.5 / Re));
+    const double2 im = P2 * (ia * dt * 0.5 * U) - P0 * (kmn * ia * dt * 0.5 * U + ia * dt * 0.5 * ddU);
+    return b[m + 2] - (re + muli(im));
+  };
+  // DCT-I: FFT of the even extension; coefficient k = value / N, halved at
+  // k = 0 and k = N, written over the line (its last pass read it all)
+  auto ld = [&](int, int n) -> double2 { return fval(n <= N ? n : L - n); };
+  auto st = [&](int, int k, double2 v) {
+    if (k <= N) line[k] = v * ((k == 0 || k == N) ? 0.5 / N : 1.0 / N);
+  };
+  wfft_io<double2, L, 1, false>(line, wtw_of(tab, 0), ld, st, LS);
+  __syncwarp();
+  for (int k = Ny + lane; k < LB; k += 32) line[k] = cx(0, 0);
+  // K-fold integration: (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  const int K = (warp == 0 && !zero) ? 4 : 2;
+  double2* x = line;
+  double2* yb = line + LB;
+  for (int it = 0; it < K; ++it) {
+    __syncwarp();
+    for (int k = lane; k < LB; k += 32) {
+      double2 r = cx(0, 0);
+      if (k >= 1) {
+        const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
+        const double2 xp = (k + 1 < LB) ? x[k + 1] : cx(0, 0);
+        r = (xm - xp) * (1.0 / (2.0 * k));
+      }
+      yb[k] = r;
+    }
+    double2* t = x;
+    x = yb;
+    yb = t;
+  }
+  __syncwarp();
+  double2* out = (warp ? go : gv) + p * gp;
+  const int n = warp ? no : nv;
+  for (int r = lane; r < n; r += 32) out[r] = (K + r < LB) ? x[K + r] : cx(0, 0);
+}
+
 }  // namespace
 
 cudaError_t launch_nonfinite(const double2* a, const double2* b, long long n, int* flag,
@@ -214,4 +315,32 @@ cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const dou
   const long long n = g.H * g.Ny;
   k_colloc_finish<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(Xv, Xo, pbc, ov, oo, op, g.Ny, g.H);
   return cudaGetLastError();
+}
+
+cudaError_t launch_colloc_fused(const double2* bv, const double2* bo, long long bp, double2* pbc,
+                                const double* cosk, const double* Ut, const double* ddUt, double2* gv,
+                                double2* go, const WallDims& wd, const DnsGeom& g, const PhysParams& ph,
+                                FftTab<double2> tab, cudaStream_t st) {
+  auto go1 = [&](auto LL) -> cudaError_t {
+    constexpr int L = decltype(LL)::value;
+    if constexpr (WPlan<L, 1, FftMaxRadix<double2>::v>::ok) {
+      if (tab.plan.L != L || g.Ny != L / 2 + 1 || !tab.tw) return cudaErrorNotSupported;
+      constexpr int LB = L / 2 + 9;
+      constexpr int LS = (wlen<double2>(L) > 2 * LB) ? wlen<double2>(L) : 2 * LB;
+      const size_t sm = (size_t)2 * LS * 16;
+      cudaFuncSetAttribute(k_colloc_fused<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_colloc_fused<L><<<(unsigned)g.H, 64, sm, st>>>(bv, bo, bp, pbc, cosk, Ut, ddUt, gv, go, wd.nv, wd.no,
+                                                       wd.gp, g, ph, tab);
+      return cudaGetLastError();
+    }
+    return cudaErrorNotSupported;
+  };
+  switch (tab.plan.L) {
+    case 128: return go1(std::integral_constant<int, 128>());
+    case 256: return go1(std::integral_constant<int, 256>());
+    case 384: return go1(std::integral_constant<int, 384>());
+    case 512: return go1(std::integral_constant<int, 512>());
+    case 768: return go1(std::integral_constant<int, 768>());
+  }
+  return cudaErrorNotSupported;
 }

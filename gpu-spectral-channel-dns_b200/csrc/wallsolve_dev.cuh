@@ -49,6 +49,13 @@ cudaError_t launch_colloc_prep(const double2* bv, const double2* bo, long long b
                                const PhysParams& ph, cudaStream_t st);
 cudaError_t launch_colloc_integrate(const double2* cv, const double2* co, long long cp, double2* gv,
                                     double2* go, const WallDims& wd, const DnsGeom& g, cudaStream_t st);
+// prep, DCT-I and integration in one kernel (warp FFTs over L = 2 (Ny - 1)
+// with the no-padding plan tab); cudaErrorNotSupported, nothing launched,
+// for lengths without a warp plan
+cudaError_t launch_colloc_fused(const double2* bv, const double2* bo, long long bp, double2* pbc,
+                                const double* cosk, const double* Ut, const double* ddUt, double2* gv,
+                                double2* go, const WallDims& wd, const DnsGeom& g, const PhysParams& ph,
+                                FftTab<double2> tab, cudaStream_t st);
 cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
                                  double2* ov, double2* oo, long long op, const DnsGeom& g,
                                  cudaStream_t st);
