@@ -799,6 +799,10 @@ dns_status dns_set_variant(dns_ctx* c, int pass, int v) {
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
+  if (c->variant[pass] != v && c->solve_graph) {  // the solve-only sequence holds the wall solve
+    cudaGraphExecDestroy(c->solve_graph);
+    c->solve_graph = nullptr;
+  }
   c->variant[pass] = v;
   return DNS_OK;
 }

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) k_nonfinite(const double2* __restrict__ a
 // Compile-time L = 2 (Ny - 1); the launcher falls back to the three kernels
 // above for lengths without a warp plan.
 template <int L>
-__global__ void __launch_bounds__(64) k_colloc_fused(const double2* __restrict__ bv, const double2* __restrict__ bo,
+__global__ void __launch_bounds__(64, 16) k_colloc_fused(const double2* __restrict__ bv, const double2* __restrict__ bo,
                                                      long long bp, double2* pbc, const double* __restrict__ cosk,
                                                      const double* __restrict__ Ut, const double* __restrict__ ddUt,
                                                      double2* gv, double2* go, int nv, int no, long long gp,
@@ -224,27 +224,34 @@ __global__ void __launch_bounds__(64) k_colloc_fused(const double2* __restrict__
   double ia, ib;
   wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
   const double kmn = ia * ia + ib * ib, dt = ph.dt, Re = ph.Re;
+  // the operator's constants (the same expressions as the three-kernel path)
+  const double cv2 = 1 + kmn * dt / Re, cv0 = kmn * (1 + kmn * dt * 0.5 / Re), co0 = 1 + kmn * dt * 0.5 / Re;
+  const double ah = ia * dt * 0.5;
   // point value m of the interior right-hand side minus A p (zero where the
-  // equation has no row)
-  auto fval = [&](int m) -> double2 {
+  // equation has no row), staged at line[m] in natural order: the FFT's
+  // first pass reads them all before it writes the line
+  for (int m = lane; m <= N; m += 32) {
     const double y = __ldg(cosk + m);
+    double2 f = cx(0, 0);
     if (zero || warp == 1) {
-      if (m < 1 || m > N - 1) return cx(0, 0);
-      const double2 P0 = pc0 + pc1 * y;
-      if (zero) return b[m + 1] - P0;
-      return b[m + 1] - (P0 * (1 + kmn * dt * 0.5 / Re) + muli(P0 * (ia * dt * 0.5 * __ldg(Ut + m))));
+      if (m >= 1 && m <= N - 1) {
+        const double2 P0 = pc0 + pc1 * y;
+        f = zero ? b[m + 1] - P0 : b[m + 1] - (P0 * co0 + muli(P0 * (ah * __ldg(Ut + m))));
+      }
+    } else if (m >= 2 && m <= N - 2) {
+      const double2 P0 = pc0 + pc1 * y + pc2 * (2 * y * y - 1) + pc3 * (y * (4 * y * y - 3));
+      const double2 P2 = pc2 * 4.0 + pc3 * (24.0 * y);
+      const double U = __ldg(Ut + m), ddU = __ldg(ddUt + m);
+      const double2 re = P2 * cv2 - P0 * cv0;
+      const double2 im = P2 * (ah * U) - P0 * (kmn * ah * U + ah * ddU);
+      f = b[m + 2] - (re + muli(im));
     }
-    if (m < 2 || m > N - 2) return cx(0, 0);
-    const double2 P0 = pc0 + pc1 * y + pc2 * (2 * y * y - 1) + pc3 * (y * (4 * y * y - 3));
-    const double2 P2 = pc2 * 4.0 + pc3 * (24.0 * y);
-    const double U = __ldg(Ut + m), ddU = __ldg(ddUt + m);
-    const double2 re = P2 * (1 + kmn * dt / Re) - P0 * (kmn * (1 + kmn * dt * 0.5 / Re));
-    const double2 im = P2 * (ia * dt * 0.5 * U) - P0 * (kmn * ia * dt * 0.5 * U + ia * dt * 0.5 * ddU);
-    return b[m + 2] - (re + muli(im));
-  };
+    line[m] = f;
+  }
+  __syncwarp();
   // DCT-I: FFT of the even extension; coefficient k = value / N, halved at
   // k = 0 and k = N, written over the line (its last pass read it all)
-  auto ld = [&](int, int n) -> double2 { return fval(n <= N ? n : L - n); };
+  auto ld = [&](int, int n) -> double2 { return line[n <= N ? n : L - n]; };
   auto st = [&](int, int k, double2 v) {
     if (k <= N) line[k] = v * ((k == 0 || k == N) ? 0.5 / N : 1.0 / N);
   };

@@ -82,3 +82,43 @@ def test_reference_program_matches_oracle_and_library(pkg, tmp_path, parity_log)
                       "library vs reference program v %.1e omega %.1e Nv %.1e Nomega %.1e" % (*e_ro, *e_rl))
     assert max(e_ro) < 1e-12, e_ro
     assert max(e_rl) < 1e-11, e_rl
+
+
+def _run_prog(exe, root, params, recovery=None):
+    """Run a reference-layout program (reference or dns_run) in root/run with
+    root/input/parameter.txt; optionally start from a copy of `recovery`."""
+    import shutil
+    (root / "input").mkdir(parents=True, exist_ok=True)
+    (root / "input" / "parameter.txt").write_text(params)
+    d = root / "run"
+    (d / "out").mkdir(parents=True, exist_ok=True)
+    if recovery is not None:
+        shutil.copy(recovery, d / "recovery.dat")
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
+    ok = r.returncode == 0 or (exe == REF_EXE and r.returncode == -6 and
+                               r.stderr.strip() == "terminate called without an active exception")
+    assert ok, (exe, r.returncode, r.stdout[-2000:], r.stderr[-2000:])
+    return d / "recovery.dat"
+
+
+def test_reference_program_restarts_from_library_recovery(pkg, tmp_path, parity_log):
+    """Byte compatibility of the recovery file in the library -> reference
+    direction: the library's driver runs 10 steps and writes recovery.dat;
+    the reference program restarts from that file (start_type 1, its own
+    read_recover_data) and runs to step 15, as does the library's driver; the
+    two files at step 15 (state and AB2 history) agree to the level of the
+    two programs' rounding.  (The other direction, the library reading the
+    reference program's file, is the test above.)"""
+    if not os.path.exists(REF_EXE):
+        pytest.skip("oracle/_ref/ref_program not built (needs the reference's sources)")
+    base = "48 48 128\n4.0 2.0\n1300 0.1 0.005\n"
+    rec10 = _run_prog(DNS_RUN, tmp_path / "lib10", base + "0 0 10 100 10\nout/o\nout/r\n")
+    restart = base + "1 10 15 100 5\nout/o\nout/r\n"
+    rec_ref = _run_prog(REF_EXE, tmp_path / "ref15", restart, rec10)
+    rec_lib = _run_prog(DNS_RUN, tmp_path / "lib15", restart, rec10)
+    ref = _read(pkg, rec_ref)
+    lib = _read(pkg, rec_lib)
+    e = [_rel(lib[i], ref[i]) for i in range(4)]
+    parity_log.append("reference program restarted from the library's recovery file, steps 10..15 at "
+                      "48x48x128, vs the library's own restart: v %.1e omega %.1e Nv %.1e Nomega %.1e" % tuple(e))
+    assert max(e) < 1e-11, e
