@@ -437,6 +437,7 @@ dns_status ctx_create(const dns_params* p, SlabState* slab, dns_ctx** out, int n
     return fail(DNS_ERR_ARG, "unknown precision");
   DnsGeom g = dns_make_geom(p->mx, p->my, p->mz);
   g.nrun = nrun;
+  if ((double)g.H * nrun >= 2147483648.0) return fail(DNS_ERR_ARG, "too many pencils (2^31 or more in one launch)");
   if (g.Nx < 2 || g.Nz < 2 || g.Nx % 2 || g.Nz % 2 || g.Ny < 5)
     return fail(DNS_ERR_ARG, "need even Nx, Nz >= 2 and Ny >= 5");
   if (!fft_len_ok(g.Px) || !fft_len_ok(g.Pz) || !fft_len_ok(p->mz) || !fft_len_ok(p->mz / 2))

@@ -82,11 +82,15 @@ static inline DnsGeom dns_make_geom(int mx, int my, int mz) {
 }
 
 // member, streamwise and spanwise index of pencil p of a wall-normal launch
+// (32-bit arithmetic: a launch covers fewer than 2^31 pencils, checked when
+// the context is created)
 DNS_HD void pencil_modes(const DnsGeom& g, long long p, int& run, int& kx, int& kz) {
-  run = (int)(p / g.Hrun);
-  const long long q = p - (long long)run * g.Hrun;
-  kx = (int)(q % g.Kx);
-  kz = g.kz0 + (int)(q / g.Kx);
+  const unsigned pu = (unsigned)p, hr = (unsigned)g.Hrun, K = (unsigned)g.Kx;
+  const unsigned r = g.nrun > 1 ? pu / hr : 0u;
+  const unsigned q = pu - r * hr;
+  run = (int)r;
+  kx = (int)(q % K);
+  kz = g.kz0 + (int)(q / K);
 }
 
 // ia^2 + ib^2 rounded like the reference's host code (no FMA contraction)
