@@ -13,6 +13,7 @@
 // Pass twiddles come from the table W_L^j (host long double); codelet
 // constants are the exact values cos, sin (2 pi m / R) for R <= 16.
 #pragma once
+#include <type_traits>
 #include "dns_common.cuh"
 
 DNS_HD int fpos(int i) { return i + (i >> 4); }
@@ -177,17 +178,121 @@ DNS_HD void dft4(C& y0, C& y1, C& y2, C& y3) {
   else { y1 = b - id; y3 = b + id; }
 }
 
+// FP32 radix-2, -3 and -4 butterflies on packed pairs: a complex value's
+// (re, im) is one 64-bit register pair, so a complex add or subtract is one
+// add/sub.rn.f32x2 (sm_100) instead of two scalar instructions, b -+ i d is
+// one fma.rn.f32x2 of the swapped d with (+-1, -+1), and radix 3's products
+// with constants are one mul/fma.rn.f32x2 (the same roundings as the scalar
+// form: the results equal it bit for bit).  Host code takes the scalar form.
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ unsigned long long f2u(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 u2f(unsigned long long u) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(u));
+  return r;
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+// (y.im, y.re)
+__device__ __forceinline__ unsigned long long swap2(unsigned long long a) {
+  unsigned long long r;
+  asm("{\n\t.reg .b32 lo, hi;\n\tmov.b64 {lo, hi}, %1;\n\tmov.b64 %0, {hi, lo};\n\t}" : "=l"(r) : "l"(a));
+  return r;
+}
+template <bool INV>
+__device__ __forceinline__ void dft2_f32x2(float2& a, float2& b) {
+  const unsigned long long ua = f2u(a), ub = f2u(b);
+  a = u2f(add2(ua, ub));
+  b = u2f(sub2(ua, ub));
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long pair2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+template <bool INV>
+__device__ __forceinline__ void dft3_f32x2(float2& y0, float2& y1, float2& y2) {
+  const float c3 = -0.5f, s3 = 0.86602540378443864676372317075294f;
+  const unsigned long long u0 = f2u(y0), u1 = f2u(y1), u2 = f2u(y2);
+  const unsigned long long t1 = add2(u1, u2), t2 = sub2(u1, u2);
+  const unsigned long long base = fma2(t1, pair2(c3, c3), u0);
+  const unsigned long long its = mul2(swap2(t2), pair2(-s3, s3));  // i t2 s3
+  y0 = u2f(add2(u0, t1));
+  if (INV) { y1 = u2f(add2(base, its)); y2 = u2f(sub2(base, its)); }
+  else { y1 = u2f(sub2(base, its)); y2 = u2f(add2(base, its)); }
+}
+template <bool INV>
+__device__ __forceinline__ void dft4_f32x2(float2& y0, float2& y1, float2& y2, float2& y3) {
+  const unsigned long long u0 = f2u(y0), u1 = f2u(y1), u2 = f2u(y2), u3 = f2u(y3);
+  const unsigned long long a = add2(u0, u2), b = sub2(u0, u2), c = add2(u1, u3), d = sub2(u1, u3);
+  const unsigned long long ds = swap2(d);
+  // (1, -1) and (-1, 1) as f32x2 bit patterns (low word = re)
+  const unsigned long long pm = 0xBF8000003F800000ull, mp = 0x3F800000BF800000ull;
+  y0 = u2f(add2(a, c));
+  y2 = u2f(sub2(a, c));
+  // forward: y1 = b - i d = (b.re + d.im, b.im - d.re), y3 = b + i d
+  y1 = u2f(fma2(ds, INV ? mp : pm, b));
+  y3 = u2f(fma2(ds, INV ? pm : mp, b));
+}
+#endif
+
 // Generic R = R1 * R2 codelet: x[r2 + R2 r1] -> X[k1 + R1 k2]
 template <int R, bool INV, typename C> struct Codelet;
 
 template <bool INV, typename C> struct Codelet<2, INV, C> {
-  DNS_HD static void run(C* v) { dft2<INV>(v[0], v[1]); }
+  DNS_HD static void run(C* v) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (std::is_same<C, float2>::value) {
+      dft2_f32x2<INV>(v[0], v[1]);
+      return;
+    }
+#endif
+    dft2<INV>(v[0], v[1]);
+  }
 };
 template <bool INV, typename C> struct Codelet<3, INV, C> {
-  DNS_HD static void run(C* v) { dft3<INV>(v[0], v[1], v[2]); }
+  DNS_HD static void run(C* v) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (std::is_same<C, float2>::value) {
+      dft3_f32x2<INV>(v[0], v[1], v[2]);
+      return;
+    }
+#endif
+    dft3<INV>(v[0], v[1], v[2]);
+  }
 };
 template <bool INV, typename C> struct Codelet<4, INV, C> {
-  DNS_HD static void run(C* v) { dft4<INV>(v[0], v[1], v[2], v[3]); }
+  DNS_HD static void run(C* v) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (std::is_same<C, float2>::value) {
+      dft4_f32x2<INV>(v[0], v[1], v[2], v[3]);
+      return;
+    }
+#endif
+    dft4<INV>(v[0], v[1], v[2], v[3]);
+  }
 };
 
 template <int R1, int R2, int R, bool INV, typename C>
