@@ -626,6 +626,31 @@ __device__ __forceinline__ double2 umul_gl(const double2* X, int k, int N, const
   if (k == N - 1 || k == N - 2) r = r + u(2 * N - k);
   return r;
 }
+// the same for X given element-wise by a functor (X(j) for 0 <= j <= N):
+// one interpolant of a combination in place of a combination of interpolants
+template <class F>
+__device__ __forceinline__ double2 umul_fn(F X, int k, int N, const PhysParams& ph) {
+  const double2 z = make_double2(0.0, 0.0);
+  auto xm = [&](int j) { return (j >= 0 && j <= N) ? X(j) : z; };
+  auto ym = [&](int j) {
+    if (j < 0) return z;
+    if (j == 0) return xm(1) * 0.5;
+    return (xm(j - 1) * (j == 1 ? 2.0 : 1.0) + xm(j + 1)) * 0.5;
+  };
+  auto u = [&](int j) {
+    double2 r = xm(j) * ph.U0 + ym(j) * ph.U1;
+    if (ph.U2 != 0.0) {
+      const double2 y2 = (j < 0) ? z
+                         : (j == 0) ? ym(1) * 0.5
+                                    : (ym(j - 1) * (j == 1 ? 2.0 : 1.0) + ym(j + 1)) * 0.5;
+      r = r + y2 * ph.U2;
+    }
+    return r;
+  };
+  double2 r = u(k);
+  if (k == N - 1 || k == N - 2) r = r + u(2 * N - k);
+  return r;
+}
 // ... of U'(y) X(y)
 __device__ __forceinline__ double2 upmul_gl(const double2* X, int k, int N, const PhysParams& ph) {
   auto u = [&](int j) { return cget(X, j, N) * ph.U1 + ymul(X, j, N) * (2.0 * ph.U2); };
@@ -943,6 +968,8 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
   const double dt = run_dt(ph, run), Re = run_Re(ph, run), gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
+  // the CN operators' coefficients, one division per CTA
+  const double h = dt * 0.5 / Re, c2v = 1 - 2.0 * kmn * h, c0v = kmn * (1 - kmn * h), c0o = 1 - kmn * h;
   double2* fv = lx;
   double2* fo = ly;
   for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
@@ -959,15 +986,15 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
     if (boot) continue;
     double2 a, b;
     if (zero) {
-      a = Vc[k] + D2V[k] * (dt * 0.5 / Re) - (hv * 1.5 - nvc[k] * 0.5) * dt;
-      b = Oc[k] + D2O[k] * (dt * 0.5 / Re) - (ho * 1.5 - noc[k] * 0.5) * dt;
+      a = Vc[k] + D2V[k] * h - (hv * 1.5 - nvc[k] * 0.5) * dt;
+      b = Oc[k] + D2O[k] * h - (ho * 1.5 - noc[k] * 0.5) * dt;
     } else {
-      const double2 re = D4V[k] * (dt * 0.5 / Re) + D2V[k] * (1 - kmn * dt / Re)
-                         - Vc[k] * (kmn * (1 - kmn * dt * 0.5 / Re));
-      const double2 im = umul_gl(D2V, k, N, ph) * (-gam) + umul_gl(Vc, k, N, ph) * (kmn * gam)
+      const double2 re = D4V[k] * h + D2V[k] * c2v - Vc[k] * c0v;
+      // U (-gam D^2 v + k^2 gam v) as one interpolant
+      const double2 im = umul_fn([&](int j) { return D2V[j] * (-gam) + Vc[j] * (kmn * gam); }, k, N, ph)
                          + Vc[k] * (gam * 2.0 * ph.U2);
       a = re + muli(im) + (hv * 1.5 - nvc[k] * 0.5) * dt;
-      const double2 ro = D2O[k] * (0.5 / Re * dt) + Oc[k] * (1 - kmn * dt * 0.5 / Re);
+      const double2 ro = D2O[k] * h + Oc[k] * c0o;
       b = ro + muli(umul_gl(Oc, k, N, ph) * (-gam)) + (ho * 1.5 - noc[k] * 0.5) * dt
           + muli(upmul_gl(Vc, k, N, ph) * kap);
     }
