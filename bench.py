@@ -422,7 +422,10 @@ def run_ensemble(args):
     per pass for all 12), the four batches stepped concurrently
     (dns_step_many); beside it the same runs as 48 separate contexts, all
     concurrent (one stream each) and one after another.  Per-run error of the
-    batched runs against each run's own FP64 result after the same steps."""
+    batched runs against each run's own FP64 result after min(K, 20) steps:
+    at dt 0.002 the 128x97x128 runs pass the explicit term's stability limit
+    (their FP64 runs overflow between steps 80 and 200, finite at dt 0.001),
+    and the mixed form, seeded by FP32 rounding, diverges earlier."""
     import numpy as np
     import torch
     pkg = load_pkg()
@@ -444,8 +447,9 @@ def run_ensemble(args):
         b.set_state(np.stack([states[m][0] for m in grp]), np.stack([states[m][1] for m in grp]))
         b.bootstrap()
         batches.append(b)
-    # accuracy: K steps of every run, batched mixed vs its own FP64 run alone
-    pkg.step_many(batches, K)
+    # accuracy: KE steps of every run, batched mixed vs its own FP64 run alone
+    KE = min(K, 20)
+    pkg.step_many(batches, KE)
     err = {}
     for grp, b in zip(groups, batches):
         b.synchronize()
@@ -455,7 +459,7 @@ def run_ensemble(args):
             f = pkg.Context(params(c, pkg.PREC_FP64))
             f.set_state(*states[m])
             f.bootstrap()
-            f.step(K)
+            f.step(KE)
             f.synchronize()
             Vf, Of = f.get_state()
             f.close()
@@ -518,6 +522,7 @@ def run_ensemble(args):
         "separate_contexts_concurrent": {"value": rate(ms_conc), "ms": round(ms_conc, 3)},
         "one_after_another": {"value": rate(ms_seq), "ms": round(ms_seq, 3)},
         "max_rel_l2_err_vs_own_fp64_run": {k: float("%.3g" % v) for k, v in err.items()},
+        "err_after_steps": KE,
         "clocks": clk.summary(),
         "timing": "CUDA events: one before the first launch, one at the end of each context's stream; max",
         "data": "synthetic seeded divergence-free fields (seeds 1000..1047, amplitude 0.1)",
@@ -616,7 +621,7 @@ def other_workloads(args):
             ("ensemble_48_runs", run_ensemble, 10, ("metric", "value", "unit", "steps", "ms_all_runs_K_steps",
                                                     "batches", "separate_contexts_concurrent",
                                                     "one_after_another", "max_rel_l2_err_vs_own_fp64_run",
-                                                    "clocks"))):
+                                                    "err_after_steps", "clocks"))):
         a = copy.copy(args)
         a.steps, a.warmup, a.solve_grid = steps, 3, "576,576,768"
         try:

@@ -5,9 +5,10 @@
 // of the previous radices, butterfly j in [0, L/R) reads x[j + r L/R],
 // applies W_{Ns R}^{r (j mod Ns)}, takes the R-point DFT in registers and
 // writes y[(j/Ns) Ns R + (j mod Ns) + r Ns].  The NL L / R butterflies of a
-// pass are spread evenly over the 32 lanes (every radix of a plan divides
-// NL L / 32), a lane loads all its inputs before the warp synchronises and
-// writes, so the transform runs in place.
+// pass are dealt to the 32 lanes in rounds of 32 (where NL L / R is not a
+// multiple of 32 the last round leaves lanes idle); a lane loads all its
+// inputs before the warp synchronises and writes, so the transform runs in
+// place.
 //
 // Layout: element i of a line sits at wsw(i) = i + i / 2^S, one padding
 // slot after every 2^S elements (2^S x the element size = 128 bytes), which
@@ -38,8 +39,8 @@ template <typename C> DNS_HD constexpr int wsw(int i) { return i + (i >> WSwz<C>
 // line length covering positions wsw(0..L-1)
 template <typename C> DNS_HD constexpr int wlen(int L) { return L + (L >> WSwz<C>::S); }
 
-// plans: radices (up to 48 FP32, 8 FP64 for register pressure), each
-// dividing NL L / 32
+// plans: radices (up to 48 FP32, 8 FP64 for register pressure); a radix
+// that divides NL L / 32 keeps every lane busy in every round
 template <int L, int NL, int MAXR> struct WPlan { enum { ok = 0 }; };
 #define WPLAN(L, NL, MAXR, ...) \
   template <> struct WPlan<L, NL, MAXR> { enum { ok = 1 }; typedef Radices<__VA_ARGS__> R; };
@@ -58,6 +59,17 @@ WPLAN(768, 2, 16, 16, 48)
 WPLAN(384, 3, 16, 12, 4, 4, 2)
 WPLAN(384, 4, 16, 16, 24)
 WPLAN(192, 4, 16, 8, 24)
+WPLAN(192, 1, 16, 8, 8, 3)
+// the ensemble grids' streamwise and spanwise lengths (ragged rounds)
+WPLAN(48, 1, 16, 6, 8)
+WPLAN(48, 2, 16, 6, 8)
+WPLAN(48, 4, 16, 6, 8)
+WPLAN(96, 1, 16, 12, 8)
+WPLAN(96, 2, 16, 12, 8)
+WPLAN(96, 4, 16, 12, 8)
+WPLAN(144, 1, 16, 12, 12)
+WPLAN(144, 2, 16, 12, 12)
+WPLAN(144, 4, 16, 12, 12)
 // FP64
 WPLAN(128, 1, 8, 4, 4, 4, 2)
 WPLAN(256, 1, 8, 8, 8, 4)
@@ -73,6 +85,16 @@ WPLAN(768, 2, 8, 8, 8, 4, 3)
 WPLAN(384, 3, 8, 6, 4, 4, 4)
 WPLAN(384, 4, 8, 8, 8, 6)
 WPLAN(192, 4, 8, 8, 4, 6)
+WPLAN(192, 1, 8, 8, 8, 3)
+WPLAN(48, 1, 8, 6, 8)
+WPLAN(48, 2, 8, 6, 8)
+WPLAN(48, 4, 8, 6, 8)
+WPLAN(96, 1, 8, 4, 4, 6)
+WPLAN(96, 2, 8, 4, 4, 6)
+WPLAN(96, 4, 8, 4, 4, 6)
+WPLAN(144, 1, 8, 4, 6, 6)
+WPLAN(144, 2, 8, 4, 6, 6)
+WPLAN(144, 4, 8, 4, 6, 6)
 #undef WPLAN
 
 // One pass, split into the load (inputs of the lane's butterfly q, twiddled,
@@ -114,9 +136,12 @@ template <int... Rs> constexpr int wtw_size(Radices<Rs...>) {
 
 template <typename C, int L, int NL, bool INV, int R, int Ns>
 struct WPass {
-  static constexpr int NB = L / R;        // butterflies per line
-  static constexpr int B = NL * NB / 32;  // butterflies per lane
-  static_assert((NL * NB) % 32 == 0, "radix does not divide the lane share");
+  static constexpr int NB = L / R;           // butterflies per line
+  static constexpr int NT = NL * NB;         // butterflies of the pass
+  static constexpr int B = (NT + 31) / 32;   // rounds: butterfly lane + 32 q in round q
+  static_assert(L % R == 0, "radix does not divide the length");
+  // lanes past the last butterfly idle in the last round
+  DNS_HD static bool on(int lane, int q) { return NT % 32 == 0 || lane + 32 * q < NT; }
   static constexpr int S = WSwz<C>::S, M = (1 << S) - 1;
   // loads i = j + r NB: no carry for any j when NB is a multiple of 2^S
   static constexpr bool LIN_LD = (NB & M) == 0;
@@ -233,6 +258,9 @@ template <typename C, int L, int NL> int wtw_table(std::vector<C>& out) {
 // runtime length: the lengths that have warp plans
 template <typename C, int NL> int wtw_table_any(int L, std::vector<C>& out) {
   switch (L) {
+    case 48: return wtw_table<C, 48, NL>(out);
+    case 96: return wtw_table<C, 96, NL>(out);
+    case 144: return wtw_table<C, 144, NL>(out);
     case 128: return wtw_table<C, 128, NL>(out);
     case 192: return wtw_table<C, 192, NL>(out);
     case 256: return wtw_table<C, 256, NL>(out);
@@ -249,10 +277,12 @@ __device__ __forceinline__ void wfft_pass(C* buf, int ls, const C* __restrict__ 
   typedef WPass<C, L, NL, INV, R, Ns> P;
   C v[P::B][R];
 #pragma unroll
-  for (int q = 0; q < P::B; ++q) P::load(buf, ls, tw, lane, q, v[q]);
+  for (int q = 0; q < P::B; ++q)
+    if (P::on(lane, q)) P::load(buf, ls, tw, lane, q, v[q]);
   __syncwarp();
 #pragma unroll
-  for (int q = 0; q < P::B; ++q) P::store(buf, ls, lane, q, v[q]);
+  for (int q = 0; q < P::B; ++q)
+    if (P::on(lane, q)) P::store(buf, ls, lane, q, v[q]);
   __syncwarp();
 }
 
@@ -289,12 +319,14 @@ struct WRunIO {
     C v[P::B][R];
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
+      if (!P::on(lane, q)) continue;
       if constexpr (FIRST) P::template load_fn<LD>(ld, lane, q, v[q]);
       else P::load(buf, ls, tw, lane, q, v[q]);
     }
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < P::B; ++q) {
+      if (!P::on(lane, q)) continue;
       if constexpr (LAST) P::template store_fn<ST>(st, lane, q, v[q]);
       else P::store(buf, ls, lane, q, v[q]);
     }

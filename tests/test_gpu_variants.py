@@ -4,9 +4,11 @@ the block shapes of the banded solve) gives the step of the
 default variants: in FP64 to 1e-12 relative (the parity bar; measured
 differences are rounding, ~1e-15), in the mixed form to 1e-6 against the
 FP64 step.  384x384x128 (256x33x256 modes): lengths with warp plans in both
-precisions (Px = Pz = 384, M = 128), so every variant is available, and
-192x192x128 (its streamwise warp form); 3 steps after
-the bootstrap from the seeded state, Re 1300, Ro 0.1, dt 0.005."""
+precisions (Px = Pz = 384, M = 128), so every variant is available,
+192x192x128 (its streamwise warp form), and the ensemble grids 48x48x128,
+96x96x192 and 144x144x256 (warp plans whose passes leave lanes idle in
+their last round); 3 steps after the bootstrap from the seeded state,
+Re 1300, Ro 0.1, dt 0.005."""
 import numpy as np
 import pytest
 
@@ -70,7 +72,20 @@ def test_available_variants(pkg):
     assert amx[pkg.PASS_Y3] == [pkg.Y3_FFT, pkg.Y3_BLOCK]  # the tensor form needs Ny = 129
 
 
-@pytest.mark.parametrize("grid", [GRID, (192, 192, 128)])
+ENSEMBLE_GRIDS = [(48, 48, 128), (96, 96, 192), (144, 144, 256)]
+
+
+@pytest.mark.parametrize("grid", ENSEMBLE_GRIDS)
+def test_ensemble_grids_have_warp_forms(pkg, grid):
+    for prec in (pkg.PREC_FP64, pkg.PREC_MIXED):
+        a = _available(pkg, prec, grid)
+        assert a[pkg.PASS_X] == [pkg.X_WARP3, pkg.X_WARP6, pkg.X_BLOCK], (grid, prec)
+        assert pkg.Z_WARP in a[pkg.PASS_ZB] and pkg.Z_WARP in a[pkg.PASS_ZF], (grid, prec)
+        assert a[pkg.PASS_Y1] == [pkg.Y1_WARP, pkg.Y1_BLOCK], (grid, prec)
+        assert a[pkg.PASS_Y3][0] == pkg.Y3_FFT, (grid, prec)
+
+
+@pytest.mark.parametrize("grid", [GRID, (192, 192, 128)] + ENSEMBLE_GRIDS)
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_every_variant_same_step(pkg, prec, grid, parity_log):
     P = pkg.PREC_FP64 if prec == "fp64" else pkg.PREC_MIXED
