@@ -836,36 +836,35 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
     if ((st = dns_set_variant(c, DNS_PASS_Y3, keep)) != DNS_OK) return st;
   }
   // Every candidate is timed inside whole steps (its inputs as the step
-  // leaves them, its neighbours running): round r runs variant r of every
-  // pass that has one (the current variant elsewhere), one warm-up step and
-  // three timed steps with events around each kernel.  The state and the
-  // AB2 history are saved first and put back after.
+  // leaves them, its neighbours running), one pass at a time: pass p's
+  // variants run with every other pass at its best so far (the context's
+  // variant for the passes not yet tuned), one warm-up step and three timed
+  // steps with events around each kernel; p then keeps its fastest.  The
+  // state and the AB2 history are saved first and put back after.
   const size_t hn = (size_t)c->g.H * c->g.nrun * c->g.Ny;
   double2* save = nullptr;
   CK(cudaMalloc(&save, 4 * hn * 16));
   double2* const bufs[4] = {c->V, c->O, c->Nvp, c->Nop};
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < 4 && !e; ++i) e = cudaMemcpyAsync(save + i * hn, bufs[i], hn * 16, cudaMemcpyDeviceToDevice, c->st);
-  int keep[DNS_NUM_PASSES];
-  for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = c->variant[p];
+  int keep[DNS_NUM_PASSES], best[DNS_NUM_PASSES];
+  for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = best[p] = c->variant[p];
   // kernel slot of each pass in a step's events
   static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3, 5, 2};
   const int ne = DNS_NUM_KERNELS + 1, nt = 3;
   std::vector<cudaEvent_t> ev((size_t)ne * (nt + 1));
   for (auto& x : ev)
     if (!e) e = cudaEventCreate(&x);
-  for (int r = 0; r < DNS_MAX_VARIANTS && !e && st == DNS_OK; ++r) {
-    bool any = false;
-    for (int p = 0; p < DNS_NUM_PASSES; ++p) {
-      c->variant[p] = avail[p][r] ? r : keep[p];
-      any = any || avail[p][r];
-    }
-    if (!any) continue;
-    for (int i = 0; i <= nt && !e; ++i) e = enqueue(c, 0, &ev[(size_t)i * ne]);
-    if (!e) e = cudaStreamSynchronize(c->st);
-    if (!e) st = check_status(c);
-    for (int p = 0; p < DNS_NUM_PASSES && !e && st == DNS_OK; ++p) {
+  for (int p = 0; p < DNS_NUM_PASSES && !e && st == DNS_OK; ++p) {
+    double bt = 1e300;
+    for (int r = 0; r < DNS_MAX_VARIANTS && !e && st == DNS_OK; ++r) {
       if (!avail[p][r]) continue;
+      for (int q = 0; q < DNS_NUM_PASSES; ++q) c->variant[q] = best[q];
+      c->variant[p] = r;
+      for (int i = 0; i <= nt && !e; ++i) e = enqueue(c, 0, &ev[(size_t)i * ne]);
+      if (!e) e = cudaStreamSynchronize(c->st);
+      if (!e) st = check_status(c);
+      if (e || st != DNS_OK) break;
       double sum = 0.0;
       for (int i = 1; i <= nt; ++i) {
         float x = 0.f;
@@ -873,6 +872,10 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
         sum += x;
       }
       t[p * DNS_MAX_VARIANTS + r] = sum / nt;
+      if (sum / nt < bt) {
+        bt = sum / nt;
+        best[p] = r;
+      }
     }
   }
   for (auto& x : ev)
@@ -887,15 +890,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   for (int p = 0; p < DNS_NUM_PASSES; ++p) c->variant[p] = keep[p];
   if (e) return fail(DNS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
   if (st != DNS_OK) return st;
-  for (int p = 0; p < DNS_NUM_PASSES && st == DNS_OK; ++p) {
-    int pick = keep[p];
-    double best = 1e300;
-    for (int v = 0; v < DNS_MAX_VARIANTS; ++v) {
-      const double x = t[p * DNS_MAX_VARIANTS + v];
-      if (x >= 0 && x < best) { best = x; pick = v; }
-    }
-    st = dns_set_variant(c, p, pick);
-  }
+  for (int p = 0; p < DNS_NUM_PASSES && st == DNS_OK; ++p) st = dns_set_variant(c, p, best[p]);
   if (ms)
     for (int i = 0; i < DNS_NUM_PASSES * DNS_MAX_VARIANTS; ++i) ms[i] = t[i];
   return st;

@@ -108,3 +108,6 @@ DNS_HD void wavenumbers(int kx, int kz, int Nz, double aphi, double beta,
   ia = (double)kx / aphi;
   ib = (kz >= Nz / 2 + 1) ? (double)(kz - Nz) / beta : (double)kz / beta;
 }
+
+// a complex value of element type E (float2 / double2) as C
+template <typename C, typename E> DNS_HD C from_e(E a) { return cmk<C>(a.x, a.y); }

@@ -103,10 +103,9 @@ __device__ __forceinline__ uint32_t b_off(int n, int kc) {
 __device__ __forceinline__ uint32_t tf32_bits(uint32_t u) { return (u + 0x1000u) & ~0x1FFFu; }
 
 // x = hi + lo to FP32 rounding (~2^-24 |x| beyond the 2^-22 of the TF32 pair)
-__device__ __forceinline__ void split_f(double x, uint32_t& hi, uint32_t& lo) {
-  const float xf = (float)x;
-  hi = tf32_bits(__float_as_uint(xf));
-  lo = tf32_bits(__float_as_uint(xf - __uint_as_float(hi)));
+__device__ __forceinline__ void split_f(float x, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_bits(__float_as_uint(x));
+  lo = tf32_bits(__float_as_uint(x - __uint_as_float(hi)));
 }
 
 __device__ __forceinline__ float2 cmul_i(float2 a, float s) { return make_float2(-a.y * s, a.x * s); }  // i s a
@@ -266,25 +265,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const bool ok = t * TC_NP + j < H;
       // backward sweep k = 127 .. 0: b_k = b_k+2 + 2(k+1) a_k+1 (D),
       // c_k = c_k+2 + 2(k+1) b_k+1 (D^2), b_0 and c_0 halved; the centre
-      // values sum_k x_k T_k(0) on the way
-      const double a128 = ok ? src[2 * 128] : 0.0;
-      double a_next = a128;
-      double b1 = 0.0, b2 = 0.0, c1 = 0.0, c2 = 0.0;
-      double z0 = a128, z1 = 0.0, z2 = 0.0;  // T_128(0) = 1
+      // values sum_k x_k T_k(0) on the way.  In FP32: the products are
+      // FP32-accurate (3xTF32) and feed FP32 transforms only.
+      const float a128 = ok ? (float)src[2 * 128] : 0.f;
+      float a_next = a128;
+      float b1 = 0.f, b2 = 0.f, c1 = 0.f, c2 = 0.f;
+      float z0 = a128, z1 = 0.f, z2 = 0.f;  // T_128(0) = 1
       for (int kc = TC_KP / 4 - 1; kc >= 0; --kc) {
         uint32_t h[3][2][4], l[3][2][4];  // [vector][parity][slot]
 #pragma unroll
         for (int i = 7; i >= 0; --i) {
           const int k = 8 * kc + i;
-          const double ak = ok ? src[2 * k] : 0.0;
-          double bk = b2 + 2.0 * (k + 1) * a_next;
-          double ck = c2 + 2.0 * (k + 1) * b1;
+          const float ak = ok ? (float)src[2 * k] : 0.f;
+          const float f = (float)(2 * (k + 1));
+          float bk = b2 + f * a_next;
+          float ck = c2 + f * b1;
           if (k == 0) {
-            bk *= 0.5;
-            ck *= 0.5;
+            bk *= 0.5f;
+            ck *= 0.5f;
           }
           if (!(i & 1)) {  // T_k(0) = (-1)^(k/2) for even k, 0 for odd k
-            const double w = (i & 2) ? -1.0 : 1.0;
+            const float w = (i & 2) ? -1.f : 1.f;
             z0 += w * ak;
             z1 += w * bk;
             z2 += w * ck;
@@ -315,10 +316,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       // side data of this tile (slot it % 4)
       Side& sd = side[it & (TC_NSIDE - 1)];
-      sd.a128[j][fld][r] = (float)a128;
-      sd.centre[j * 10 + q0 * 2 + r] = (float)z0;
-      sd.centre[j * 10 + (q0 + 1) * 2 + r] = (float)z1;
-      if (!fld) sd.centre[j * 10 + 4 + r] = (float)z2;
+      sd.a128[j][fld][r] = a128;
+      sd.centre[j * 10 + q0 * 2 + r] = z0;
+      sd.centre[j * 10 + (q0 + 1) * 2 + r] = z1;
+      if (!fld) sd.centre[j * 10 + 4 + r] = z2;
       // the staging buffer is free: fetch this warp's next tile under the
       // other producer's and the epilogue's work
       fence_proxy_async();

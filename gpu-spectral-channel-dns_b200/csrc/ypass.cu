@@ -74,40 +74,43 @@ __device__ __noinline__ void ddz_warp(const double2* a, double2* b, int N) {
 // The same derivative with CH (even) coefficients per lane: every lane's
 // run starts at an even index, so the parity of each of its elements is
 // known at compile time (the sums split by parity without divergent
-// branches), and the run stays in registers between the two sweeps.
-template <int CH>
-__device__ __noinline__ void ddz_fast(const double2* __restrict__ a, double2* __restrict__ b, int N) {
+// branches), and the run stays in registers between the two sweeps.  E is
+// the element type: double2, or float2 where the result feeds FP32
+// transforms only.
+template <int CH, typename E = double2>
+__device__ __noinline__ void ddz_fast(const E* __restrict__ a, E* __restrict__ b, int N) {
   static_assert(CH % 2 == 0, "runs of even length");
+  typedef T_of<E> S;
   const int lane = threadIdx.x & 31;
   const int j0 = lane * CH;
-  double2 v[CH];
+  E v[CH];
 #pragma unroll
-  for (int i = 0; i < CH; ++i) v[i] = (j0 + i < N) ? a[j0 + i] : make_double2(0.0, 0.0);
-  double2 te = make_double2(0.0, 0.0), to = te;  // this run's sums of 2 j a_j, even / odd j
+  for (int i = 0; i < CH; ++i) v[i] = (j0 + i < N) ? a[j0 + i] : cmk<E>(0.0, 0.0);
+  E te = cmk<E>(0.0, 0.0), to = te;  // this run's sums of 2 j a_j, even / odd j
 #pragma unroll
   for (int i = 0; i < CH; ++i) {
-    const double f = 2.0 * (j0 + i);
+    const S f = (S)(2 * (j0 + i));
     if (i & 1) to = to + v[i] * f;
     else te = te + v[i] * f;
   }
-  double s0 = te.x, s1 = te.y, s2 = to.x, s3 = to.y;
+  S s0 = te.x, s1 = te.y, s2 = to.x, s3 = to.y;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
-    const double t0 = __shfl_down_sync(0xffffffffu, s0, d);
-    const double t1 = __shfl_down_sync(0xffffffffu, s1, d);
-    const double t2 = __shfl_down_sync(0xffffffffu, s2, d);
-    const double t3 = __shfl_down_sync(0xffffffffu, s3, d);
+    const S t0 = __shfl_down_sync(0xffffffffu, s0, d);
+    const S t1 = __shfl_down_sync(0xffffffffu, s1, d);
+    const S t2 = __shfl_down_sync(0xffffffffu, s2, d);
+    const S t3 = __shfl_down_sync(0xffffffffu, s3, d);
     if (lane + d < 32) { s0 += t0; s1 += t1; s2 += t2; s3 += t3; }
   }
   // sums over the runs of the lanes above, then down this run
-  double2 re = make_double2(s0 - te.x, s1 - te.y), ro = make_double2(s2 - to.x, s3 - to.y);
+  E re = cmk<E>(s0 - te.x, s1 - te.y), ro = cmk<E>(s2 - to.x, s3 - to.y);
 #pragma unroll
   for (int i = CH - 1; i >= 0; --i) {
     const int j = j0 + i;
-    double2 out = (i & 1) ? re : ro;  // j' > j of the other parity
-    if (j == 0) out = out * 0.5;
+    E out = (i & 1) ? re : ro;  // j' > j of the other parity
+    if (j == 0) out = out * (S)0.5;
     if (j < N) b[j] = out;
-    const double f = 2.0 * j;
+    const S f = (S)(2 * j);
     if (i & 1) ro = ro + v[i] * f;
     else re = re + v[i] * f;
   }
@@ -514,40 +517,62 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   // linearity, u = i(ia Dw - ib oz)/k^2, v = i(ib Dw + ia oz)/k^2 and their
   // derivatives from D^2 w, D oz (source/velocity.cu:90-170).  The mean
   // mode holds u0, w0 in (w, oz): u = w, v = oz, omega_x = D oz, omega_y = -D w.
+  // The FP32 form takes the state to FP32 first and forms the velocities
+  // and vorticities in FP32: they feed FP32 transforms only.
+  typedef typename std::conditional<sizeof(C) == 8, float2, double2>::type E;
+  typedef T_of<E> S;
+  E *ew = (E*)w, *eDw = (E*)Dw, *eD2w = (E*)D2w, *eoz = (E*)oz, *eDoz = (E*)Doz;
+  if constexpr (sizeof(C) == 8) {
+    // in place: element n of the FP32 copy lies below element n of the
+    // FP64 vector, so the conversion runs in one pass per warp
+    const int warp0 = threadIdx.x >> 5, lane0 = threadIdx.x & 31;
+    if (warp0 < 2) {
+      const double2* src = warp0 ? oz : w;
+      E* dst = warp0 ? eoz : ew;
+      for (int n0 = 0; n0 < Ny; n0 += 32) {
+        const int n = n0 + lane0;
+        const double2 x = n < Ny ? src[n] : make_double2(0.0, 0.0);
+        __syncwarp();
+        if (n < Ny) dst[n] = make_float2((float)x.x, (float)x.y);
+      }
+    }
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5;
   constexpr int CH = ddz_run(Ny);
   if (warp == 0) {
-    ddz_fast<CH>(w, Dw, Ny);
+    ddz_fast<CH, E>(ew, eDw, Ny);
     __syncwarp();
-    if (!zero) ddz_fast<CH>(Dw, D2w, Ny);
+    if (!zero) ddz_fast<CH, E>(eDw, eD2w, Ny);
   } else if (warp == 1) {
-    ddz_fast<CH>(oz, Doz, Ny);
+    ddz_fast<CH, E>(eoz, eDoz, Ny);
   }
   __syncthreads();
+  const S sia = (S)(ia * kmn1), sib = (S)(ib * kmn1), fia = (S)ia, fib = (S)ib;
   for (int n = threadIdx.x; n < Ny; n += blockDim.x) {
-    const double2 wn = w[n], on = oz[n], d1 = Dw[n], dz = Doz[n];
-    double2 u, v, ox, oy;
+    const E wn = ew[n], on = eoz[n], d1 = eDw[n], dz = eDoz[n];
+    E u, v, ox, oy;
     if (zero) {
       u = wn;
       v = on;
       ox = dz;
-      oy = make_double2(-d1.x, -d1.y);
+      oy = cmk<E>(-d1.x, -d1.y);
     } else {
-      const double2 d2 = D2w[n];
-      u = muli(d1 * (ia * kmn1)) - muli(on * (ib * kmn1));
-      v = muli(d1 * (ib * kmn1)) + muli(on * (ia * kmn1));
-      const double2 du = muli(d2 * (ia * kmn1)) - muli(dz * (ib * kmn1));
-      const double2 dv = muli(d2 * (ib * kmn1)) + muli(dz * (ia * kmn1));
-      ox = dv - muli(wn * ib);
-      oy = muli(wn * ia) - du;
+      const E d2 = eD2w[n];
+      u = muli(d1 * sia) - muli(on * sib);
+      v = muli(d1 * sib) + muli(on * sia);
+      const E du = muli(d2 * sia) - muli(dz * sib);
+      const E dv = muli(d2 * sib) + muli(dz * sia);
+      ox = dv - muli(wn * fib);
+      oy = muli(wn * fia) - du;
     }
-    const double h = n ? 0.5 : 1.0;  // even extension: c_0, then c_n / 2
-    fu[n] = from_d2<C>(u * h);
-    fv[n] = from_d2<C>(v * h);
-    fw[n] = from_d2<C>(wn * h);
-    fox[n] = from_d2<C>(ox * h);
-    foy[n] = from_d2<C>(oy * h);
-    foz[n] = from_d2<C>(on * h);
+    const S h = n ? (S)0.5 : (S)1.0;  // even extension: c_0, then c_n / 2
+    fu[n] = from_e<C>(u * h);
+    fv[n] = from_e<C>(v * h);
+    fw[n] = from_e<C>(wn * h);
+    fox[n] = from_e<C>(ox * h);
+    foy[n] = from_e<C>(oy * h);
+    foz[n] = from_e<C>(on * h);
   }
   __syncthreads();
   // this warp's two lines: fields 2 warp, 2 warp + 1; the first FFT pass
