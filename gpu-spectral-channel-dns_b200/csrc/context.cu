@@ -838,7 +838,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   // Every candidate is timed inside whole steps (its inputs as the step
   // leaves them, its neighbours running), one pass at a time: pass p's
   // variants run with every other pass at its best so far (the context's
-  // variant for the passes not yet tuned), one warm-up step and three timed
+  // variant for the passes not yet tuned), two warm-up steps and five timed
   // steps with events around each kernel; p then keeps its fastest.  The
   // state and the AB2 history are saved first and put back after.
   const size_t hn = (size_t)c->g.H * c->g.nrun * c->g.Ny;
@@ -851,7 +851,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
   for (int p = 0; p < DNS_NUM_PASSES; ++p) keep[p] = best[p] = c->variant[p];
   // kernel slot of each pass in a step's events
   static const int slot[DNS_NUM_PASSES] = {0, 4, 1, 3, 5, 2};
-  const int ne = DNS_NUM_KERNELS + 1, nt = 3;
+  const int ne = DNS_NUM_KERNELS + 1, nt = 5;
   std::vector<cudaEvent_t> ev((size_t)ne * (nt + 1));
   for (auto& x : ev)
     if (!e) e = cudaEventCreate(&x);
@@ -861,6 +861,7 @@ dns_status dns_autotune(dns_ctx* c, double ms[DNS_NUM_PASSES * DNS_MAX_VARIANTS]
       if (!avail[p][r]) continue;
       for (int q = 0; q < DNS_NUM_PASSES; ++q) c->variant[q] = best[q];
       c->variant[p] = r;
+      e = enqueue(c, 0);
       for (int i = 0; i <= nt && !e; ++i) e = enqueue(c, 0, &ev[(size_t)i * ne]);
       if (!e) e = cudaStreamSynchronize(c->st);
       if (!e) st = check_status(c);

@@ -338,23 +338,31 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const float cs = (m & 3) == 0 ? 1.f : ((m & 3) == 2 ? -1.f : 0.f);  // T_128(y_m)
     long long it = 0;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-      // per-pencil factors while the tensor cores work
-      float fa[TC_NP], fb[TC_NP], fia[TC_NP], fib[TC_NP];
-      unsigned zero_mask = 0;
-#pragma unroll
-      for (int j = 0; j < TC_NP; ++j) {
-        const long long p = t * TC_NP + j;
+      // per-pencil factors while the tensor cores work: lane j < 8 forms
+      // pencil j's (FP64 divisions, once per warp), the warp shares them
+      float lfa = 0.f, lfb = 0.f, lfia = 0.f, lfib = 0.f;
+      bool lzero = false;
+      if (lane < TC_NP) {
+        const long long p = t * TC_NP + lane;
         int run, kx, kz;
         pencil_modes(g, p, run, kx, kz);
         double ia, ib;
         wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-        const bool zero = kx == 0 && kz == 0;
-        const double kmn1 = zero ? 0.0 : 1.0 / kmn_of(ia, ib);
-        fa[j] = (float)(ia * kmn1);
-        fb[j] = (float)(ib * kmn1);
-        fia[j] = (float)ia;
-        fib[j] = (float)ib;
-        zero_mask |= (zero ? 1u : 0u) << j;
+        lzero = kx == 0 && kz == 0;
+        const double kmn1 = lzero ? 0.0 : 1.0 / kmn_of(ia, ib);
+        lfa = (float)(ia * kmn1);
+        lfb = (float)(ib * kmn1);
+        lfia = (float)ia;
+        lfib = (float)ib;
+      }
+      float fa[TC_NP], fb[TC_NP], fia[TC_NP], fib[TC_NP];
+      const unsigned zero_mask = __ballot_sync(0xffffffffu, lzero) & ((1u << TC_NP) - 1u);
+#pragma unroll
+      for (int j = 0; j < TC_NP; ++j) {
+        fa[j] = __shfl_sync(0xffffffffu, lfa, j);
+        fb[j] = __shfl_sync(0xffffffffu, lfb, j);
+        fia[j] = __shfl_sync(0xffffffffu, lfia, j);
+        fib[j] = __shfl_sync(0xffffffffu, lfib, j);
       }
       const int sl = (int)(it & (TC_NSIDE - 1));
       if (!tc_wait(&bs->side[sl], (uint32_t)(it >> 2) & 1u, bs, status)) break;
@@ -407,14 +415,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (p < H) {
           float2 x[5];
           for (int q = 0; q < 5; ++q) x[q] = make_float2(sd.centre[j * 10 + 2 * q], sd.centre[j * 10 + 2 * q + 1]);
-          int run, kx, kz;
-        pencil_modes(g, p, run, kx, kz);
-          double ia, ib;
-          wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-          const bool zero = kx == 0 && kz == 0;
-          const double kmn1 = zero ? 0.0 : 1.0 / kmn_of(ia, ib);
           float2 f[6];
-          uvw_point(x, zero, (float)(ia * kmn1), (float)(ib * kmn1), (float)ia, (float)ib, f);
+          uvw_point(x, lzero, lfa, lfb, lfia, lfib, f);  // this lane's own pencil j
           float2* base = (float2*)out.base + p * out.ps;
           for (int fi = 0; fi < 6; ++fi) base[fi * out.fs + TC_NH] = f[fi];
         }
