@@ -190,11 +190,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (warp < 4) {
     const int m = warp * 32 + lane;
     const uint32_t lane_addr = tbase + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < 4 * TC_KP; c0 += 8) {
-      uint32_t w[8];
+    // 32 loads in flight per thread
+    for (int c0 = 0; c0 < 4 * TC_KP; c0 += 32) {
+      uint32_t w[4][8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) w[i] = __ldg(&atab[(size_t)(c0 + i) * TC_NH + m]);
-      tmem_st_x8(lane_addr + TC_COL_A + (uint32_t)c0, w);
+      for (int i = 0; i < 32; ++i) w[i >> 3][i & 7] = __ldg(&atab[(size_t)(c0 + i) * TC_NH + m]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) tmem_st_x8(lane_addr + TC_COL_A + (uint32_t)(c0 + 8 * q), w[q]);
     }
     tmem_wait_st();
   }

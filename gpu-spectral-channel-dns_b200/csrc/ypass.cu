@@ -492,10 +492,9 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
   int run, kx, kz;
   pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
-  double ia, ib;
-  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-  const double kmn = kmn_of(ia, ib);
-  const double kmn1 = zero ? 0.0 : 1.0 / kmn;
+  // the pencil's wavenumbers and 1 / k^2: the FP64 divisions once per CTA
+  // (thread 0, under the copies), shared through shared memory
+  __shared__ double pen[3];
   // twiddles and the pencil's state by bulk copies on one barrier
   __shared__ uint64_t bar;
   if (threadIdx.x == 0) {
@@ -504,8 +503,14 @@ __global__ void __launch_bounds__(96) k_y3w(const double2* __restrict__ V, const
     mbar_expect_tx(&bar, (uint32_t)(2 * Ny * 16));
     bulk_g2s(w, V + p * Ny, (uint32_t)(Ny * 16), &bar);
     bulk_g2s(oz, O + p * Ny, (uint32_t)(Ny * 16), &bar);
+    double a, b;
+    wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, a, b);
+    pen[0] = a;
+    pen[1] = b;
+    pen[2] = zero ? 0.0 : 1.0 / kmn_of(a, b);
   }
   __syncthreads();
+  const double ia = pen[0], ib = pen[1], kmn1 = pen[2];
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, ph.wait_limit, status))) {
     if (threadIdx.x == 0) {
       atomicOr(status, 1);
@@ -932,10 +937,10 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   int run, kx, kz;
   pencil_modes(g, p, run, kx, kz);
   const bool zero = (kx == 0 && kz == 0);
-  double ia, ib;
-  wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, ia, ib);
-  const double kmn = kmn_of(ia, ib);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // the pencil's wavenumbers, k^2, dt and dt / (2 Re): the FP64 divisions
+  // once per CTA (thread 0, under the copies), shared through shared memory
+  __shared__ double pen[5];
 
   // 1. bulk copies on one barrier: the three Lamb pencils (Py
   //    values, natural order, at the start of each warp's line: the first
@@ -953,8 +958,17 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
       bulk_g2s(nvc, Nvp + p * Ny, (uint32_t)(Ny * 16), &bar);
       bulk_g2s(noc, Nop + p * Ny, (uint32_t)(Ny * 16), &bar);
     }
+    double a, b;
+    wavenumbers(kx, kz, g.Nz, ph.aphi, ph.beta, a, b);
+    const double dt = run_dt(ph, run), Re = run_Re(ph, run);
+    pen[0] = a;
+    pen[1] = b;
+    pen[2] = kmn_of(a, b);
+    pen[3] = dt;
+    pen[4] = dt * 0.5 / Re;
   }
   __syncthreads();
+  const double ia = pen[0], ib = pen[1], kmn = pen[2];
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, ph.wait_limit, status))) {
     if (threadIdx.x == 0) {
       atomicOr(status, 1);
@@ -991,10 +1005,10 @@ __global__ void __launch_bounds__(160, sizeof(C) == 8 ? 6 : 4) k_y1w(PencilArr l
   }
   __syncthreads();
   // 3. nonlinear terms (coefficients) -> history; interpolated right-hand sides
-  const double dt = run_dt(ph, run), Re = run_Re(ph, run), gam = ia * dt * 0.5;
+  const double dt = pen[3], gam = ia * dt * 0.5;
   const double kap = -0.5 * ib * dt;  // tilting weight (source/linear.cpp:147-151)
-  // the CN operators' coefficients, one division per CTA
-  const double h = dt * 0.5 / Re, c2v = 1 - 2.0 * kmn * h, c0v = kmn * (1 - kmn * h), c0o = 1 - kmn * h;
+  // the CN operators' coefficients
+  const double h = pen[4], c2v = 1 - 2.0 * kmn * h, c0v = kmn * (1 - kmn * h), c0o = 1 - kmn * h;
   double2* fv = lx;
   double2* fo = ly;
   for (int k = threadIdx.x; k < Ny; k += blockDim.x) {
