@@ -134,6 +134,12 @@ class ClockSampler:
                  "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a while to start: wait for its first sample,
+            # then keep only the samples taken from here on (the timed region)
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.rows = []
         except Exception:
             self.proc = None
         return self
