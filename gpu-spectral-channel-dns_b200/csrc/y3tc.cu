@@ -102,10 +102,12 @@ __device__ __forceinline__ uint32_t b_off(int n, int kc) {
 // 10-bit mantissa, clear the 13 low bits
 __device__ __forceinline__ uint32_t tf32_bits(uint32_t u) { return (u + 0x1000u) & ~0x1FFFu; }
 
-// x = hi + lo to FP32 rounding (~2^-24 |x| beyond the 2^-22 of the TF32 pair)
+// x = hi + lo: hi rounded to TF32, lo the exact FP32 remainder passed as
+// it is (the tensor core reads the top 19 bits of a TF32 operand, so lo
+// enters truncated: error < 2^-10 |lo| <= 2^-21 |x|)
 __device__ __forceinline__ void split_f(float x, uint32_t& hi, uint32_t& lo) {
   hi = tf32_bits(__float_as_uint(x));
-  lo = tf32_bits(__float_as_uint(x - __uint_as_float(hi)));
+  lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
 __device__ __forceinline__ float2 cmul_i(float2 a, float s) { return make_float2(-a.y * s, a.x * s); }  // i s a
