@@ -258,18 +258,30 @@ __global__ void __launch_bounds__(64, 16) k_colloc_fused(const double2* __restri
   wfft_io<double2, L, 1, false>(line, wtw_of(tab, 0), ld, st, LS);
   __syncwarp();
   for (int k = Ny + lane; k < LB; k += 32) line[k] = cx(0, 0);
-  // K-fold integration: (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0
+  // K-fold integration: (B x)_k = (c_{k-1} x_{k-1} - x_{k+1}) / (2k), (B x)_0 = 0;
+  // each lane keeps the weights 1 / (2k) of its elements k = lane + 32 i
+  // (the divisions once, not once per sweep)
   const int K = (warp == 0 && !zero) ? 4 : 2;
+  constexpr int KPL = (LB + 31) / 32;
+  double w2k[KPL];
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    w2k[i] = k >= 1 ? 1.0 / (2.0 * k) : 0.0;
+  }
   double2* x = line;
   double2* yb = line + LB;
   for (int it = 0; it < K; ++it) {
     __syncwarp();
-    for (int k = lane; k < LB; k += 32) {
+#pragma unroll
+    for (int i = 0; i < KPL; ++i) {
+      const int k = lane + 32 * i;
+      if (k >= LB) break;
       double2 r = cx(0, 0);
       if (k >= 1) {
         const double2 xm = x[k - 1] * (k == 1 ? 2.0 : 1.0);
         const double2 xp = (k + 1 < LB) ? x[k + 1] : cx(0, 0);
-        r = (xm - xp) * (1.0 / (2.0 * k));
+        r = (xm - xp) * w2k[i];
       }
       yb[k] = r;
     }
