@@ -1163,7 +1163,7 @@ cudaError_t enqueue_solve_wall(dns_ctx* c, const double2* bv, const double2* bo,
   const double* cosk = c->rtab + 4 * (size_t)c->wd.nv + 2 * (size_t)c->wd.no;
   // one kernel where the DCT length has a warp plan, else three
   cudaError_t e = launch_colloc_fused(bv, bo, bp, pbc, cosk, c->Ut, c->ddUt, c->rv, c->ro, c->wd, g, c->ph,
-                                      c->fy0_d.tab(), c->st);
+                                      c->fy0_d.tab(), c->status, c->st);
   if (e == cudaErrorNotSupported) {
     e = launch_colloc_prep(bv, bo, bp, sv, so, ls, pbc, cosk, c->Ut, c->ddUt, g, c->ph, c->st);
     if (!e) e = launch_cheby_inplace<double2>(PencilArr{sv, ls, 0}, 2 * g.H, 3, g.Ny, c->fy0_d.tab(), c->st);

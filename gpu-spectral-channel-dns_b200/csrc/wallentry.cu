@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "mbar.cuh"
 #include "wallsolve_dev.cuh"
 #include "wfft.cuh"
 
@@ -189,16 +190,38 @@ __global__ void __launch_bounds__(64, 16) k_colloc_fused(const double2* __restri
                                                      long long bp, double2* pbc, const double* __restrict__ cosk,
                                                      const double* __restrict__ Ut, const double* __restrict__ ddUt,
                                                      double2* gv, double2* go, int nv, int no, long long gp,
-                                                     DnsGeom g, PhysParams ph, FftTab<double2> tab) {
+                                                     DnsGeom g, PhysParams ph, FftTab<double2> tab, int* status) {
   constexpr int N = L / 2, Ny = N + 1, LB = Ny + 8;
   constexpr int LS = (wlen<double2>(L) > 2 * LB) ? wlen<double2>(L) : 2 * LB;  // line stride
+  static_assert(LS - Ny >= Ny, "the staged right-hand side lies above the point values");
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint64_t bars[2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2* line = (double2*)smem_raw + (size_t)warp * LS;
   const long long p = blockIdx.x;
   const int kx = (int)(p % g.Kx), kz = (int)(p / g.Kx);
   const bool zero = p == 0;
-  const double2* b = (warp ? bo : bv) + p * bp;
+  // this warp's right-hand side (Ny point values) by one bulk copy into the
+  // top of its line, above the point values the next loop writes (the
+  // launcher checks the 16-byte alignment)
+  const double2* b = line + (LS - Ny);
+  {
+    uint64_t* bar = &bars[warp];
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+      mbar_expect_tx(bar, (uint32_t)(Ny * 16));
+      bulk_g2s(line + (LS - Ny), (warp ? bo : bv) + p * bp, (uint32_t)(Ny * 16), bar);
+    }
+    __syncwarp();
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, 0, ph.wait_limit, status))) {
+      if (lane == 0) {
+        atomicOr(status, 1);
+        mbar_wait_bounded(bar, 0, DNS_WAIT_LIMIT, nullptr);  // let the copy land before leaving
+      }
+      return;
+    }
+  }
   // wall polynomial (every lane; rows 0..3 of the right-hand side)
   double2 pc0, pc1, pc2 = cx(0, 0), pc3 = cx(0, 0);
   {
@@ -339,17 +362,18 @@ cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const dou
 cudaError_t launch_colloc_fused(const double2* bv, const double2* bo, long long bp, double2* pbc,
                                 const double* cosk, const double* Ut, const double* ddUt, double2* gv,
                                 double2* go, const WallDims& wd, const DnsGeom& g, const PhysParams& ph,
-                                FftTab<double2> tab, cudaStream_t st) {
+                                FftTab<double2> tab, int* status, cudaStream_t st) {
   auto go1 = [&](auto LL) -> cudaError_t {
     constexpr int L = decltype(LL)::value;
     if constexpr (WPlan<L, 1, FftMaxRadix<double2>::v>::ok) {
-      if (tab.plan.L != L || g.Ny != L / 2 + 1 || !tab.tw) return cudaErrorNotSupported;
+      if (tab.plan.L != L || g.Ny != L / 2 + 1 || !tab.tw || !status || !aligned16(bv) || !aligned16(bo))
+        return cudaErrorNotSupported;
       constexpr int LB = L / 2 + 9;
       constexpr int LS = (wlen<double2>(L) > 2 * LB) ? wlen<double2>(L) : 2 * LB;
       const size_t sm = (size_t)2 * LS * 16;
       cudaFuncSetAttribute(k_colloc_fused<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_colloc_fused<L><<<(unsigned)g.H, 64, sm, st>>>(bv, bo, bp, pbc, cosk, Ut, ddUt, gv, go, wd.nv, wd.no,
-                                                       wd.gp, g, ph, tab);
+                                                       wd.gp, g, ph, tab, status);
       return cudaGetLastError();
     }
     return cudaErrorNotSupported;

@@ -55,7 +55,7 @@ cudaError_t launch_colloc_integrate(const double2* cv, const double2* co, long l
 cudaError_t launch_colloc_fused(const double2* bv, const double2* bo, long long bp, double2* pbc,
                                 const double* cosk, const double* Ut, const double* ddUt, double2* gv,
                                 double2* go, const WallDims& wd, const DnsGeom& g, const PhysParams& ph,
-                                FftTab<double2> tab, cudaStream_t st);
+                                FftTab<double2> tab, int* status, cudaStream_t st);
 cudaError_t launch_colloc_finish(const double2* Xv, const double2* Xo, const double2* pbc,
                                  double2* ov, double2* oo, long long op, const DnsGeom& g,
                                  cudaStream_t st);
