@@ -47,13 +47,13 @@ template <int L, int NL, int MAXR> struct WPlan { enum { ok = 0 }; };
 // FP32
 WPLAN(128, 1, 16, 4, 4, 4, 2)
 WPLAN(256, 1, 16, 8, 8, 4)
-WPLAN(384, 1, 16, 12, 4, 4, 2)
+WPLAN(384, 1, 16, 8, 8, 6)
 WPLAN(512, 1, 16, 8, 8, 8)
 WPLAN(768, 1, 16, 8, 8, 12)
 WPLAN(128, 2, 16, 8, 4, 4)
-WPLAN(192, 2, 16, 12, 4, 4)
+WPLAN(192, 2, 16, 16, 12)
 WPLAN(256, 2, 16, 16, 16)
-WPLAN(384, 2, 16, 8, 8, 6)
+WPLAN(384, 2, 16, 16, 24)
 WPLAN(512, 2, 16, 32, 16)
 WPLAN(768, 2, 16, 16, 48)
 WPLAN(384, 3, 16, 12, 4, 4, 2)
