@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(32 * NW) k_zbw(PencilArr in, RowArr out, DnsGe
 // columns beyond Kx read as the copy's zero fill.  No per-element global
 // loads, no L1 dependence.
 template <typename C, int L, int NW, int TX, int TY>
-__global__ void __launch_bounds__(32 * NW, 4) k_zbt(const __grid_constant__ CUtensorMap tin, RowArr out,
+__global__ void __launch_bounds__(32 * NW, 3) k_zbt(const __grid_constant__ CUtensorMap tin, RowArr out,
                                                  DnsGeom g, FftTab<C> tab, int* status) {
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
   constexpr int NL = ST::NL, LS = ST::LS, Pz = L;
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(32 * NW) k_zfw(RowArr in, PencilArr out, DnsGe
 // first FFT pass reads them there.  Rows beyond Py and columns beyond Kx
 // read as the copy's zero fill.
 template <typename C, int L, int NW>
-__global__ void __launch_bounds__(32 * NW, 4) k_zft(const __grid_constant__ CUtensorMap tin, PencilArr out,
+__global__ void __launch_bounds__(32 * NW, 3) k_zft(const __grid_constant__ CUtensorMap tin, PencilArr out,
                                                     DnsGeom g, FftTab<C> tab, int* status) {
   constexpr int TX = 4, TY = 4;
   typedef SpanTile<C, L, TX, TY, 32 * NW> ST;
